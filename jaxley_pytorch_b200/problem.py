@@ -1,0 +1,293 @@
+"""The problem format: everything one simulation of the hot path consumes.
+
+A `Problem` holds, in the reference's node order, what `jx.integrate` assembles
+before its step loop (`integrate.py:481-622` in jaxley-pytorch):
+
+* the tree system of the implicit-Euler voltage step, as the reference stores it:
+  axial conductances per compartment edge (`utils/morph_attributes.py:315-436`), the
+  edge sinks (`modules/base.py:3080-3084`) and the DHS solve order with its lower /
+  upper maps and parent lookup (`modules/base.py:1142-1266`,
+  `modules/network.py:192-293`);
+* the inserted channels in insertion order with their node indices
+  (`modules/base.py:3050-3068`);
+* all parameters and initial states as `(B, n_nodes)` or `(n_nodes,)` arrays,
+  including the initial channel currents (`modules/base.py:2375-2383`);
+* the step-current stimuli (`integrate.py:495-568`) and the recordings
+  (`integrate.py:53-84`);
+* regular-layout synapse types (`modules/network.py:295-348`).
+
+A `Problem` comes either from a reference `Module` (`problem_from_module`, for users
+of jaxley-pytorch and for the parity fixtures) or from the seeded generators in
+`synth.py`. Both the CUDA path (`lower.py`) and the CPU restatement consume it.
+"""
+from __future__ import annotations
+
+from dataclasses import dataclass, field
+from typing import Dict, List, Optional, Tuple
+
+import numpy as np
+
+from .channels import ChannelInstance, spec_for_reference_channel, current_name
+
+
+@dataclass
+class SynapseType:
+    """A synapse type in the regular layout: synapses ordered by postsynaptic node,
+    `k` per node (`utils/syn_utils.py:13-27`). `model` is 0 for `KineticSynapse`,
+    1 for `SigmoidRateSynapse` (`kernels/synapse_step.py:43`)."""
+
+    model: int
+    name: str
+    pre: np.ndarray  # (E,) presynaptic node index (reference node order)
+    post: np.ndarray  # (E,) postsynaptic node index
+    k: int
+    targets: np.ndarray  # (E // k,) postsynaptic nodes, increasing
+    params: List[np.ndarray]  # one (E,) array per parameter, in the reference order
+    param_names: List[str]
+    state: Optional[np.ndarray]  # (B or 1, E) initial `s` (kinetic), else None
+    current: Optional[np.ndarray] = None  # (B or 1, E) initial current (recording)
+
+
+@dataclass
+class Problem:
+    n_nodes: int
+    comp_inds: np.ndarray  # compartments (nodes that are not branchpoints)
+    # Tree system (reference layout).
+    sinks: np.ndarray  # (E_ax,) sink node of every compartment edge
+    axial: np.ndarray  # (E_ax,) or (B, E_ax) axial conductances (divided by cm)
+    parent_lookup: np.ndarray  # (n_nodes,) parent in solve order, -1 for roots
+    to_solve: np.ndarray  # (n_nodes,) node index of solve position j
+    map_lower: np.ndarray  # (n_nodes,) axial edge of the lower of solve position j
+    map_upper: np.ndarray  # (n_nodes,) axial edge of the upper of solve position j
+    channels: List[ChannelInstance]
+    params: Dict[str, np.ndarray]
+    states: Dict[str, np.ndarray]
+    dt: float
+    n_steps: int  # number of steps simulated (recordings have n_steps + 1 samples)
+    stim_inds: np.ndarray = field(default_factory=lambda: np.zeros(0, np.int64))
+    stim: Optional[np.ndarray] = None  # (B or 1, n_stim, >= n_steps) in nA
+    recordings: List[Tuple[str, int]] = field(default_factory=list)
+    synapses: List[SynapseType] = field(default_factory=list)
+    batch: int = 1
+    current_names: List[str] = field(default_factory=list)
+
+    def solve_order_system(self):
+        """Per solve position `j`: parent, `g_low[j]` (coupling of row `j` to its
+        parent) and `g_up[j]` (coupling of the parent's row to `j`), both as axial
+        conductances before the `-dt` factor (`solver_voltage.py:330-348`)."""
+        parent = np.asarray(self.parent_lookup, dtype=np.int64)
+        ax = np.asarray(self.axial, dtype=np.float64)
+        if ax.shape[-1] == 0:
+            z = np.zeros(ax.shape[:-1] + (self.n_nodes,))
+            return parent, z, z
+        g_low = ax[..., self.map_lower]
+        g_up = ax[..., self.map_upper]
+        has = parent >= 0
+        g_low = np.where(has, g_low, 0.0)
+        g_up = np.where(has, g_up, 0.0)
+        return parent, g_low, g_up
+
+    def gsum(self):
+        """Sum of the axial conductances of the edges that sink into every node."""
+        ax = np.asarray(self.axial, dtype=np.float64)
+        rows = ax.reshape(-1, ax.shape[-1])
+        out = np.zeros((rows.shape[0], self.n_nodes))
+        for b in range(rows.shape[0]):
+            np.add.at(out[b], np.asarray(self.sinks, dtype=np.int64), rows[b])
+        return out if ax.ndim == 2 else out[0]
+
+
+def _np(x, dtype=np.float64):
+    import torch
+
+    if isinstance(x, torch.Tensor):
+        return x.detach().cpu().numpy().astype(dtype)
+    return np.asarray(x, dtype=dtype)
+
+
+def _flatten_batch(a: np.ndarray) -> np.ndarray:
+    """`(..., n)` -> `(n,)` without batch dims, else `(B, n)`."""
+    if a.ndim <= 1:
+        return a
+    return a.reshape(-1, a.shape[-1])
+
+
+def problem_from_module(
+    module,
+    params: list = [],
+    param_state: Optional[list] = None,
+    data_stimuli=None,
+    t_max: Optional[float] = None,
+    delta_t: float = 0.025,
+) -> Problem:
+    """Lower a reference `jx.Module` (jaxley-pytorch) into a `Problem`.
+
+    Follows `jx.integrate` (`integrate.py:476-622`): the stimulus is padded or
+    truncated to `int(t_max // delta_t + 1)` samples, parameters come from
+    `get_all_parameters`, initial states from `get_all_states` plus the initial
+    currents (`_append_currents_with_plan`). Only the `bwd_euler` step with the DHS
+    solve is covered, with at most one leading batch dimension.
+    """
+    import torch
+
+    from jaxley_pytorch.integrate import _batch_shape, _expand_states  # noqa: F401
+    from jaxley_pytorch.utils.cell_utils import params_to_pstate
+    from jaxley_pytorch.utils.torch_utils import tree_tensors
+
+    base = module.base
+    device = torch.device("cpu")
+    dtype = torch.float64
+    module.to_torch(device=device, dtype=dtype)
+
+    # Externals (stimuli only; clamps are not part of this path).
+    externals = {k: torch.as_tensor(v, dtype=dtype) for k, v in module.externals.items()}
+    external_inds = dict(module.external_inds)
+    if data_stimuli is not None:
+        from jaxley_pytorch.integrate import add_stimuli
+
+        externals, external_inds = add_stimuli(externals, external_inds, data_stimuli)
+    if any(k != "i" for k in externals):
+        raise NotImplementedError("clamps are not part of the CUDA step path")
+    if "i" in externals:
+        stim = externals["i"]
+        n_samples = stim.shape[-1]
+        if t_max is not None:
+            want = int(t_max // delta_t + 1)
+            if want > n_samples:
+                pad = torch.zeros((*stim.shape[:-1], want - n_samples), dtype=dtype)
+                stim = torch.cat([stim, pad], dim=-1)
+            else:
+                stim = stim[..., :want]
+        n_steps = stim.shape[-1]
+        stim_np = _np(stim)
+        if stim_np.ndim == 2:
+            stim_np = stim_np[None]
+        stim_np = stim_np.reshape(-1, *stim_np.shape[-2:])
+        stim_inds = np.asarray(external_inds["i"], dtype=np.int64)
+    else:
+        assert t_max is not None
+        n_steps = int(t_max // delta_t + 1)
+        stim_np, stim_inds = None, np.zeros(0, np.int64)
+
+    pstate = params_to_pstate(params, module.indices_set_by_trainables)
+    if param_state is not None:
+        pstate = pstate + list(param_state)
+    all_params = module.get_all_parameters(pstate)
+    init_states = module.get_all_states(pstate)
+    batch = _batch_shape(list(tree_tensors(all_params)) + list(tree_tensors(init_states)))
+    init_states = _expand_states(init_states, batch)
+    plan = module._get_step_plan(device, "jaxley.dhs.gpu", "bwd_euler")
+    gathered = module._gather_step_params(plan, all_params)
+    init_states = module._append_currents_with_plan(init_states, delta_t, plan, gathered)
+
+    n = int(base._n_nodes)
+    indexer = base._dhs_solve_indexer
+    channels = []
+    for cp in plan["channels"]:
+        ch = cp["channel"]
+        type_name, spec = spec_for_reference_channel(ch)
+        pnames = list(ch.channel_params.keys())
+        snames = list(ch.channel_states.keys())
+        consts = [float(ch.channel_constants[k]) for k, _ in spec.constants]
+        channels.append(
+            ChannelInstance(
+                type_name=type_name,
+                name=ch._name,
+                inds=_np(cp["inds"], np.int64),
+                params=pnames,
+                states=snames,
+                current=ch.current_name,
+                constants=consts,
+            )
+        )
+
+    def flat(d):
+        out = {}
+        for k, v in d.items():
+            if isinstance(v, dict):
+                continue
+            if isinstance(v, torch.Tensor) and v.ndim >= 1 and v.shape[-1] == n:
+                out[k] = _flatten_batch(_np(v))
+        return out
+
+    params_np = flat(all_params)
+    states_np = flat(init_states)
+    axial = _flatten_batch(_np(all_params["axial_conductances"]["v"]))
+
+    synapses = []
+    for sp, gp in zip(plan["synapses"], gathered["synapses"]):
+        synapses.append(_synapse_from_plan(sp, gp, init_states))
+
+    rec = []
+    for idx, name in zip(
+        module.recordings.rec_index.to_numpy().astype(int), module.recordings.state.to_numpy()
+    ):
+        rec.append((str(name), int(idx)))
+
+    batches = [a.shape[0] for a in list(params_np.values()) + list(states_np.values()) if a.ndim == 2]
+    if stim_np is not None:
+        batches.append(stim_np.shape[0])
+    if axial.ndim == 2:
+        batches.append(axial.shape[0])
+    B = max(batches) if batches else 1
+
+    return Problem(
+        n_nodes=n,
+        comp_inds=np.asarray(base._internal_node_inds, dtype=np.int64),
+        sinks=_np(plan["sinks"], np.int64),
+        axial=axial,
+        parent_lookup=np.asarray(indexer["parent_lookup"], dtype=np.int64)[:n],
+        to_solve=np.asarray(indexer["map_to_solve_order"], dtype=np.int64),
+        map_lower=np.asarray(indexer["map_to_solve_order_lower"], dtype=np.int64),
+        map_upper=np.asarray(indexer["map_to_solve_order_upper"], dtype=np.int64),
+        channels=channels,
+        params=params_np,
+        states=states_np,
+        dt=float(delta_t),
+        n_steps=int(n_steps),
+        stim_inds=stim_inds,
+        stim=stim_np,
+        recordings=rec,
+        synapses=synapses,
+        batch=int(B),
+        current_names=list(base.membrane_current_names),
+    )
+
+
+def _synapse_from_plan(sp, gp, states) -> SynapseType:
+    if "k" not in sp:
+        raise NotImplementedError("only synapse types in the regular layout are covered")
+    syn = sp["synapse"]
+    cls = type(syn).__name__
+    if cls == "KineticSynapse":
+        model = 0
+    elif cls == "SigmoidRateSynapse":
+        model = 1
+    else:
+        raise NotImplementedError(f"synapse {cls} has no sm_100a implementation")
+    names = list(syn.synapse_params.keys())
+    E = int(sp["pre"].shape[0])
+    prm = []
+    for nm in names:
+        v = _np(gp["params"][nm])
+        if v.ndim != 1:
+            raise NotImplementedError("batched synapse parameters are not covered")
+        prm.append(np.broadcast_to(v, (E,)).copy())
+    state = None
+    if model == 0:
+        s = _np(states[f"{syn._name}_s"])
+        state = s.reshape(-1, E)
+    cur_name = f"i_{syn._name}"
+    current = _np(states[cur_name]).reshape(-1, E) if cur_name in states else None
+    return SynapseType(
+        model=model,
+        name=syn._name,
+        pre=_np(sp["pre"], np.int64),
+        post=_np(sp["post"], np.int64),
+        k=int(sp["k"]),
+        targets=_np(sp["targets"], np.int64),
+        params=prm,
+        param_names=names,
+        state=state,
+        current=current,
+    )
