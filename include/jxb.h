@@ -1,0 +1,221 @@
+/*
+ * jxb.h - C ABI of libjxb, the sm_100a kernels behind jaxley_pytorch_b200.
+ *
+ * Every entry point takes plain device pointers, sizes and a CUDA stream, returns an
+ * int status (JXB_OK = 0) and never allocates device memory; buffers are owned by the
+ * caller. The ABI replaces these reference interfaces of jaxley-pytorch:
+ *
+ *   jxb_tree_solve_registers  <- kernels/tree_solve.py:228-287 (_tree_solve_kernel),
+ *                                launched by TreeSolveKernel.solve, :396-422, and the
+ *                                custom op jaxley_pytorch::tree_solve, :518-563
+ *   jxb_tree_solve_levels     <- kernels/tree_solve.py:290-375 (_tree_solve_levels_kernel),
+ *                                launched by _launch_levels, :467-482, and the custom
+ *                                op jaxley_pytorch::tree_solve_levels, :589-609
+ *   jxb_synapse_forward       <- kernels/synapse_step.py:121-182 (_forward_kernel) and
+ *                                the op jaxley_pytorch::synapse_step, :336-363
+ *   jxb_synapse_backward      <- kernels/synapse_step.py:184-305 (_backward_kernel) and
+ *                                :307-330 (_presynaptic_sum_kernel), the op
+ *                                jaxley_pytorch::synapse_step_backward, :372-416
+ *   jxb_sim_forward           <- the per-step body of jx.integrate: integrate.py:624-636
+ *                                -> Module._step_with_plan, modules/base.py:3214-3400
+ *                                (channels :3402-3542, voltage solve
+ *                                solver_voltage.py:294-359), fused into one launch per
+ *                                segment of steps
+ *   jxb_sim_backward          <- loss.backward() through the same loop: the autograd
+ *                                of _step_with_plan and _DHSSolve.backward,
+ *                                solver_voltage.py:143-187, with the time
+ *                                checkpointing of utils/torch_utils.py:141-198
+ */
+#ifndef JXB_H_
+#define JXB_H_
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum {
+  JXB_OK = 0,
+  JXB_ERR_ARG = 1,        /* bad pointer, size or shape */
+  JXB_ERR_DTYPE = 2,      /* dtype not float32/float64 */
+  JXB_ERR_SMEM = 3,       /* the work item does not fit in shared memory */
+  JXB_ERR_LAUNCH = 4,     /* the CUDA launch failed (see jxb_last_error) */
+  JXB_ERR_TOO_LARGE = 5   /* a tree is larger than the selected kernel supports */
+};
+
+enum { JXB_F32 = 0, JXB_F64 = 1 };
+
+/* ---------------------------------------------------------------------------------
+ * Tree solve: x = A^{-1} s for a forest, A[i,i] = d[i], A[i,p] = l[i], A[p,i] = u[i]
+ * (p = parent of i), batch-major arrays of shape (batch, n).
+ * ------------------------------------------------------------------------------- */
+
+/* Schedule of the level variant: whole trees packed into blocks; inside a block the
+ * nodes are grouped into chains (a node and its only child form one chain), chains
+ * are ordered by level (leaf chains first). Node indices are solve-order indices of
+ * the caller's arrays; `perm` lists the block's nodes in chain order. */
+typedef struct {
+  int32_t n_nodes;        /* nodes per batch row */
+  int32_t n_blocks;
+  int32_t max_block_nodes;
+  int32_t max_levels;
+  const int32_t* block_info;  /* (n_blocks, 4): node start, node count, chain start, level-ptr start */
+  const int32_t* block_levels;/* (n_blocks,) number of chain levels */
+  const int32_t* perm;        /* (n_nodes,) chain-order position -> node index */
+  const int32_t* chain_top;   /* (n_chains,) first node (chain-order position, block-relative) */
+  const int32_t* chain_len;   /* (n_chains,) */
+  const int32_t* chain_ptop;  /* (n_chains,) parent of the top (block-relative) or -1 */
+  const int32_t* chain_cptr;  /* (n_chains+1,) child chains: CSR into chain_child */
+  const int32_t* chain_child; /* tops of the child chains (block-relative) */
+  const int32_t* level_ptr;   /* per block (levels+1) chain offsets */
+} JxbTreeSchedule;
+
+int jxb_tree_solve_levels(int dtype, const void* d, const void* l, const void* u,
+                          const void* s, void* x, int64_t batch,
+                          const JxbTreeSchedule* sched, void* stream);
+
+/* Register variant: every warp solves one block of whole trees of at most
+ * 32 * regs_per_lane nodes for one batch row, the block held in registers and the
+ * parent/child exchanges done with warp shuffles. */
+typedef struct {
+  int32_t n_nodes;
+  int32_t n_blocks;
+  int32_t regs_per_lane;      /* 1, 2, 4 or 8 */
+  int32_t num_slots;          /* max children per node */
+  const int32_t* block_info;  /* (n_blocks, 4): start, length, levels (height), depth */
+  const int32_t* rel_parent;  /* (n_blocks, 32*regs) parent (block-relative), self for roots */
+  const int32_t* rel_height;  /* (n_blocks, 32*regs) height, -1 for padding */
+  const int32_t* rel_children;/* (n_blocks, num_slots, 32*regs) children or -1 */
+} JxbRegSchedule;
+
+int jxb_tree_solve_registers(int dtype, const void* d, const void* l, const void* u,
+                             const void* s, void* x, int64_t batch,
+                             const JxbRegSchedule* sched, void* stream);
+
+/* ---------------------------------------------------------------------------------
+ * Fused simulation step (bwd_euler + DHS) over segments of steps.
+ * ------------------------------------------------------------------------------- */
+
+typedef struct {
+  int32_t node0, n_nodes;     /* internal node range of the block */
+  int32_t slot0, n_slots;     /* state-slot range */
+  int32_t chain0, n_chains;   /* chains of the block, sorted by level */
+  int32_t level0, n_levels;   /* level_ptr[level0 .. level0 + n_levels] */
+  int32_t pslot0, n_pslots;   /* parameter-slot range */
+  int32_t pad0, pad1;
+} JxbBlock;
+
+typedef struct {
+  int32_t block;              /* index into blocks */
+  int32_t row0, n_rows;       /* batch rows of the state buffer */
+  int32_t pad;
+} JxbItem;
+
+typedef struct {
+  int32_t dtype;
+  int32_t batch;              /* rows of state / pscale / rec buffers */
+  int32_t n_nodes, n_slots, n_pslots, n_cols;
+  int32_t n_items, n_steps;   /* steps in this launch */
+  int32_t t0;                 /* absolute index of the first step */
+  int32_t max_rows;           /* rows per item (shared-memory sizing) */
+  int32_t max_nodes, max_slots;
+  double dt;
+  /* topology, internal (chain) node order */
+  const int32_t* node_class;  /* (n_nodes,) */
+  const int32_t* soff;        /* (n_nodes+1,) state-slot offsets */
+  const int32_t* poff;        /* (n_nodes+1,) parameter-slot offsets */
+  const void* a_low;          /* (n_nodes,) axial conductance row i -> parent */
+  const void* a_up;           /* (n_nodes,) axial conductance parent row -> i */
+  const void* gsum;           /* (n_nodes,) sum of axial conductances sinking into i */
+  const void* cm;             /* (n_nodes,) capacitance */
+  const int32_t* cls_ptr;     /* (n_classes+1,) entries of every node class */
+  const int32_t* cls_comp;    /* (n_classes,) 1 for compartments, 0 for branchpoints */
+  const void* entries;        /* channel entries (16-bit fields, see jxb_channels.cuh) */
+  int32_t n_classes, n_entries;
+  const void* pbase;          /* (n_pslots,) */
+  const int32_t* pcol;        /* (n_pslots,) column of pscale, 0 = no scale */
+  const void* pscale;         /* (batch, n_cols); column 0 holds 1 */
+  const JxbBlock* blocks;
+  const JxbItem* items;
+  const int32_t* chain_top;   /* internal node index */
+  const int32_t* chain_len;
+  const int32_t* chain_ptop;  /* internal node index or -1 */
+  const int32_t* chain_cptr;
+  const int32_t* chain_child; /* internal node index of child-chain tops */
+  const int32_t* level_ptr;   /* chain offsets relative to the block's chain0 */
+  /* stimulus: i_ext[node] += stim[t][b][idx] / area[node] * 1e5 */
+  const int32_t* stim_ptr;    /* (n_nodes+1,) CSR over nodes */
+  const int32_t* stim_idx;
+  const void* area;           /* (n_nodes,) */
+  const void* stim;           /* (stim_steps, stim_rows, n_stim) */
+  int32_t n_stim, stim_steps, stim_rows, pad0;
+  /* synaptic terms added to lin/const before dividing by cm (may be null) */
+  const void* syn_lin;        /* (batch, n_nodes) */
+  const void* syn_const;      /* (batch, n_nodes) */
+  /* recordings: CSR over nodes */
+  const int32_t* rec_ptr;     /* (n_nodes+1,) */
+  const int32_t* rec_slot;    /* node-relative slot, -1 records 0 */
+  const int32_t* rec_col;     /* output column */
+  void* rec_out;              /* (T + 1, batch, n_rec), time index t0 + step + 1 */
+  int32_t n_rec, pad1;
+  /* state */
+  void* state;                /* (batch, n_slots), updated in place */
+  void* ckpt;                 /* optional (n_ckpt, batch, n_slots): state at t0 + m*ckpt_every */
+  int32_t ckpt_every, ckpt_base;  /* ckpt index of t0 is (t0 - ckpt_base) / ckpt_every */
+  void* traj;                 /* optional (n_steps, batch, n_slots): state before each step */
+  /* adjoint */
+  void* adj;                  /* (batch, n_slots) adjoint of the state, updated in place */
+  const void* rec_grad;       /* (T + 1, batch, n_rec) gradient of the recordings */
+  void* pgrad;                /* (batch, n_pslots) float64, accumulated */
+  int32_t mode, pad2;         /* 0 = step, 1 = initial currents only */
+} JxbSimArgs;
+
+int jxb_sim_forward(const JxbSimArgs* args, void* stream);
+int jxb_sim_backward(const JxbSimArgs* args, void* stream);
+int64_t jxb_sim_smem_bytes(const JxbSimArgs* args, int backward);
+
+/* ---------------------------------------------------------------------------------
+ * Synapses in the regular layout (E = T * k synapses ordered by target).
+ * ------------------------------------------------------------------------------- */
+typedef struct {
+  int32_t dtype, model;       /* 0 KineticSynapse, 1 SigmoidRateSynapse */
+  int32_t batch, n_nodes, n_syn, k;
+  int32_t targets_are_nodes, store_current;
+  const void* v;              /* (batch, n_nodes) */
+  const void* s;              /* (batch, n_syn) kinetic state or null */
+  const int32_t* pre;         /* (n_syn,) */
+  const int32_t* targets;     /* (n_syn / k,) */
+  const void* p[6];           /* (n_syn,) parameters in the reference order */
+  const void* area;           /* (n_syn,) area of the postsynaptic compartment */
+  const void* scalars;        /* (2,) dt, diff */
+  void* s_new;                /* (batch, n_syn) or null */
+  void* current;              /* (batch, n_syn) or null */
+  void* lin;                  /* (batch, n_syn / k) */
+  void* cst;                  /* (batch, n_syn / k) */
+  /* backward */
+  const void* g_s_new;        /* (batch, n_syn) or null */
+  const void* g_current;      /* (batch, n_syn) or null */
+  const void* g_lin;          /* (batch, n_syn / k) */
+  const void* g_const;        /* (batch, n_syn / k) */
+  void* g_s;                  /* (batch, n_syn) or null */
+  void* g_v;                  /* (batch, n_nodes), overwritten */
+  void* g_params;             /* (n_need, n_syn), overwritten */
+  void* g_pre;                /* (n_syn, batch) scratch for the presynaptic sum */
+  int32_t need;               /* bit mask of parameters that need gradients */
+  int32_t inv_width, n_pre_nodes, pad;
+  const int32_t* inv;         /* (n_pre_nodes, inv_width) synapses of every pre node */
+  const int32_t* pre_nodes;   /* (n_pre_nodes,) */
+} JxbSynArgs;
+
+int jxb_synapse_forward(const JxbSynArgs* args, void* stream);
+int jxb_synapse_backward(const JxbSynArgs* args, void* stream);
+
+/* Text of the last error of this thread (static storage). */
+const char* jxb_last_error(void);
+int jxb_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* JXB_H_ */

@@ -1,0 +1,223 @@
+// Channel models of the step kernels: gating rates, exponential-Euler updates and
+// ohmic currents, written once for a scalar type S (float, double, or a Dual of
+// them for the adjoint's derivative with respect to the voltage).
+//
+// Each rate function restates the reference class at the cited line
+// (jaxley-pytorch). Type ids match jaxley_pytorch_b200/channels.py.
+#pragma once
+#include "jxb_math.cuh"
+
+namespace jxb {
+
+enum ChannelType {
+  CH_HH = 0, CH_LEAK = 1, CH_NATAT = 2, CH_NATS2T = 3, CH_NAPET2 = 4, CH_KPST = 5,
+  CH_KTST = 6, CH_SKE2 = 7, CH_SKV3_1 = 8, CH_M = 9, CH_CAHVA = 10, CH_CALVA = 11,
+  CH_CAPUMP = 12, CH_CANERNST = 13, CH_H = 14
+};
+
+// One channel of a node class: its type and the node-relative slots of its states
+// (role order of the reference's `channel_states`), of its current state and of its
+// parameters (role order of `channel_params`, then `channel_constants`).
+struct ChanEntry {
+  short type, ns, np, cur;
+  short s[6];
+  short p[8];
+};
+
+enum GateId {
+  G_HH_M, G_HH_H, G_HH_N, G_NATAT_M, G_NATAT_H, G_NATS2T_M, G_NATS2T_H, G_NAP_M,
+  G_NAP_H, G_KPST_M, G_KPST_H, G_KTST_M, G_KTST_H, G_SKV31_M, G_M_M, G_CAHVA_M,
+  G_CAHVA_H, G_CALVA_M, G_CALVA_H, G_H_M
+};
+
+// Gates in alpha/beta form (`solve_gate_exponential`, solver_gate.py:45-53) versus
+// x_inf/tau form (`solve_inf_gate_exponential`, solver_gate.py:67-87).
+__device__ __forceinline__ bool gate_is_alpha_beta(int g) {
+  return g == G_HH_M || g == G_HH_H || g == G_HH_N || g == G_CAHVA_M || g == G_CAHVA_H;
+}
+
+template <typename S> struct Pair { S a, b; };
+
+// Rates of every gate: (alpha, beta) or (x_inf, tau).
+template <typename S>
+__device__ __forceinline__ Pair<S> gate_rates(int g, S v) {
+  typedef typename Base<S>::type B;
+  const B qt = B(2.952882641412121);  // 2.3 ** ((34 - 21) / 10), l5pc.py
+  Pair<S> r;
+  switch (g) {
+    case G_HH_M:  // channels/hh.py:88-92
+      r.a = B(0.1) * x_over_expm1(-(v + B(40)), B(10));
+      r.b = B(4.0) * save_exp(-(v + B(65)) / B(18));
+      break;
+    case G_HH_H:  // channels/hh.py:94-98
+      r.a = B(0.07) * save_exp(-(v + B(65)) / B(20));
+      r.b = B(1.0) / (save_exp(-(v + B(35)) / B(10)) + B(1));
+      break;
+    case G_HH_N:  // channels/hh.py:100-104
+      r.a = B(0.01) * x_over_expm1(-(v + B(55)), B(10));
+      r.b = B(0.125) * save_exp(-(v + B(65)) / B(80));
+      break;
+    case G_NATAT_M:
+    case G_NATS2T_M: {  // l5pc.py:95-103, 177-185
+      B off = g == G_NATAT_M ? B(38) : B(32);
+      S alpha = (B(0.182) * (v + off + B(1e-6))) / (B(1) - save_exp(-(v + off + B(1e-6)) / B(6)));
+      S beta = (B(0.124) * (-v - off + B(1e-6))) / (B(1) - save_exp(-(-v - off + B(1e-6)) / B(6)));
+      r.a = alpha / (alpha + beta);
+      r.b = B(1) / (alpha + beta) / qt;
+      break;
+    }
+    case G_NATAT_H:
+    case G_NATS2T_H: {  // l5pc.py:105-113, 187-195
+      B off = g == G_NATAT_H ? B(66) : B(60);
+      S alpha = (B(-0.015) * (v + off + B(1e-6))) / (B(1) - save_exp((v + off + B(1e-6)) / B(6)));
+      S beta = (B(-0.015) * (-v - off + B(1e-6))) / (B(1) - save_exp((-v - off + B(1e-6)) / B(6)));
+      r.a = alpha / (alpha + beta);
+      r.b = B(1) / (alpha + beta) / qt;
+      break;
+    }
+    case G_NAP_M: {  // l5pc.py:268-276
+      S alpha = (B(0.182) * (v + B(38) + B(1e-6))) / (B(1) - save_exp(-(v + B(38) + B(1e-6)) / B(6)));
+      S beta = (B(0.124) * (-v - B(38) + B(1e-6))) / (B(1) - save_exp(-(-v - B(38) + B(1e-6)) / B(6)));
+      r.b = B(6) / (alpha + beta) / qt;
+      r.a = B(1.0) / (B(1) + save_exp((v + B(52.6)) / B(-4.6)));
+      break;
+    }
+    case G_NAP_H: {  // l5pc.py:278-289
+      S alpha = (B(-2.88e-6) * (v + B(17) + B(1e-6))) / (B(1) - save_exp((v + B(17) + B(1e-6)) / B(4.63)));
+      S beta = (B(6.94e-6) * (v + B(64.4) + B(1e-6))) /
+               (B(1) - save_exp((-(v + B(64.4)) + B(1e-6)) / B(2.63)));
+      r.b = B(1) / (alpha + beta) / qt;
+      r.a = B(1.0) / (B(1) + save_exp((v + B(48.8)) / B(10)));
+      break;
+    }
+    case G_KPST_M: {  // l5pc.py:355-369
+      S va = v + B(10);
+      r.a = B(1) / (B(1) + save_exp(-(va + B(1)) / B(12)));
+      if (val(va) < B(-50.0))
+        r.b = (B(1.25) + B(175.03) * save_exp(va * B(0.026))) / qt;
+      else
+        r.b = (B(1.25) + B(13) * save_exp(-va * B(0.026))) / qt;
+      break;
+    }
+    case G_KPST_H: {  // l5pc.py:371-381
+      S va = v + B(10);
+      r.a = B(1) / (B(1) + save_exp(-(va + B(54)) / B(-11)));
+      S q = (va + B(75)) / B(48);
+      r.b = (B(360) + (B(1010) + B(24) * (va + B(55))) * save_exp(-(q * q))) / qt;
+      break;
+    }
+    case G_KTST_M: {  // l5pc.py:444-451
+      S va = v + B(10);
+      r.a = B(1) / (B(1) + save_exp(-(va + B(0)) / B(19)));
+      S q = (va + B(71)) / B(59);
+      r.b = (B(0.34) + B(0.92) * save_exp(-(q * q))) / qt;
+      break;
+    }
+    case G_KTST_H: {  // l5pc.py:453-460
+      S va = v + B(10);
+      r.a = B(1) / (B(1) + save_exp(-(va + B(66)) / B(-10)));
+      S q = (va + B(73)) / B(23);
+      r.b = (B(8) + B(49) * save_exp(-(q * q))) / qt;
+      break;
+    }
+    case G_SKV31_M:  // l5pc.py:585-590
+      r.a = B(1) / (B(1) + save_exp((v - B(18.7)) / B(-9.7)));
+      r.b = B(0.2) * B(20.0) / (B(1) + save_exp((v + B(46.56)) / B(-44.14)));
+      break;
+    case G_M_M: {  // l5pc.py:653-661
+      S ma = B(3.3e-3) * save_exp(B(2.5) * B(0.04) * (v + B(35)));
+      S mb = B(3.3e-3) * save_exp(B(-2.5) * B(0.04) * (v + B(35)));
+      r.a = ma / (ma + mb);
+      r.b = (B(1) / (ma + mb)) / qt;
+      break;
+    }
+    case G_CAHVA_M:  // l5pc.py:723-727
+      r.a = (B(0.055) * (B(-27) - v + B(1e-6))) / (save_exp((B(-27.0) - v + B(1e-6)) / B(3.8)) - B(1.0));
+      r.b = B(0.94) * save_exp((B(-75.0) - v + B(1e-6)) / B(17.0));
+      break;
+    case G_CAHVA_H:  // l5pc.py:729-734
+      r.a = B(0.000457) * save_exp((B(-13.0) - v) / B(50.0));
+      r.b = B(0.0065) / (save_exp((-v - B(15.0)) / B(28.0)) + B(1.0));
+      break;
+    case G_CALVA_M: {  // l5pc.py:795-802
+      S vs = v + B(10);
+      r.a = B(1.0) / (B(1) + save_exp((vs + B(30)) / B(-6)));
+      r.b = (B(5.0) + B(20.0) / (B(1) + save_exp((vs + B(25)) / B(5)))) / qt;
+      break;
+    }
+    case G_CALVA_H: {  // l5pc.py:804-811
+      S vs = v + B(10);
+      r.a = B(1.0) / (B(1) + save_exp((vs + B(80)) / B(6.4)));
+      r.b = (B(20.0) + B(50.0) / (B(1) + save_exp((vs + B(40)) / B(7)))) / qt;
+      break;
+    }
+    default: {  // G_H_M, l5pc.py:973-984
+      S ma = B(0.001) * B(6.43) * (v + B(154.9) + B(1e-6)) / (save_exp((v + B(154.9) + B(1e-6)) / B(11.9)) - B(1));
+      S mb = B(0.001) * B(193) * save_exp(v / B(33.1));
+      r.a = ma / (ma + mb);
+      r.b = B(1) / (ma + mb);
+      break;
+    }
+  }
+  return r;
+}
+
+// One exponential-Euler gate step. Returns x'; `e` receives d x'/d x.
+template <typename S, typename B>
+__device__ __forceinline__ S gate_step(int g, S v, B x, B dt, B* e_out) {
+  Pair<S> r = gate_rates<S>(g, v);
+  S xinf, e;
+  if (gate_is_alpha_beta(g)) {  // solver_gate.py:45-64
+    S tau = B(1) / (r.a + r.b);
+    xinf = r.a * tau;
+    e = save_exp(-dt / tau);
+  } else {  // solver_gate.py:67-87
+    S slope = B(-1.0) / r.b;
+    e = save_exp(slope * dt);
+    xinf = r.a;
+  }
+  if (e_out) *e_out = val(e);
+  return x * e + xinf * (B(1) - e);
+}
+
+// Steady state of a gate (`init_state` of the channel classes).
+template <typename B>
+__device__ __forceinline__ B gate_steady(int g, B v) {
+  Pair<B> r = gate_rates<B>(g, v);
+  if (gate_is_alpha_beta(g)) return r.a / (r.a + r.b);
+  return r.a;
+}
+
+// SKE2 z gate, a function of the calcium concentration (l5pc.py:519-530).
+template <typename S>
+__device__ __forceinline__ S ske2_zinf(S cai) {
+  typedef typename Base<S>::type B;
+  if (val(cai) < B(1e-7)) cai = cai + B(1e-7);
+  return B(1) / (B(1) + pw(B(0.00043) / cai, B(4.8)));
+}
+
+// Gate ids and exponents of the gated ohmic channels.
+struct GateLayout { int g0, g1, e0; };
+__device__ __forceinline__ GateLayout gate_layout(int type) {
+  switch (type) {
+    case CH_NATAT: return {G_NATAT_M, G_NATAT_H, 3};
+    case CH_NATS2T: return {G_NATS2T_M, G_NATS2T_H, 3};
+    case CH_NAPET2: return {G_NAP_M, G_NAP_H, 3};
+    case CH_KPST: return {G_KPST_M, G_KPST_H, 2};
+    case CH_KTST: return {G_KTST_M, G_KTST_H, 4};
+    case CH_CAHVA: return {G_CAHVA_M, G_CAHVA_H, 2};
+    case CH_CALVA: return {G_CALVA_M, G_CALVA_H, 2};
+    case CH_SKV3_1: return {G_SKV31_M, -1, 1};
+    case CH_M: return {G_M_M, -1, 1};
+    case CH_H: return {G_H_M, -1, 1};
+    default: return {-1, -1, 0};
+  }
+}
+
+template <typename B> __device__ __forceinline__ B ipow(B x, int n) {
+  B r = x;
+  for (int i = 1; i < n; ++i) r *= x;
+  return r;
+}
+
+}  // namespace jxb

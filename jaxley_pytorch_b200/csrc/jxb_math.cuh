@@ -1,0 +1,82 @@
+// Scalar helpers shared by the step kernels: float/double overloads and a
+// forward-mode dual number used by the adjoint to differentiate rate functions.
+#pragma once
+#include <cuda_runtime.h>
+#include <math.h>
+
+namespace jxb {
+
+__device__ __forceinline__ float ex(float x) { return expf(x); }
+__device__ __forceinline__ double ex(double x) { return exp(x); }
+__device__ __forceinline__ float exm1(float x) { return expm1f(x); }
+__device__ __forceinline__ double exm1(double x) { return expm1(x); }
+__device__ __forceinline__ float lg(float x) { return logf(x); }
+__device__ __forceinline__ double lg(double x) { return log(x); }
+__device__ __forceinline__ float pw(float x, float y) { return powf(x, y); }
+__device__ __forceinline__ double pw(double x, double y) { return pow(x, y); }
+__device__ __forceinline__ float fab(float x) { return fabsf(x); }
+__device__ __forceinline__ double fab(double x) { return fabs(x); }
+
+// Dual number a + b*eps (eps^2 = 0): `d` carries the derivative with respect to
+// one seeded input.
+template <typename T>
+struct Dual {
+  T v, d;
+  __device__ __forceinline__ Dual() {}
+  __device__ __forceinline__ Dual(T a) : v(a), d(T(0)) {}
+  __device__ __forceinline__ Dual(T a, T b) : v(a), d(b) {}
+};
+template <typename T> __device__ __forceinline__ Dual<T> operator+(Dual<T> a, Dual<T> b) { return Dual<T>(a.v + b.v, a.d + b.d); }
+template <typename T> __device__ __forceinline__ Dual<T> operator-(Dual<T> a, Dual<T> b) { return Dual<T>(a.v - b.v, a.d - b.d); }
+template <typename T> __device__ __forceinline__ Dual<T> operator-(Dual<T> a) { return Dual<T>(-a.v, -a.d); }
+template <typename T> __device__ __forceinline__ Dual<T> operator*(Dual<T> a, Dual<T> b) { return Dual<T>(a.v * b.v, a.d * b.v + a.v * b.d); }
+template <typename T> __device__ __forceinline__ Dual<T> operator/(Dual<T> a, Dual<T> b) {
+  T q = a.v / b.v;
+  return Dual<T>(q, (a.d - q * b.d) / b.v);
+}
+template <typename T> __device__ __forceinline__ Dual<T> operator+(Dual<T> a, T b) { return Dual<T>(a.v + b, a.d); }
+template <typename T> __device__ __forceinline__ Dual<T> operator+(T a, Dual<T> b) { return Dual<T>(a + b.v, b.d); }
+template <typename T> __device__ __forceinline__ Dual<T> operator-(Dual<T> a, T b) { return Dual<T>(a.v - b, a.d); }
+template <typename T> __device__ __forceinline__ Dual<T> operator-(T a, Dual<T> b) { return Dual<T>(a - b.v, -b.d); }
+template <typename T> __device__ __forceinline__ Dual<T> operator*(Dual<T> a, T b) { return Dual<T>(a.v * b, a.d * b); }
+template <typename T> __device__ __forceinline__ Dual<T> operator*(T a, Dual<T> b) { return Dual<T>(a * b.v, a * b.d); }
+template <typename T> __device__ __forceinline__ Dual<T> operator/(Dual<T> a, T b) { return Dual<T>(a.v / b, a.d / b); }
+template <typename T> __device__ __forceinline__ Dual<T> operator/(T a, Dual<T> b) {
+  T q = a / b.v;
+  return Dual<T>(q, -q * b.d / b.v);
+}
+template <typename T> __device__ __forceinline__ Dual<T> ex(Dual<T> a) { T e = ex(a.v); return Dual<T>(e, e * a.d); }
+template <typename T> __device__ __forceinline__ Dual<T> exm1(Dual<T> a) { return Dual<T>(exm1(a.v), ex(a.v) * a.d); }
+template <typename T> __device__ __forceinline__ Dual<T> lg(Dual<T> a) { return Dual<T>(lg(a.v), a.d / a.v); }
+template <typename T> __device__ __forceinline__ Dual<T> pw(Dual<T> a, T y) {
+  T p = pw(a.v, y);
+  return Dual<T>(p, y * pw(a.v, y - T(1)) * a.d);
+}
+template <typename T> __device__ __forceinline__ Dual<T> fab(Dual<T> a) { return a.v < T(0) ? -a : a; }
+
+template <typename T> __device__ __forceinline__ T val(T a) { return a; }
+template <typename T> __device__ __forceinline__ T val(Dual<T> a) { return a.v; }
+
+template <typename S> struct Base { typedef S type; };
+template <typename T> struct Base<Dual<T>> { typedef T type; };
+
+// `min(x, 20)` keeping NaN (torch.clamp semantics); the derivative is zero on the
+// clamped side.
+template <typename T> __device__ __forceinline__ T clamp20(T x) { return x > T(20) ? T(20) : x; }
+template <typename T> __device__ __forceinline__ Dual<T> clamp20(Dual<T> x) {
+  return x.v > T(20) ? Dual<T>(T(20), T(0)) : x;
+}
+
+// solver_gate.py:8-11
+template <typename S> __device__ __forceinline__ S save_exp(S x) { return ex(clamp20(x)); }
+
+// solver_gate.py:14-30: x / (exp(x/y) - 1), series y*(1 - z/2 + z^2/12) for |z| < 1e-4.
+template <typename S, typename T> __device__ __forceinline__ S x_over_expm1(S x, T y) {
+  typedef typename Base<S>::type B;
+  S z = clamp20(x / y);
+  bool small = fab(val(z)) < B(1e-4);
+  if (small) return y * (B(1) - z / B(2) + z * z / B(12));
+  return x / exm1(z);
+}
+
+}  // namespace jxb

@@ -90,6 +90,8 @@ class Problem:
     def gsum(self):
         """Sum of the axial conductances of the edges that sink into every node."""
         ax = np.asarray(self.axial, dtype=np.float64)
+        if ax.shape[-1] == 0:
+            return np.zeros(ax.shape[:-1] + (self.n_nodes,))
         rows = ax.reshape(-1, ax.shape[-1])
         out = np.zeros((rows.shape[0], self.n_nodes))
         for b in range(rows.shape[0]):
@@ -291,3 +293,90 @@ def _synapse_from_plan(sp, gp, states) -> SynapseType:
         state=state,
         current=current,
     )
+
+
+# --------------------------------------------------------------------------------------
+# Serialization (npz, no pickle): fixtures travel to machines without the reference.
+# --------------------------------------------------------------------------------------
+def save_problem(problem: Problem, path: str, **extra) -> None:
+    import json
+
+    arrays = {
+        "comp_inds": problem.comp_inds, "sinks": problem.sinks, "axial": problem.axial,
+        "parent_lookup": problem.parent_lookup, "to_solve": problem.to_solve,
+        "map_lower": problem.map_lower, "map_upper": problem.map_upper,
+        "stim_inds": problem.stim_inds,
+    }
+    if problem.stim is not None:
+        arrays["stim"] = problem.stim
+    meta = {
+        "n_nodes": problem.n_nodes, "dt": problem.dt, "n_steps": problem.n_steps,
+        "batch": problem.batch, "current_names": problem.current_names,
+        "recordings": [[n, int(i)] for n, i in problem.recordings],
+        "params": list(problem.params), "states": list(problem.states),
+        "channels": [], "synapses": [],
+    }
+    for k, v in problem.params.items():
+        arrays[f"param/{k}"] = v
+    for k, v in problem.states.items():
+        arrays[f"state/{k}"] = v
+    for q, ch in enumerate(problem.channels):
+        meta["channels"].append({"type": ch.type_name, "name": ch.name, "params": ch.params,
+                                 "states": ch.states, "current": ch.current,
+                                 "constants": list(ch.constants)})
+        arrays[f"channel/{q}"] = np.asarray(ch.inds)
+    for q, syn in enumerate(problem.synapses):
+        meta["synapses"].append({"model": syn.model, "name": syn.name, "k": syn.k,
+                                 "param_names": syn.param_names,
+                                 "has_state": syn.state is not None,
+                                 "has_current": syn.current is not None})
+        arrays[f"syn/{q}/pre"] = syn.pre
+        arrays[f"syn/{q}/post"] = syn.post
+        arrays[f"syn/{q}/targets"] = syn.targets
+        arrays[f"syn/{q}/params"] = np.stack(syn.params)
+        if syn.state is not None:
+            arrays[f"syn/{q}/state"] = syn.state
+        if syn.current is not None:
+            arrays[f"syn/{q}/current"] = syn.current
+    for k, v in extra.items():
+        arrays[f"extra/{k}"] = np.asarray(v)
+    arrays["meta"] = np.frombuffer(json.dumps(meta).encode(), dtype=np.uint8)
+    np.savez_compressed(path, **arrays)
+
+
+def load_problem(path: str):
+    """Returns `(problem, extra)` where `extra` holds the additional arrays."""
+    import json
+
+    from .channels import ChannelInstance
+
+    z = np.load(path, allow_pickle=False)
+    meta = json.loads(bytes(z["meta"]).decode())
+    channels = [
+        ChannelInstance(type_name=c["type"], name=c["name"], inds=z[f"channel/{q}"],
+                        params=c["params"], states=c["states"], current=c["current"],
+                        constants=c["constants"])
+        for q, c in enumerate(meta["channels"])
+    ]
+    synapses = []
+    for q, s in enumerate(meta["synapses"]):
+        synapses.append(SynapseType(
+            model=s["model"], name=s["name"], pre=z[f"syn/{q}/pre"], post=z[f"syn/{q}/post"],
+            k=s["k"], targets=z[f"syn/{q}/targets"], params=list(z[f"syn/{q}/params"]),
+            param_names=s["param_names"],
+            state=z[f"syn/{q}/state"] if s["has_state"] else None,
+            current=z[f"syn/{q}/current"] if s["has_current"] else None,
+        ))
+    prob = Problem(
+        n_nodes=meta["n_nodes"], comp_inds=z["comp_inds"], sinks=z["sinks"], axial=z["axial"],
+        parent_lookup=z["parent_lookup"], to_solve=z["to_solve"], map_lower=z["map_lower"],
+        map_upper=z["map_upper"], channels=channels,
+        params={k: z[f"param/{k}"] for k in meta["params"]},
+        states={k: z[f"state/{k}"] for k in meta["states"]},
+        dt=meta["dt"], n_steps=meta["n_steps"], stim_inds=z["stim_inds"],
+        stim=z["stim"] if "stim" in z else None,
+        recordings=[(n, i) for n, i in meta["recordings"]], synapses=synapses,
+        batch=meta["batch"], current_names=meta["current_names"],
+    )
+    extra = {k[len("extra/"):]: z[k] for k in z.files if k.startswith("extra/")}
+    return prob, extra

@@ -1,0 +1,61 @@
+"""Host-side lowering: the chain schedule replayed on the CPU must solve the same
+system as the oracle, and the library must export the C ABI."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import oracle
+from conftest import REPO, fixture_names, load_fixture
+from jaxley_pytorch_b200.lower import chain_order, emulate_block_solve, lower
+
+
+@pytest.mark.parametrize("name", fixture_names())
+@pytest.mark.parametrize("max_block", [4096, 16])
+def test_chain_schedule_solves_the_tree(name, max_block):
+    prob, _ = load_fixture(name)
+    low = lower(prob, max_block_nodes=max_block)
+    n = prob.n_nodes
+    parent, gl, gu = prob.solve_order_system()
+    rng = np.random.default_rng(1)
+    B, dt = 3, 0.025
+    d = rng.uniform(1, 3, (B, n))
+    s = rng.normal(size=(B, n))
+    ref = oracle.tree_solve(d, -dt * gl * np.ones((B, 1)), -dt * gu * np.ones((B, 1)), s, parent)
+    solve_of_node = np.empty(n, np.int64)
+    solve_of_node[prob.to_solve] = np.arange(n)
+    int2solve = solve_of_node[low.int2node]
+    got = emulate_block_solve(low, d[:, int2solve], s[:, int2solve], -dt * low.a_low, -dt * low.a_up)
+    np.testing.assert_allclose(got, ref[:, int2solve], rtol=1e-12, atol=1e-12)
+
+
+def test_chain_order_properties():
+    rng = np.random.default_rng(2)
+    parent = [-1] + [int(rng.integers(0, j)) for j in range(1, 200)]
+    parent += [-1] + [200 + int(rng.integers(0, j)) for j in range(1, 50)]
+    order, trees, chains = chain_order(np.asarray(parent))
+    assert sorted(order.tolist()) == list(range(250))
+    assert trees.tolist() == [0, 200, 250]
+    pos = np.empty(250, np.int64)
+    pos[order] = np.arange(250)
+    for top, ln, ptop, kids in chains:
+        for j in range(top + 1, top + ln):
+            assert parent[order[j]] == order[j - 1]
+        if ptop >= 0:
+            assert parent[order[top]] == order[ptop]
+            assert ptop < top
+
+
+def test_library_exports_every_declared_symbol():
+    from jaxley_pytorch_b200 import _lib
+
+    header = open(os.path.join(REPO, "include", "jxb.h")).read()
+    declared = set(re.findall(r"^\s*(?:int|int64_t|const char\*)\s+(jxb_\w+)\s*\(", header, re.M))
+    assert declared == set(_lib.EXPORTED)
+    if not os.path.exists(_lib.LIB_PATH):
+        pytest.skip("libjxb is not built")
+    lib = ctypes.CDLL(_lib.LIB_PATH)
+    for name in declared:
+        assert hasattr(lib, name), name
