@@ -119,12 +119,15 @@ typedef struct {
   int32_t n_items, n_steps;   /* steps in this launch */
   int32_t t0;                 /* absolute index of the first step */
   int32_t max_rows;           /* rows per item (shared-memory sizing) */
-  int32_t max_nodes, max_slots;
+  int32_t max_nodes, max_slots;   /* largest block: nodes, state slots */
+  int32_t max_chains, max_child;  /* largest block: chains, child-chain links */
+  int32_t max_levels, max_pslots; /* largest block: chain levels, parameter slots */
+  int32_t threads, pad3;          /* threads per CTA (0 = default) */
   double dt;
   /* topology, internal (chain) node order */
   const int32_t* node_class;  /* (n_nodes,) */
   const int32_t* soff;        /* (n_nodes+1,) state-slot offsets */
-  const int32_t* poff;        /* (n_nodes+1,) parameter-slot offsets */
+  const int32_t* poff;        /* (n_nodes,) first parameter slot (runs may be shared) */
   const void* a_low;          /* (n_nodes,) axial conductance row i -> parent */
   const void* a_up;           /* (n_nodes,) axial conductance parent row -> i */
   const void* gsum;           /* (n_nodes,) sum of axial conductances sinking into i */
@@ -144,6 +147,9 @@ typedef struct {
   const int32_t* chain_cptr;
   const int32_t* chain_child; /* internal node index of child-chain tops */
   const int32_t* level_ptr;   /* chain offsets relative to the block's chain0 */
+  const int32_t* parent;      /* (n_nodes,) parent (internal order) or -1 */
+  const int32_t* kid_ptr;     /* (n_nodes+1,) children CSR */
+  const int32_t* kid;         /* children (internal order) */
   /* stimulus: i_ext[node] += stim[t][b][idx] / area[node] * 1e5 */
   const int32_t* stim_ptr;    /* (n_nodes+1,) CSR over nodes */
   const int32_t* stim_idx;
@@ -167,7 +173,7 @@ typedef struct {
   /* adjoint */
   void* adj;                  /* (batch, n_slots) adjoint of the state, updated in place */
   const void* rec_grad;       /* (T + 1, batch, n_rec) gradient of the recordings */
-  void* pgrad;                /* (batch, n_pslots) float64, accumulated */
+  double* pgrad;              /* (batch, n_cols) float64, accumulated: d loss / d pscale */
   int32_t mode, pad2;         /* 0 = step, 1 = initial currents only */
 } JxbSimArgs;
 

@@ -45,6 +45,9 @@ class JxbSimArgs(C.Structure):
         ("n_items", C.c_int32), ("n_steps", C.c_int32),
         ("t0", C.c_int32), ("max_rows", C.c_int32),
         ("max_nodes", C.c_int32), ("max_slots", C.c_int32),
+        ("max_chains", C.c_int32), ("max_child", C.c_int32),
+        ("max_levels", C.c_int32), ("max_pslots", C.c_int32),
+        ("threads", C.c_int32), ("pad3", C.c_int32),
         ("dt", C.c_double),
         ("node_class", _p), ("soff", _p), ("poff", _p),
         ("a_low", _p), ("a_up", _p), ("gsum", _p), ("cm", _p),
@@ -54,6 +57,7 @@ class JxbSimArgs(C.Structure):
         ("blocks", _p), ("items", _p),
         ("chain_top", _p), ("chain_len", _p), ("chain_ptop", _p), ("chain_cptr", _p),
         ("chain_child", _p), ("level_ptr", _p),
+        ("parent", _p), ("kid_ptr", _p), ("kid", _p),
         ("stim_ptr", _p), ("stim_idx", _p), ("area", _p), ("stim", _p),
         ("n_stim", C.c_int32), ("stim_steps", C.c_int32), ("stim_rows", C.c_int32), ("pad0", C.c_int32),
         ("syn_lin", _p), ("syn_const", _p),

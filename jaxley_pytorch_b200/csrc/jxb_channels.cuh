@@ -162,22 +162,28 @@ __device__ __forceinline__ Pair<S> gate_rates(int g, S v) {
   return r;
 }
 
+// exp(min(arg, 20)) - 1, the decay factor of exponential Euler minus one.
+template <typename S> __device__ __forceinline__ S save_expm1(S x) { return exm1(clamp20(x)); }
+
 // One exponential-Euler gate step. Returns x'; `e` receives d x'/d x.
+// x * e + x_inf * (1 - e) (solver_gate.py:56-64) is evaluated as
+// x + (x - x_inf) * (e - 1) with e - 1 from expm1: the same value, without the
+// cancellation of 1 - e for slow gates in float32.
 template <typename S, typename B>
 __device__ __forceinline__ S gate_step(int g, S v, B x, B dt, B* e_out) {
   Pair<S> r = gate_rates<S>(g, v);
-  S xinf, e;
+  S xinf, em1;
   if (gate_is_alpha_beta(g)) {  // solver_gate.py:45-64
     S tau = B(1) / (r.a + r.b);
     xinf = r.a * tau;
-    e = save_exp(-dt / tau);
+    em1 = save_expm1(-dt / tau);
   } else {  // solver_gate.py:67-87
     S slope = B(-1.0) / r.b;
-    e = save_exp(slope * dt);
+    em1 = save_expm1(slope * dt);
     xinf = r.a;
   }
-  if (e_out) *e_out = val(e);
-  return x * e + xinf * (B(1) - e);
+  if (e_out) *e_out = B(1) + val(em1);
+  return x + (x - xinf) * em1;
 }
 
 // Steady state of a gate (`init_state` of the channel classes).

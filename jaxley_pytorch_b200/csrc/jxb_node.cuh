@@ -5,13 +5,12 @@
 
 namespace jxb {
 
-// Parameter accessor of one node and batch row: value = base * scale[col].
+// Parameter values of one channel entry of one node and batch row (staged in shared
+// memory as base * scale[col] when the launch starts).
 template <typename T>
 struct Prm {
-  const T* base;
-  const int* col;
-  const T* scale;
-  __device__ __forceinline__ T operator()(int k) const { return base[k] * scale[col[k]]; }
+  const T* val;
+  __device__ __forceinline__ T operator()(int k) const { return val[k]; }
 };
 
 // `update_states` of one channel entry, in place on the node's state block `x`
@@ -29,8 +28,9 @@ __device__ __forceinline__ void channel_update(const ChanEntry& e, T* x, const P
       break;
     case CH_SKE2: {  // l5pc.py:488-500, tau_z = 1
       T zinf = ske2_zinf<T>(x[e.s[1]]);
-      T ez = save_exp(T(-1.0) / T(1.0) * dt);
-      x[e.s[0]] = x[e.s[0]] * ez + zinf * (T(1) - ez);
+      T em1 = save_expm1(T(-1.0) / T(1.0) * dt);
+      T z = x[e.s[0]];
+      x[e.s[0]] = z + (z - zinf) * em1;
       break;
     }
     case CH_CAPUMP: {  // l5pc.py:842-861
@@ -39,8 +39,8 @@ __device__ __forceinline__ void channel_update(const ChanEntry& e, T* x, const P
       T gamma = P(0), decay = P(1), depth = P(2), minCai = P(3);
       T drive = T(-10000.0) * ica * gamma / (T(2) * T(96485) * depth);
       T cai_inf = minCai + decay * drive;
-      T ee = save_exp(-dt / decay);
-      x[e.s[0]] = cai * ee + cai_inf * (T(1) - ee);
+      T em1 = save_expm1(-dt / decay);
+      x[e.s[0]] = cai + (cai - cai_inf) * em1;
       break;
     }
     case CH_CANERNST: {  // l5pc.py:891-902; constants F, T, R
@@ -138,7 +138,215 @@ __device__ __forceinline__ void channel_current(const ChanEntry& e, T* x, const 
       break;
     }
   }
-  x[e.cur] += cur;
+  if (e.cur >= 0) x[e.cur] += cur;
+}
+
+}  // namespace jxb
+
+namespace jxb {
+
+// ---------------------------------------------------------------------------------
+// Adjoint (vector-Jacobian products) of one node's channel step.
+//
+// `lam` is the node's adjoint block (same slot layout as the state); `lv` collects
+// the adjoint of the node voltage before the step. Parameter adjoints go through
+// `PGrad::add(k, value)` with `k` relative to the entry's first parameter.
+// ---------------------------------------------------------------------------------
+
+template <typename T>
+struct PGradSink {
+  // Accumulates d loss / d parameter value times the parameter base, i.e. the
+  // gradient of the column scale, in float64; column 0 (fixed parameters) is skipped.
+  const T* base;
+  const int* col;
+  double* acc;  // per-column accumulator of this row (shared memory)
+  __device__ __forceinline__ void add(int k, T g) const {
+    int c = col[k];
+    if (c != 0) atomicAdd(acc + c, (double)(g * base[k]));
+  }
+};
+
+// VJP of `channel_current` at the post-update state `x` and voltage `v`.
+// The node's summed slope s and g*E term q enter the solve as
+// d += dt * 1000 * s / cm and rhs += dt * 1000 * q / cm, so with
+// lr = 1000 * dt * lambda_r / cm and the new voltage x1 their adjoints are
+// -lr * x1 and lr; a conductance c with reversal E gets lr * (E - x1).
+template <typename T>
+__device__ __forceinline__ void channel_current_vjp(const ChanEntry& e, const T* x, T* lam,
+                                                    const Prm<T>& P, const PGradSink<T>& G, T v,
+                                                    T lr, T x1, T& lv) {
+  const T lI = e.cur >= 0 ? lam[e.cur] : T(0);
+  auto ohmic = [&](T c, T E, T& lc, T& lE) {
+    lc = lr * (E - x1) + (v - E) * lI;
+    lE = c * (lr - lI);
+    lv += c * lI;
+  };
+  switch (e.type) {
+    case CH_HH: {
+      T m = x[e.s[0]], h = x[e.s[1]], n = x[e.s[2]];
+      T G1 = (m * m * m) * h, G2 = (n * n * n * n);
+      T gNa = P(0), gK = P(1), gL = P(2);
+      T lc1, lE1, lc2, lE2, lc3, lE3;
+      ohmic(gNa * G1, P(3), lc1, lE1);
+      ohmic(gK * G2, P(4), lc2, lE2);
+      ohmic(gL, P(5), lc3, lE3);
+      lam[e.s[0]] += gNa * T(3) * m * m * h * lc1;
+      lam[e.s[1]] += gNa * m * m * m * lc1;
+      lam[e.s[2]] += gK * T(4) * n * n * n * lc2;
+      G.add(0, G1 * lc1);
+      G.add(1, G2 * lc2);
+      G.add(2, lc3);
+      G.add(3, lE1);
+      G.add(4, lE2);
+      G.add(5, lE3);
+      break;
+    }
+    case CH_LEAK: {
+      T lc, lE;
+      ohmic(P(0), P(1), lc, lE);
+      G.add(0, lc);
+      G.add(1, lE);
+      break;
+    }
+    case CH_SKE2: {
+      T g = P(0), z = x[e.s[0]];
+      T lc, lE;
+      ohmic(g * z, P(1), lc, lE);
+      lam[e.s[0]] += g * lc;
+      G.add(0, z * lc);
+      G.add(1, lE);
+      break;
+    }
+    case CH_CAPUMP:
+    case CH_CANERNST:
+      break;
+    default: {
+      GateLayout gl = gate_layout(e.type);
+      bool ca = e.type == CH_CAHVA || e.type == CH_CALVA;
+      T g = P(0);
+      T m = x[e.s[0]];
+      T h = gl.g1 >= 0 ? x[e.s[1]] : T(1);
+      T mp = ipow(m, gl.e0);
+      T Gv = mp * h;
+      T E = ca ? x[e.s[2]] : P(1);
+      T lc, lE;
+      ohmic(g * Gv, E, lc, lE);
+      T dm = gl.e0 == 1 ? T(1) : T(gl.e0) * ipow(m, gl.e0 - 1);
+      lam[e.s[0]] += g * dm * h * lc;
+      if (gl.g1 >= 0) lam[e.s[1]] += g * mp * lc;
+      G.add(0, Gv * lc);
+      if (ca)
+        lam[e.s[2]] += lE;
+      else
+        G.add(1, lE);
+      break;
+    }
+  }
+}
+
+// d x'/d x and d x'/d v of one gate step at voltage v.
+template <typename T>
+__device__ __forceinline__ void gate_vjp(int g, T v, T x, T dt, T lx_new, T& lx_old, T& lv) {
+  T e;
+  Dual<T> xn = gate_step<Dual<T>, T>(g, Dual<T>(v, T(1)), x, dt, &e);
+  lx_old = e * lx_new;
+  lv += xn.d * lx_new;
+}
+
+// VJP of `channel_update` at the pre-update state `x` (the values this entry read).
+// On entry lam holds the adjoint of the slots after the update; on return the adjoint
+// of the slots before it.
+template <typename T>
+__device__ __forceinline__ void channel_update_vjp(const ChanEntry& e, const T* x, T* lam,
+                                                   const Prm<T>& P, const PGradSink<T>& G, T v,
+                                                   T dt, T& lv) {
+  switch (e.type) {
+    case CH_HH: {
+      T lo;
+      gate_vjp<T>(G_HH_M, v, x[e.s[0]], dt, lam[e.s[0]], lo, lv);
+      lam[e.s[0]] = lo;
+      gate_vjp<T>(G_HH_H, v, x[e.s[1]], dt, lam[e.s[1]], lo, lv);
+      lam[e.s[1]] = lo;
+      gate_vjp<T>(G_HH_N, v, x[e.s[2]], dt, lam[e.s[2]], lo, lv);
+      lam[e.s[2]] = lo;
+      break;
+    }
+    case CH_LEAK:
+      break;
+    case CH_SKE2: {
+      T ez = T(1) + save_expm1(T(-1.0) / T(1.0) * dt);
+      T lz = lam[e.s[0]];
+      Dual<T> zi = ske2_zinf<Dual<T>>(Dual<T>(x[e.s[1]], T(1)));
+      lam[e.s[0]] = ez * lz;
+      lam[e.s[1]] += (T(1) - ez) * zi.d * lz;
+      break;
+    }
+    case CH_CAPUMP: {
+      T ica = x[e.cur];
+      T cai = x[e.s[0]];
+      T gamma = P(0), decay = P(1), depth = P(2), minCai = P(3);
+      const T F2 = T(2) * T(96485);
+      T drive = T(-10000.0) * ica * gamma / (F2 * depth);
+      T cai_inf = minCai + decay * drive;
+      T arg = -dt / decay;
+      T em1 = save_expm1(arg);
+      T ee = T(1) + em1;
+      T lnew = lam[e.s[0]];
+      T l_inf = -em1 * lnew;
+      T l_ee = (cai - cai_inf) * lnew;
+      T l_drive = decay * l_inf;
+      lam[e.s[0]] = ee * lnew;
+      if (e.cur >= 0) lam[e.cur] += T(-10000.0) * gamma / (F2 * depth) * l_drive;
+      T l_decay = drive * l_inf + (arg > T(20) ? T(0) : l_ee * ee * dt / (decay * decay));
+      G.add(0, T(-10000.0) * ica / (F2 * depth) * l_drive);
+      G.add(1, l_decay);
+      G.add(2, -drive / depth * l_drive);
+      G.add(3, l_inf);
+      break;
+    }
+    case CH_CANERNST: {
+      T F = P(0), Tk = P(1), R = P(2);
+      T C = R * Tk / (T(2) * F) * T(1000);
+      T le = lam[e.s[0]];
+      lam[e.s[0]] = T(0);
+      lam[e.s[1]] += -C / x[e.s[1]] * le;
+      lam[e.s[2]] += C / x[e.s[2]] * le;
+      break;
+    }
+    default: {
+      GateLayout gl = gate_layout(e.type);
+      T lo;
+      gate_vjp<T>(gl.g0, v, x[e.s[0]], dt, lam[e.s[0]], lo, lv);
+      lam[e.s[0]] = lo;
+      if (gl.g1 >= 0) {
+        gate_vjp<T>(gl.g1, v, x[e.s[1]], dt, lam[e.s[1]], lo, lv);
+        lam[e.s[1]] = lo;
+      }
+      break;
+    }
+  }
+}
+
+// Slots written by `channel_update` of an entry, for the undo log of the adjoint.
+__device__ __forceinline__ int update_writes(const ChanEntry& e, short* out) {
+  switch (e.type) {
+    case CH_HH:
+      out[0] = e.s[0]; out[1] = e.s[1]; out[2] = e.s[2];
+      return 3;
+    case CH_LEAK:
+      return 0;
+    case CH_SKE2:
+    case CH_CAPUMP:
+    case CH_CANERNST:
+      out[0] = e.s[0];
+      return 1;
+    default: {
+      GateLayout gl = gate_layout(e.type);
+      out[0] = e.s[0];
+      if (gl.g1 >= 0) { out[1] = e.s[1]; return 2; }
+      return 1;
+    }
+  }
 }
 
 }  // namespace jxb

@@ -1,17 +1,21 @@
-// Fused bwd_euler + DHS simulation kernels.
+// Fused bwd_euler + DHS simulation kernels (forward and adjoint).
 //
 // One CTA owns one work item: a block of whole trees (cells) and a few batch rows.
-// The rows' state vectors live in shared memory for the whole segment of steps; the
-// per-step work is
+// Everything the step reads repeatedly is staged in shared memory when the launch
+// starts: the block's node metadata, its chain schedule, the off-diagonal entries of
+// the tree system, the channel programs, the rows' parameter values and the rows'
+// state vectors, which stay resident for the whole segment of steps. Per step:
 //   1. channels, node-parallel: gate updates in insertion order, linearised currents
 //      (modules/base.py:3402-3542), stimulus (:3234-3242), assembly of the diagonal
 //      and right-hand side of the implicit system (solver_voltage.py:250-291);
 //   2. the Hines solve of every tree (solver_voltage.py:78-108), organised by chains
 //      (a node and its only child share a chain): one thread eliminates a whole
-//      chain bottom-up in registers, chains of one level run in parallel and levels
-//      are separated by a barrier; back-substitution runs the levels top-down.
-// Recordings, checkpoints and the trajectory for the adjoint are written from the
-// resident state.
+//      chain bottom-up in registers, the chains of one level run in parallel and
+//      levels are separated by a barrier; back-substitution runs the levels top-down.
+// The adjoint kernel recomputes a segment from its checkpoint (storing the state
+// before every step), then runs the steps in reverse: the transposed tree solve
+// (the same chain schedule with the off-diagonals swapped, solver_voltage.py:143-187)
+// and the vector-Jacobian products of the channel step, node by node.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -28,119 +32,202 @@ void set_err(const char* what, cudaError_t e) {
   snprintf(g_err, sizeof(g_err), "%s: %s", what, e == cudaSuccess ? "ok" : cudaGetErrorString(e));
 }
 
+constexpr int kMaxWrites = 24;  // undo-log entries of one node's channel updates
+constexpr int FLAG_COMP = 1, FLAG_STIM = 2, FLAG_REC = 4;
+
 template <typename T>
 struct SimSmem {
-  T* st;    // rows * n_slots
-  T* D;     // rows * n_nodes
-  T* S;     // rows * n_nodes
-  T* al;    // n_nodes: -dt * a_low
-  T* au;    // n_nodes: -dt * a_up
-  T* dg;    // n_nodes: is_comp + dt * gsum
-  T* cm;    // n_nodes
-  T* adj;   // rows * n_slots (adjoint only)
-  T* X1;    // rows * n_nodes (adjoint only)
+  // per block
+  T *al, *au, *dg, *cm;      // n_nodes
+  int* soff;                 // n_nodes, relative to the block's first slot
+  short *cls, *poff;         // n_nodes (poff relative to the block's first parameter slot)
+  unsigned char* flags;      // n_nodes
+  short *ctop, *clen, *cptop;  // n_chains (node indices relative to the block)
+  int* ccp;                  // n_chains + 1 (relative)
+  short* cchild;             // n_child
+  int* lp;                   // n_levels + 1
+  short *par, *kptr, *kids;  // parent, children CSR (block-relative)
   ChanEntry* ents;
+  int* cptr;                 // n_classes + 1 (entries of every node class)
+  T* pb;                     // n_pslots (parameter bases)
+  int* pc;                   // n_pslots (parameter columns)
+  // per row
+  T *st, *D, *S, *pv;        // rows * (n_slots | n_nodes | n_nodes | n_pslots)
+  T* V;                      // rows * n_nodes: voltages during the segment
+  // adjoint
+  T *adj, *X1;               // rows * n_slots, rows * n_nodes
+  double* pg;                // rows * n_cols
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
 template <typename T>
-__host__ __device__ inline size_t sim_smem_layout(const JxbSimArgs& a, bool backward, SimSmem<T>* out,
+__host__ __device__ inline size_t sim_smem_layout(const JxbSimArgs& a, bool backward, SimSmem<T>* o,
                                                   char* base) {
-  size_t rows = a.max_rows, nn = a.max_nodes, ns = a.max_slots;
+  const size_t R = a.max_rows, nn = a.max_nodes, ns = a.max_slots, nc = a.max_chains,
+               nk = a.max_child, nl = a.max_levels, np = a.max_pslots, ne = a.n_entries,
+               ncol = a.n_cols;
   size_t off = 0;
   auto take = [&](size_t bytes) {
-    size_t o = off;
+    size_t r = off;
     off = align_up(off + bytes, 16);
-    return o;
+    return base ? (void*)(base + r) : nullptr;
   };
-  size_t o_st = take(sizeof(T) * rows * ns);
-  size_t o_D = take(sizeof(T) * rows * nn);
-  size_t o_S = take(sizeof(T) * rows * nn);
-  size_t o_al = take(sizeof(T) * nn);
-  size_t o_au = take(sizeof(T) * nn);
-  size_t o_dg = take(sizeof(T) * nn);
-  size_t o_cm = take(sizeof(T) * nn);
-  size_t o_adj = backward ? take(sizeof(T) * rows * ns) : 0;
-  size_t o_X1 = backward ? take(sizeof(T) * rows * nn) : 0;
-  size_t o_e = take(sizeof(ChanEntry) * (size_t)a.n_entries);
-  if (out) {
-    out->st = (T*)(base + o_st);
-    out->D = (T*)(base + o_D);
-    out->S = (T*)(base + o_S);
-    out->al = (T*)(base + o_al);
-    out->au = (T*)(base + o_au);
-    out->dg = (T*)(base + o_dg);
-    out->cm = (T*)(base + o_cm);
-    out->adj = backward ? (T*)(base + o_adj) : nullptr;
-    out->X1 = backward ? (T*)(base + o_X1) : nullptr;
-    out->ents = (ChanEntry*)(base + o_e);
-  }
+  SimSmem<T> s;
+  // 8-byte types first.
+  s.pg = backward ? (double*)take(sizeof(double) * R * ncol) : nullptr;
+  s.st = (T*)take(sizeof(T) * R * ns);
+  s.adj = backward ? (T*)take(sizeof(T) * R * ns) : nullptr;
+  s.D = (T*)take(sizeof(T) * R * nn);
+  s.S = (T*)take(sizeof(T) * R * nn);
+  s.V = (T*)take(sizeof(T) * R * nn);
+  s.X1 = backward ? (T*)take(sizeof(T) * R * nn) : nullptr;
+  s.pv = (T*)take(sizeof(T) * R * np);
+  s.al = (T*)take(sizeof(T) * nn);
+  s.au = (T*)take(sizeof(T) * nn);
+  s.dg = (T*)take(sizeof(T) * nn);
+  s.cm = (T*)take(sizeof(T) * nn);
+  s.pb = (T*)take(sizeof(T) * np);
+  s.soff = (int*)take(sizeof(int) * nn);
+  s.pc = (int*)take(sizeof(int) * np);
+  s.ccp = (int*)take(sizeof(int) * (nc + 1));
+  s.lp = (int*)take(sizeof(int) * (nl + 1));
+  s.ents = (ChanEntry*)take(sizeof(ChanEntry) * ne);
+  s.cptr = (int*)take(sizeof(int) * (a.n_classes + 1));
+  s.cls = (short*)take(sizeof(short) * nn);
+  s.poff = (short*)take(sizeof(short) * nn);
+  s.ctop = (short*)take(sizeof(short) * nc);
+  s.clen = (short*)take(sizeof(short) * nc);
+  s.cptop = (short*)take(sizeof(short) * nc);
+  s.cchild = (short*)take(sizeof(short) * (nk + 1));
+  s.par = (short*)take(sizeof(short) * nn);
+  s.kptr = (short*)take(sizeof(short) * (nn + 1));
+  s.kids = (short*)take(sizeof(short) * (nn + 1));
+  s.flags = (unsigned char*)take(nn);
+  if (o) *o = s;
   return off;
 }
 
-// Loads the block's shared topology and the rows' states into shared memory.
+// Stages the block's topology, the channel programs, the parameter values of the
+// item's rows and the rows' states (and adjoints) in shared memory.
 template <typename T>
-__device__ void load_item(const JxbSimArgs& a, const JxbBlock& blk, int row0, int rows,
-                          const SimSmem<T>& sm, T dt) {
+__device__ void stage_item(const JxbSimArgs& a, const JxbBlock& blk, int row0, int rows,
+                           const SimSmem<T>& sm, T dt, const T* state_src, const T* adj_src) {
   const int tid = threadIdx.x, NT = blockDim.x;
-  const int nn = blk.n_nodes, ns = blk.n_slots;
+  const int nn = blk.n_nodes, ns = blk.n_slots, node0 = blk.node0;
   const T* gl = (const T*)a.a_low;
   const T* gu = (const T*)a.a_up;
   const T* gs = (const T*)a.gsum;
   const T* cmv = (const T*)a.cm;
   for (int j = tid; j < nn; j += NT) {
-    int i = blk.node0 + j;
+    const int i = node0 + j;
+    const int cls = a.node_class[i];
+    const bool comp = a.cls_comp[cls] != 0;
     sm.al[j] = -(dt * gl[i]);
     sm.au[j] = -(dt * gu[i]);
-    T comp = a.cls_comp[a.node_class[i]] ? T(1) : T(0);
-    sm.dg[j] = comp + dt * gs[i];
+    sm.dg[j] = (comp ? T(1) : T(0)) + dt * gs[i];
     sm.cm[j] = cmv[i];
+    sm.soff[j] = a.soff[i] - blk.slot0;
+    sm.cls[j] = (short)cls;
+    sm.poff[j] = (short)(a.poff[i] - blk.pslot0);
+    unsigned char f = comp ? FLAG_COMP : 0;
+    if (a.stim_ptr[i + 1] > a.stim_ptr[i]) f |= FLAG_STIM;
+    if (a.n_rec > 0 && a.rec_ptr[i + 1] > a.rec_ptr[i]) f |= FLAG_REC;
+    sm.flags[j] = f;
+    const int pa = a.parent[i];
+    sm.par[j] = (short)(pa >= 0 ? pa - node0 : -1);
+    sm.kptr[j] = (short)(a.kid_ptr[i] - a.kid_ptr[node0]);
   }
+  if (tid == 0) sm.kptr[nn] = (short)(a.kid_ptr[node0 + nn] - a.kid_ptr[node0]);
+  {
+    const int kb = a.kid_ptr[node0], ke = a.kid_ptr[node0 + nn];
+    for (int q = tid; q < ke - kb; q += NT) sm.kids[q] = (short)(a.kid[kb + q] - node0);
+  }
+  const int nc = blk.n_chains, c0 = blk.chain0;
+  const int k0 = a.chain_cptr[c0];
+  for (int c = tid; c < nc; c += NT) {
+    sm.ctop[c] = (short)(a.chain_top[c0 + c] - node0);
+    sm.clen[c] = (short)a.chain_len[c0 + c];
+    int pt = a.chain_ptop[c0 + c];
+    sm.cptop[c] = (short)(pt >= 0 ? pt - node0 : -1);
+    sm.ccp[c] = a.chain_cptr[c0 + c] - k0;
+  }
+  if (tid == 0) sm.ccp[nc] = a.chain_cptr[c0 + nc] - k0;
+  const int nk = a.chain_cptr[c0 + nc] - k0;
+  for (int q = tid; q < nk; q += NT) sm.cchild[q] = (short)(a.chain_child[k0 + q] - node0);
+  for (int q = tid; q <= blk.n_levels; q += NT) sm.lp[q] = a.level_ptr[blk.level0 + q];
   const short* src = (const short*)a.entries;
   short* dst = (short*)sm.ents;
-  int nshort = a.n_entries * (int)(sizeof(ChanEntry) / sizeof(short));
+  const int nshort = a.n_entries * (int)(sizeof(ChanEntry) / sizeof(short));
   for (int q = tid; q < nshort; q += NT) dst[q] = src[q];
-  const T* state = (const T*)a.state;
+  for (int q = tid; q <= a.n_classes; q += NT) sm.cptr[q] = a.cls_ptr[q];
+  const int np = blk.n_pslots;
+  const T* pbase = (const T*)a.pbase;
+  const T* pscale = (const T*)a.pscale;
+  for (int q = tid; q < np; q += NT) {
+    sm.pb[q] = pbase[blk.pslot0 + q];
+    sm.pc[q] = a.pcol[blk.pslot0 + q];
+  }
+  for (int w = tid; w < rows * np; w += NT) {
+    const int r = w / np, q = w % np;
+    const int g = blk.pslot0 + q;
+    sm.pv[(size_t)r * np + q] = pbase[g] * pscale[(size_t)(row0 + r) * a.n_cols + a.pcol[g]];
+  }
   for (int r = 0; r < rows; ++r) {
-    const T* g = state + (size_t)(row0 + r) * a.n_slots + blk.slot0;
+    const T* g = state_src + (size_t)(row0 + r) * a.n_slots + blk.slot0;
     T* s = sm.st + (size_t)r * ns;
     for (int q = tid; q < ns; q += NT) s[q] = g[q];
+    if (adj_src) {
+      const T* ga = adj_src + (size_t)(row0 + r) * a.n_slots + blk.slot0;
+      T* sa = sm.adj + (size_t)r * ns;
+      for (int q = tid; q < ns; q += NT) sa[q] = ga[q];
+    }
+  }
+  if (sm.pg) {
+    for (int q = tid; q < rows * a.n_cols; q += NT) sm.pg[q] = 0.0;
+  }
+}
+
+// Voltages of the staged states (after a barrier that follows `stage_item`).
+template <typename T>
+__device__ void init_voltages(const JxbBlock& blk, const SimSmem<T>& sm, int rows) {
+  const int nn = blk.n_nodes, ns = blk.n_slots;
+  for (int w = threadIdx.x; w < nn * rows; w += blockDim.x) {
+    const int r = w / nn, j = w - r * nn;
+    sm.V[(size_t)r * nn + j] = sm.st[(size_t)r * ns + sm.soff[j]];
   }
 }
 
 // Chain elimination (leaves first) and back-substitution of every tree of the block
-// for all rows. `al`/`au` are the matrix entries A[i, parent] / A[parent, i]; the
-// adjoint passes them swapped to solve with the transposed matrix. On return `S`
-// holds the solution.
+// for all rows. `al`/`au` are A[i, parent] / A[parent, i]; the adjoint passes them
+// swapped to solve with the transposed matrix. On return `S` holds the solution.
 template <typename T>
-__device__ void block_solve(const JxbSimArgs& a, const JxbBlock& blk, int rows, T* D, T* S,
-                            const T* al, const T* au) {
+__device__ void block_solve(const JxbBlock& blk, const SimSmem<T>& sm, int rows, const T* al,
+                            const T* au, T* V = nullptr) {
   const int tid = threadIdx.x, NT = blockDim.x;
-  const int nn = blk.n_nodes, node0 = blk.node0;
-  const int* lp = a.level_ptr + blk.level0;
+  const int nn = blk.n_nodes;
   const int nlev = blk.n_levels;
   // Elimination, leaf chains first (solver_voltage.py:93-98).
   for (int h = 0; h < nlev; ++h) {
-    int c0 = lp[h], nch = lp[h + 1] - c0;
+    const int c0 = sm.lp[h], nch = sm.lp[h + 1] - c0;
     for (int w = tid; w < nch * rows; w += NT) {
-      int c = blk.chain0 + c0 + w % nch;
-      int r = w / nch;
-      T* Dr = D + (size_t)r * nn;
-      T* Sr = S + (size_t)r * nn;
-      int top = a.chain_top[c] - node0;
-      int bot = top + a.chain_len[c] - 1;
+      const int c = c0 + w % nch;
+      const int r = w / nch;
+      T* Dr = sm.D + (size_t)r * nn;
+      T* Sr = sm.S + (size_t)r * nn;
+      const int top = sm.ctop[c];
+      const int bot = top + sm.clen[c] - 1;
       T d = Dr[bot], s = Sr[bot];
-      for (int k = a.chain_cptr[c]; k < a.chain_cptr[c + 1]; ++k) {
-        int ct = a.chain_child[k] - node0;
-        T f = au[ct] / Dr[ct];
+      for (int k = sm.ccp[c]; k < sm.ccp[c + 1]; ++k) {
+        const int ct = sm.cchild[k];
+        const T f = au[ct] / Dr[ct];
         d -= al[ct] * f;
         s -= Sr[ct] * f;
       }
       Dr[bot] = d;
       Sr[bot] = s;
       for (int j = bot - 1; j >= top; --j) {
-        T f = au[j + 1] / d;
+        const T f = au[j + 1] / d;
         d = Dr[j] - al[j + 1] * f;
         s = Sr[j] - s * f;
         Dr[j] = d;
@@ -151,67 +238,70 @@ __device__ void block_solve(const JxbSimArgs& a, const JxbBlock& blk, int rows, 
   }
   // Back-substitution, root chains first (solver_voltage.py:100-106).
   for (int h = nlev - 1; h >= 0; --h) {
-    int c0 = lp[h], nch = lp[h + 1] - c0;
+    const int c0 = sm.lp[h], nch = sm.lp[h + 1] - c0;
     for (int w = tid; w < nch * rows; w += NT) {
-      int c = blk.chain0 + c0 + w % nch;
-      int r = w / nch;
-      T* Dr = D + (size_t)r * nn;
-      T* Sr = S + (size_t)r * nn;
-      int top = a.chain_top[c] - node0;
-      int bot = top + a.chain_len[c] - 1;
-      int pt = a.chain_ptop[c];
-      T xp = pt >= 0 ? Sr[pt - node0] : T(0);
+      const int c = c0 + w % nch;
+      const int r = w / nch;
+      const T* Dr = sm.D + (size_t)r * nn;
+      T* Sr = sm.S + (size_t)r * nn;
+      const int top = sm.ctop[c];
+      const int bot = top + sm.clen[c] - 1;
+      const int pt = sm.cptop[c];
+      T xp = pt >= 0 ? Sr[pt] : T(0);
+      T* Vr = V ? V + (size_t)r * nn : nullptr;
       for (int j = top; j <= bot; ++j) {
-        T x = (Sr[j] - al[j] * xp) / Dr[j];
+        const T x = (Sr[j] - al[j] * xp) / Dr[j];
         Sr[j] = x;
         xp = x;
+        if (Vr) Vr[j] += x;
       }
     }
     __syncthreads();
   }
 }
 
-// Channel step of one node and row: updates the node's states and returns the
-// linearised membrane terms (slope, offset) in uA/cm^2 (before the division by cm).
+// Channel step of one node and row. mode 0: updates + currents; 1: currents only;
+// 2: steady state only. Returns the summed slope and g*E terms in uA/cm^2
+// (modules/base.py:3500-3502: mA/cm^2 * 1000).
 template <typename T>
-__device__ __forceinline__ void node_forward(const JxbSimArgs& a, const SimSmem<T>& sm, int i,
-                                             T* x, int b, T dt, int mode, T& lin, T& cst) {
-  const int cls = a.node_class[i];
-  const int e0 = a.cls_ptr[cls], e1 = a.cls_ptr[cls + 1];
-  const int po = a.poff[i];
-  Prm<T> P{(const T*)a.pbase + po, a.pcol + po, (const T*)a.pscale + (size_t)b * a.n_cols};
+__device__ __forceinline__ void node_channels(const SimSmem<T>& sm, int j, T* x, const T* pv, T dt,
+                                              int mode, T& lin, T& cst) {
+  const int cls = sm.cls[j];
+  const int e0 = sm.cptr[cls], e1 = sm.cptr[cls + 1];
+  const T* pn = pv + sm.poff[j];
   const T v = x[0];
-  if (mode == 0) {
-    for (int q = e0; q < e1; ++q) {
-      ChanEntry e = sm.ents[q];
-      Prm<T> Pe{P.base + e.p[0], P.col + e.p[0], P.scale};
-      channel_update<T>(e, x, Pe, v, dt);
-    }
-  } else if (mode == 2) {
+  lin = cst = T(0);
+  if (mode == 2) {
     for (int q = e0; q < e1; ++q) channel_steady<T>(sm.ents[q], x, v);
-    lin = cst = T(0);
     return;
   }
-  for (int q = e0; q < e1; ++q) x[sm.ents[q].cur] = T(0);
+  if (mode == 0) {
+    for (int q = e0; q < e1; ++q) {
+      const ChanEntry& e = sm.ents[q];
+      channel_update<T>(e, x, Prm<T>{pn + e.p[0]}, v, dt);
+    }
+  }
+  for (int q = e0; q < e1; ++q) {
+    const int c = sm.ents[q].cur;
+    if (c >= 0) x[c] = T(0);
+  }
   T slope = T(0), gge = T(0);
   for (int q = e0; q < e1; ++q) {
-    ChanEntry e = sm.ents[q];
-    Prm<T> Pe{P.base + e.p[0], P.col + e.p[0], P.scale};
-    channel_current<T>(e, x, Pe, v, slope, gge);
+    const ChanEntry& e = sm.ents[q];
+    channel_current<T>(e, x, Prm<T>{pn + e.p[0]}, v, slope, gge);
   }
-  lin = slope * T(1000.0);  // mA/cm^2 -> uA/cm^2, modules/base.py:3500-3502
+  lin = slope * T(1000.0);
   cst = gge * T(1000.0);
 }
 
 template <typename T>
 __device__ __forceinline__ T stim_current(const JxbSimArgs& a, int i, int b, int t) {
   T acc = T(0);
-  int q0 = a.stim_ptr[i], q1 = a.stim_ptr[i + 1];
-  if (q0 == q1 || t >= a.stim_steps) return acc;
+  if (t >= a.stim_steps) return acc;
   const T* st = (const T*)a.stim + (size_t)t * a.stim_rows * a.n_stim +
                 (size_t)(a.stim_rows == 1 ? 0 : b) * a.n_stim;
   const T area = ((const T*)a.area)[i];
-  for (int q = q0; q < q1; ++q) acc += st[a.stim_idx[q]] / area * T(100000);
+  for (int q = a.stim_ptr[i]; q < a.stim_ptr[i + 1]; ++q) acc += st[a.stim_idx[q]] / area * T(100000);
   return acc;
 }
 
@@ -220,114 +310,296 @@ template <typename T>
 __device__ __forceinline__ void record_node(const JxbSimArgs& a, int i, const T* x, int b, int t) {
   T* out = (T*)a.rec_out;
   for (int q = a.rec_ptr[i]; q < a.rec_ptr[i + 1]; ++q) {
-    int sl = a.rec_slot[q];
+    const int sl = a.rec_slot[q];
     out[((size_t)t * a.batch + b) * a.n_rec + a.rec_col[q]] = sl >= 0 ? x[sl] : T(0);
   }
 }
 
+
+// Runs `n_steps` forward steps of one item from the staged state. Used by the
+// forward kernel (ckpt/rec outputs) and by the adjoint (trajectory store).
+// On return sm.st holds the state after the last step; `X1` (if not null) receives
+// the final voltages.
 template <typename T>
-__global__ void __launch_bounds__(256) sim_forward_kernel(JxbSimArgs a) {
+__device__ void run_steps(const JxbSimArgs& a, const JxbBlock& blk, int row0, int rows,
+                          const SimSmem<T>& sm, T dt, int t0, int nsteps, int mode, bool record,
+                          bool ckpt, T* traj, T* X1) {
+  const int tid = threadIdx.x, NT = blockDim.x;
+  const int nn = blk.n_nodes, ns = blk.n_slots, np = blk.n_pslots;
+  const int total = nn * rows;
+  for (int step = 0; step <= nsteps; ++step) {
+    const int t = t0 + step;
+    for (int w = tid; w < total; w += NT) {
+      const int r = w / nn, j = w - r * nn;
+      const int i = blk.node0 + j;
+      const int b = row0 + r;
+      T* x = sm.st + (size_t)r * ns + sm.soff[j];
+      const int nslot = (j + 1 < nn ? sm.soff[j + 1] : ns) - sm.soff[j];
+      const unsigned char f = sm.flags[j];
+      const T* Vr = sm.V + (size_t)r * nn;
+      if (step > 0) x[0] = Vr[j];
+      if (record && step > 0 && (f & FLAG_REC)) record_node<T>(a, i, x, b, t);
+      if (step == nsteps) {
+        if (mode != 0) {
+          T lin, cst;
+          if (mode == 2) node_channels<T>(sm, j, x, sm.pv + (size_t)r * np, dt, 2, lin, cst);
+          node_channels<T>(sm, j, x, sm.pv + (size_t)r * np, dt, 1, lin, cst);
+          if (record && (f & FLAG_REC)) record_node<T>(a, i, x, b, t);
+        }
+        if (X1) X1[(size_t)r * nn + j] = x[0];
+        continue;
+      }
+      if (traj) {
+        T* g = traj + ((size_t)step * a.batch + b) * a.n_slots + blk.slot0 + sm.soff[j];
+        for (int q = 0; q < nslot; ++q) g[q] = x[q];
+      }
+      if (ckpt && ((t - a.ckpt_base) % a.ckpt_every) == 0) {
+        const size_t m = (size_t)((t - a.ckpt_base) / a.ckpt_every);
+        T* g = (T*)a.ckpt + (m * a.batch + b) * a.n_slots + blk.slot0 + sm.soff[j];
+        for (int q = 0; q < nslot; ++q) g[q] = x[q];
+      }
+      const T v = x[0];
+      T lin, cst;
+      node_channels<T>(sm, j, x, sm.pv + (size_t)r * np, dt, 0, lin, cst);
+      if (f & FLAG_STIM) cst += stim_current<T>(a, i, b, t);
+      if (a.syn_lin) {
+        lin += ((const T*)a.syn_lin)[(size_t)b * a.n_nodes + i];
+        cst += ((const T*)a.syn_const)[(size_t)b * a.n_nodes + i];
+      }
+      const T cmv = sm.cm[j];
+      // Delta form of the implicit step: A (v' - v) = rhs - A v, with
+      // (A v)_j = d_j v_j + sum over neighbours of the off-diagonals times their v,
+      // written with voltage differences (exact algebra, small increments).
+      const T lin_t = dt * (lin / cmv);
+      T axv = T(0);
+      const int pj = sm.par[j];
+      if (pj >= 0) axv += sm.al[j] * (Vr[pj] - v);
+      for (int k = sm.kptr[j]; k < sm.kptr[j + 1]; ++k) {
+        const int c = sm.kids[k];
+        axv += sm.au[c] * (Vr[c] - v);
+      }
+      sm.D[(size_t)r * nn + j] = sm.dg[j] + lin_t;
+      sm.S[(size_t)r * nn + j] = ((f & FLAG_COMP) ? dt * (cst / cmv) - lin_t * v : T(0)) - axv;
+    }
+    if (step == nsteps) break;
+    __syncthreads();
+    block_solve<T>(blk, sm, rows, sm.al, sm.au, sm.V);
+  }
+  __syncthreads();
+}
+
+template <typename T>
+__global__ void sim_forward_kernel(JxbSimArgs a) {
   extern __shared__ __align__(16) char smem_raw[];
   SimSmem<T> sm;
   sim_smem_layout<T>(a, false, &sm, smem_raw);
   const JxbItem item = a.items[blockIdx.x];
   const JxbBlock blk = a.blocks[item.block];
   const int rows = item.n_rows, row0 = item.row0;
-  const int nn = blk.n_nodes, ns = blk.n_slots;
-  const int tid = threadIdx.x, NT = blockDim.x;
   const T dt = T(a.dt);
-  load_item<T>(a, blk, row0, rows, sm, dt);
+  stage_item<T>(a, blk, row0, rows, sm, dt, (const T*)a.state, nullptr);
   __syncthreads();
-
-  const int total = nn * rows;
+  init_voltages<T>(blk, sm, rows);
+  __syncthreads();
   const int nsteps = a.mode == 0 ? a.n_steps : 0;
-  for (int step = 0; step <= nsteps; ++step) {
-    const int t = a.t0 + step;
-    for (int w = tid; w < total; w += NT) {
-      const int r = w / nn, j = w % nn;
-      const int i = blk.node0 + j;
-      const int b = row0 + r;
-      T* x = sm.st + (size_t)r * ns + (a.soff[i] - blk.slot0);
-      const int nslot = a.soff[i + 1] - a.soff[i];
-      if (step > 0) x[0] = sm.S[(size_t)r * nn + j];
-      if (step > 0 && a.n_rec > 0) record_node<T>(a, i, x, b, t);
-      if (step == nsteps) {
-        if (a.mode != 0) {
-          // Initial currents (mode 1, modules/base.py:2375-2383), after the steady
-          // state of every channel (mode 2, modules/base.py:2419-2474).
-          T lin, cst;
-          if (a.mode == 2) node_forward<T>(a, sm, i, x, b, dt, 2, lin, cst);
-          node_forward<T>(a, sm, i, x, b, dt, 1, lin, cst);
-          if (a.n_rec > 0) record_node<T>(a, i, x, b, t);
-        }
-        T* g = (T*)a.state + (size_t)b * a.n_slots + a.soff[i];
-        for (int q = 0; q < nslot; ++q) g[q] = x[q];
-        continue;
-      }
-      if (a.traj) {
-        T* g = (T*)a.traj + ((size_t)step * a.batch + b) * a.n_slots + a.soff[i];
-        for (int q = 0; q < nslot; ++q) g[q] = x[q];
-      }
-      if (a.ckpt && ((t - a.ckpt_base) % a.ckpt_every) == 0) {
-        size_t m = (size_t)((t - a.ckpt_base) / a.ckpt_every);
-        T* g = (T*)a.ckpt + (m * a.batch + b) * a.n_slots + a.soff[i];
-        for (int q = 0; q < nslot; ++q) g[q] = x[q];
-      }
-      const T v = x[0];
-      T lin, cst;
-      node_forward<T>(a, sm, i, x, b, dt, 0, lin, cst);
-      T iext = stim_current<T>(a, i, b, t);
-      if (a.syn_lin) {
-        lin += ((const T*)a.syn_lin)[(size_t)b * a.n_nodes + i];
-        cst += ((const T*)a.syn_const)[(size_t)b * a.n_nodes + i];
-      }
-      const T cmv = sm.cm[j];
-      const T lin_t = lin / cmv;
-      const T cst_t = (cst + iext) / cmv;
-      const bool comp = a.cls_comp[a.node_class[i]] != 0;
-      sm.D[(size_t)r * nn + j] = sm.dg[j] + dt * lin_t;
-      sm.S[(size_t)r * nn + j] = comp ? v + dt * cst_t : T(0);
+  run_steps<T>(a, blk, row0, rows, sm, dt, a.t0, nsteps, a.mode, a.n_rec > 0, a.ckpt != nullptr,
+               (T*)a.traj, nullptr);
+  // Write the resident states back.
+  const int ns = blk.n_slots;
+  for (int r = 0; r < rows; ++r) {
+    T* g = (T*)a.state + (size_t)(row0 + r) * a.n_slots + blk.slot0;
+    const T* s = sm.st + (size_t)r * ns;
+    for (int q = threadIdx.x; q < ns; q += blockDim.x) g[q] = s[q];
+  }
+}
+
+// Adjoint of one node and row for one step: replays the channel updates from the
+// pre-step state `x` (restored afterwards from the undo log, one entry at a time, in
+// reverse), then applies the VJPs of the currents and of every update.
+template <typename T>
+__device__ __forceinline__ void node_adjoint(const SimSmem<T>& sm, int j, T* x, T* lam,
+                                             const T* pv, double* pg, T dt, T lr, T x1,
+                                             T& lv) {
+  const int cls = sm.cls[j];
+  const int e0 = sm.cptr[cls], e1 = sm.cptr[cls + 1];
+  const T* pn = pv + sm.poff[j];
+  const T* pb = sm.pb + sm.poff[j];
+  const int* pc = sm.pc + sm.poff[j];
+  const T v = x[0];
+  T undo[kMaxWrites];
+  short uslot[kMaxWrites];
+  int nu = 0;
+  for (int q = e0; q < e1; ++q) {
+    const ChanEntry& e = sm.ents[q];
+    short w[4];
+    const int nw = update_writes(e, w);
+    for (int k = 0; k < nw && nu < kMaxWrites; ++k) {
+      uslot[nu] = w[k];
+      undo[nu] = x[w[k]];
+      ++nu;
     }
-    if (step == nsteps) break;
-    __syncthreads();
-    block_solve<T>(a, blk, rows, sm.D, sm.S, sm.al, sm.au);
+    channel_update<T>(e, x, Prm<T>{pn + e.p[0]}, v, dt);
+  }
+  // Currents at the updated state; their slots were overwritten by the step, so
+  // the adjoint of their previous values starts from zero.
+  for (int q = e1 - 1; q >= e0; --q) {
+    const ChanEntry& e = sm.ents[q];
+    PGradSink<T> G{pb + e.p[0], pc + e.p[0], pg};
+    channel_current_vjp<T>(e, x, lam, Prm<T>{pn + e.p[0]}, G, v, lr, x1, lv);
+  }
+  for (int q = e0; q < e1; ++q) {
+    const int c = sm.ents[q].cur;
+    if (c >= 0) lam[c] = T(0);
+  }
+  for (int q = e1 - 1; q >= e0; --q) {
+    const ChanEntry& e = sm.ents[q];
+    short w[4];
+    const int nw = update_writes(e, w);
+    for (int k = nw - 1; k >= 0; --k) {
+      --nu;
+      x[uslot[nu]] = undo[nu];
+    }
+    PGradSink<T> G{pb + e.p[0], pc + e.p[0], pg};
+    channel_update_vjp<T>(e, x, lam, Prm<T>{pn + e.p[0]}, G, v, dt, lv);
   }
 }
 
 template <typename T>
-int launch_forward(const JxbSimArgs& a, cudaStream_t stream) {
-  size_t smem = sim_smem_layout<T>(a, false, nullptr, nullptr);
+__global__ void sim_backward_kernel(JxbSimArgs a) {
+  extern __shared__ __align__(16) char smem_raw[];
+  SimSmem<T> sm;
+  sim_smem_layout<T>(a, true, &sm, smem_raw);
+  const JxbItem item = a.items[blockIdx.x];
+  const JxbBlock blk = a.blocks[item.block];
+  const int rows = item.n_rows, row0 = item.row0;
+  const int tid = threadIdx.x, NT = blockDim.x;
+  const int nn = blk.n_nodes, ns = blk.n_slots, np = blk.n_pslots;
+  const T dt = T(a.dt);
+  const int K = a.n_steps;
+  T* traj = (T*)a.traj;
+  // Recompute the segment from its checkpoint, storing the state before every step.
+  stage_item<T>(a, blk, row0, rows, sm, dt, (const T*)a.ckpt, (const T*)a.adj);
+  __syncthreads();
+  init_voltages<T>(blk, sm, rows);
+  __syncthreads();
+  run_steps<T>(a, blk, row0, rows, sm, dt, a.t0, K, 0, false, false, traj, sm.X1);
+
+  const T* rec_grad = (const T*)a.rec_grad;
+  const int total = nn * rows;
+  for (int step = K - 1; step >= 0; --step) {
+    const int t = a.t0 + step;
+    // Phase 1: state before the step, recording gradients at t + 1, the diagonal of
+    // the step's matrix and the right-hand side of the transposed solve.
+    for (int w = tid; w < total; w += NT) {
+      const int r = w / nn, j = w - r * nn;
+      const int i = blk.node0 + j;
+      const int b = row0 + r;
+      T* x = sm.st + (size_t)r * ns + sm.soff[j];
+      T* lam = sm.adj + (size_t)r * ns + sm.soff[j];
+      const int nslot = (j + 1 < nn ? sm.soff[j + 1] : ns) - sm.soff[j];
+      const T* g = traj + ((size_t)step * a.batch + b) * a.n_slots + blk.slot0 + sm.soff[j];
+      for (int q = 0; q < nslot; ++q) x[q] = g[q];
+      const unsigned char f = sm.flags[j];
+      if (rec_grad && (f & FLAG_REC)) {
+        for (int q = a.rec_ptr[i]; q < a.rec_ptr[i + 1]; ++q) {
+          const int sl = a.rec_slot[q];
+          if (sl >= 0) lam[sl] += rec_grad[((size_t)(t + 1) * a.batch + b) * a.n_rec + a.rec_col[q]];
+        }
+      }
+      T lin, cst;
+      node_channels<T>(sm, j, x, sm.pv + (size_t)r * np, dt, 0, lin, cst);
+      if (a.syn_lin) lin += ((const T*)a.syn_lin)[(size_t)b * a.n_nodes + i];
+      sm.D[(size_t)r * nn + j] = sm.dg[j] + dt * (lin / sm.cm[j]);
+      sm.S[(size_t)r * nn + j] = lam[0];
+    }
+    __syncthreads();
+    // lambda_r = A^{-T} lambda_v'  (solver_voltage.py:168-187).
+    block_solve<T>(blk, sm, rows, sm.au, sm.al);
+    // Phase 4: vector-Jacobian products of the step.
+    for (int w = tid; w < total; w += NT) {
+      const int r = w / nn, j = w - r * nn;
+      const int b = row0 + r;
+      T* x = sm.st + (size_t)r * ns + sm.soff[j];
+      T* lam = sm.adj + (size_t)r * ns + sm.soff[j];
+      const int nslot = (j + 1 < nn ? sm.soff[j + 1] : ns) - sm.soff[j];
+      const T* g = traj + ((size_t)step * a.batch + b) * a.n_slots + blk.slot0 + sm.soff[j];
+      for (int q = 0; q < nslot; ++q) x[q] = g[q];
+      const T lr = sm.S[(size_t)r * nn + j];
+      const T xnew = sm.X1[(size_t)r * nn + j];
+      const bool comp = (sm.flags[j] & FLAG_COMP) != 0;
+      // d = dg + dt * lin / cm,  rhs = v + dt * cst / cm (compartments only; the
+      // branchpoints have no channels).
+      const T lrs = T(1000.0) * dt * lr / sm.cm[j];
+      T lv = comp ? lr : T(0);
+      lam[0] = T(0);
+      node_adjoint<T>(sm, j, x, lam, sm.pv + (size_t)r * np, sm.pg + (size_t)r * a.n_cols, dt,
+                      lrs, xnew, lv);
+      lam[0] = lv;
+      sm.X1[(size_t)r * nn + j] = x[0];
+    }
+    __syncthreads();
+  }
+  // Adjoint of the segment's initial state, and the parameter gradients.
+  for (int r = 0; r < rows; ++r) {
+    T* ga = (T*)a.adj + (size_t)(row0 + r) * a.n_slots + blk.slot0;
+    const T* sa = sm.adj + (size_t)r * ns;
+    for (int q = tid; q < ns; q += NT) ga[q] = sa[q];
+  }
+  for (int q = tid; q < rows * a.n_cols; q += NT) {
+    const int r = q / a.n_cols, c = q % a.n_cols;
+    const double gv = sm.pg[q];
+    if (c != 0 && gv != 0.0) atomicAdd(a.pgrad + (size_t)(row0 + r) * a.n_cols + c, gv);
+  }
+}
+
+template <typename T>
+int launch_sim(const JxbSimArgs& a, bool backward, cudaStream_t stream) {
+  const size_t smem = sim_smem_layout<T>(a, backward, nullptr, nullptr);
   if (smem > 227 * 1024) {
     snprintf(g_err, sizeof(g_err), "work item needs %zu bytes of shared memory", smem);
     return JXB_ERR_SMEM;
   }
-  cudaError_t e = cudaFuncSetAttribute(sim_forward_kernel<T>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  const int threads = a.threads > 0 ? a.threads : 256;
+  if (threads % 32 != 0 || threads > 1024) {
+    snprintf(g_err, sizeof(g_err), "threads must be a multiple of 32 up to 1024");
+    return JXB_ERR_ARG;
+  }
+  auto kern = backward ? sim_backward_kernel<T> : sim_forward_kernel<T>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) {
     set_err("cudaFuncSetAttribute", e);
     return JXB_ERR_LAUNCH;
   }
-  sim_forward_kernel<T><<<a.n_items, 256, smem, stream>>>(a);
+  kern<<<a.n_items, threads, smem, stream>>>(a);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
-    set_err("sim_forward_kernel", e);
+    set_err(backward ? "sim_backward_kernel" : "sim_forward_kernel", e);
     return JXB_ERR_LAUNCH;
   }
   return JXB_OK;
 }
 
-static int check_sim_args(const JxbSimArgs* a) {
+static int check_sim_args(const JxbSimArgs* a, bool backward) {
   if (!a) return JXB_ERR_ARG;
   if (a->dtype != JXB_F32 && a->dtype != JXB_F64) return JXB_ERR_DTYPE;
   if (a->n_items <= 0) return JXB_OK;
   if (!a->node_class || !a->soff || !a->poff || !a->a_low || !a->a_up || !a->gsum || !a->cm ||
       !a->cls_ptr || !a->cls_comp || !a->entries || !a->pbase || !a->pcol || !a->pscale ||
       !a->blocks || !a->items || !a->chain_top || !a->chain_len || !a->chain_ptop ||
-      !a->chain_cptr || !a->level_ptr || !a->stim_ptr || !a->state || !a->area) {
+      !a->chain_cptr || !a->level_ptr || !a->stim_ptr || !a->state || !a->area ||
+      !a->parent || !a->kid_ptr || !a->kid) {
     snprintf(g_err, sizeof(g_err), "null pointer in JxbSimArgs");
     return JXB_ERR_ARG;
   }
-  if (a->n_rec > 0 && (!a->rec_out || !a->rec_ptr || !a->rec_slot || !a->rec_col)) {
+  if (a->max_rows <= 0 || a->max_nodes <= 0 || a->max_nodes > 32767 || a->max_slots <= 0) {
+    snprintf(g_err, sizeof(g_err), "bad block sizes (nodes per block must be 1..32767)");
+    return JXB_ERR_ARG;
+  }
+  if (a->n_rec > 0 && (!a->rec_ptr || !a->rec_slot || !a->rec_col)) {
+    snprintf(g_err, sizeof(g_err), "recordings without their index arrays");
+    return JXB_ERR_ARG;
+  }
+  if (!backward && a->n_rec > 0 && !a->rec_out) {
     snprintf(g_err, sizeof(g_err), "recordings without output buffer");
     return JXB_ERR_ARG;
   }
@@ -335,7 +607,7 @@ static int check_sim_args(const JxbSimArgs* a) {
     snprintf(g_err, sizeof(g_err), "stimulus indices without stimulus");
     return JXB_ERR_ARG;
   }
-  if (a->ckpt && a->ckpt_every <= 0) {
+  if (a->ckpt && !backward && a->ckpt_every <= 0) {
     snprintf(g_err, sizeof(g_err), "ckpt_every must be positive");
     return JXB_ERR_ARG;
   }
@@ -343,6 +615,12 @@ static int check_sim_args(const JxbSimArgs* a) {
   if (a->syn_lin && a->n_steps != 1) {
     snprintf(g_err, sizeof(g_err), "synaptic terms require one step per launch");
     return JXB_ERR_ARG;
+  }
+  if (backward) {
+    if (!a->ckpt || !a->traj || !a->adj || !a->pgrad || a->mode != 0 || a->n_steps <= 0) {
+      snprintf(g_err, sizeof(g_err), "adjoint needs ckpt, traj, adj, pgrad and n_steps > 0");
+      return JXB_ERR_ARG;
+    }
   }
   return JXB_OK;
 }
@@ -352,10 +630,17 @@ static int check_sim_args(const JxbSimArgs* a) {
 using namespace jxb;
 
 extern "C" int jxb_sim_forward(const JxbSimArgs* a, void* stream) {
-  int rc = check_sim_args(a);
+  int rc = check_sim_args(a, false);
   if (rc != JXB_OK || a->n_items <= 0) return rc;
-  if (a->dtype == JXB_F32) return launch_forward<float>(*a, (cudaStream_t)stream);
-  return launch_forward<double>(*a, (cudaStream_t)stream);
+  if (a->dtype == JXB_F32) return launch_sim<float>(*a, false, (cudaStream_t)stream);
+  return launch_sim<double>(*a, false, (cudaStream_t)stream);
+}
+
+extern "C" int jxb_sim_backward(const JxbSimArgs* a, void* stream) {
+  int rc = check_sim_args(a, true);
+  if (rc != JXB_OK || a->n_items <= 0) return rc;
+  if (a->dtype == JXB_F32) return launch_sim<float>(*a, true, (cudaStream_t)stream);
+  return launch_sim<double>(*a, true, (cudaStream_t)stream);
 }
 
 extern "C" int64_t jxb_sim_smem_bytes(const JxbSimArgs* a, int backward) {

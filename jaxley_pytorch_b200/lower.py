@@ -41,7 +41,7 @@ class Lowered:
     area: np.ndarray
     node_class: np.ndarray
     soff: np.ndarray
-    poff: np.ndarray
+    poff: np.ndarray  # (n_nodes,) first parameter slot of every node (shared runs)
     cls_ptr: np.ndarray
     cls_comp: np.ndarray
     entries: np.ndarray  # (n_entries, 18) int16
@@ -49,6 +49,7 @@ class Lowered:
     pcol: np.ndarray
     pscale: np.ndarray  # (B, n_cols)
     col_info: List[Tuple[str, int]]  # (param name, reference node of first use) per column
+    col_members: List[List[Tuple[str, int, float]]]  # (param name, node, base) per column
     # chains and blocks
     chain_top: np.ndarray
     chain_len: np.ndarray
@@ -61,6 +62,9 @@ class Lowered:
     stim_ptr: np.ndarray
     stim_idx: np.ndarray
     stim: Optional[np.ndarray]  # (steps, rows, n_stim) time-major
+    parent: np.ndarray  # (n_nodes,) parent in internal order, -1 for roots
+    kid_ptr: np.ndarray  # (n_nodes+1,) children CSR (internal order)
+    kid: np.ndarray
     rec_ptr: np.ndarray
     rec_slot: np.ndarray
     rec_col: np.ndarray
@@ -79,7 +83,7 @@ class Lowered:
 
     @property
     def n_pslots(self) -> int:
-        return int(self.poff[-1])
+        return int(len(self.pbase))
 
     @property
     def n_cols(self) -> int:
@@ -164,7 +168,11 @@ def pack_blocks(tree_ptr: np.ndarray, max_nodes: int, weights: Optional[np.ndarr
     return blocks
 
 
-def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64) -> Lowered:
+def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
+          keep_currents: bool = True) -> Lowered:
+    """Lower `problem`. With `keep_currents=False` a channel current gets a state slot
+    only where a channel reads it (the calcium pump reads `i_Ca`) or it is recorded;
+    the other currents are not kept in the resident state."""
     p = problem
     n = p.n_nodes
     B = p.batch
@@ -206,6 +214,7 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64) -> Lo
     cols: Dict[bytes, int] = {}
     col_vecs: List[np.ndarray] = [np.ones(B)]
     col_info: List[Tuple[str, int]] = [("", -1)]
+    col_members: List[set] = [set()]
 
     def pval(name: str, r: int) -> Tuple[float, int]:
         a = np.asarray(p.params[name], dtype=np.float64)
@@ -221,7 +230,12 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64) -> Lo
             cols[key] = len(col_vecs)
             col_vecs.append(prof)
             col_info.append((name, r))
+            col_members.append(set())
+        col_members[cols[key]].add((name, int(r), base))
         return base, cols[key]
+
+    recorded = {(name, int(r)) for name, r in p.recordings}
+    readers = {"CaPump"}  # channels whose update reads their current state
 
     classes: Dict[tuple, int] = {}
     cls_entries: List[np.ndarray] = []
@@ -229,9 +243,8 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64) -> Lo
     cls_nslots: List[int] = []
     node_class = np.zeros(n, dtype=np.int32)
     soff = np.zeros(n + 1, dtype=np.int64)
-    poff = np.zeros(n + 1, dtype=np.int64)
-    pbase: List[float] = []
-    pcol: List[int] = []
+    node_pb: List[List[float]] = []
+    node_pc: List[List[int]] = []
     slot_names: List[List[str]] = []
     for i in range(n):
         r = int(int2node[i])
@@ -243,10 +256,16 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64) -> Lo
                     names.append(s)
         for ci in chs:
             cn = p.channels[ci].current
-            if cn not in names:
+            need = (keep_currents or p.channels[ci].type_name in readers
+                    or (cn, r) in recorded
+                    or any(p.channels[cj].type_name in readers and p.channels[cj].current == cn
+                           for cj in chs))
+            if need and cn not in names:
                 names.append(cn)
         ents = []
         pk = 0
+        pbs: List[float] = []
+        pcs: List[int] = []
         for ci in chs:
             ch = p.channels[ci]
             spec = SPECS[ch.type_name]
@@ -254,7 +273,7 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64) -> Lo
             e[0] = spec.type_id
             e[1] = len(ch.states)
             e[2] = len(ch.params) + len(ch.constants)
-            e[3] = names.index(ch.current)
+            e[3] = names.index(ch.current) if ch.current in names else -1
             for q, s in enumerate(ch.states):
                 e[4 + q] = names.index(s)
             e[10] = pk  # parameters are consecutive: p[0] is the first slot
@@ -263,11 +282,11 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64) -> Lo
                     e[10 + q] = pk + q
             for q, pn in enumerate(ch.params):
                 b, c = pval(pn, r)
-                pbase.append(b)
-                pcol.append(c)
+                pbs.append(b)
+                pcs.append(c)
             for cval in ch.constants:
-                pbase.append(float(cval))
-                pcol.append(0)
+                pbs.append(float(cval))
+                pcs.append(0)
             pk += int(e[2])
             ents.append(e)
         key = (bool(is_comp[r]), tuple(names), tuple(tuple(e.tolist()) for e in ents))
@@ -278,7 +297,8 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64) -> Lo
             cls_nslots.append(len(names))
         node_class[i] = classes[key]
         soff[i + 1] = soff[i] + len(names)
-        poff[i + 1] = poff[i] + pk
+        node_pb.append(pbs)
+        node_pc.append(pcs)
         slot_names.append(names)
     cls_ptr = np.zeros(len(cls_entries) + 1, dtype=np.int32)
     for c, e in enumerate(cls_entries):
@@ -300,6 +320,23 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64) -> Lo
     # ---- blocks, chains ordered by level inside each block ----
     lev = chain_levels(chains)
     blocks_nodes = pack_blocks(tree_ptr, max_block_nodes)
+    # Parameter blocks: nodes with identical parameters (values and columns) share
+    # one run of parameter slots inside their block of trees.
+    pbase: List[float] = []
+    pcol: List[int] = []
+    poff = np.zeros(n, dtype=np.int64)
+    pranges = []
+    for (n0, n1) in blocks_nodes:
+        start = len(pbase)
+        seen: Dict[tuple, int] = {}
+        for i in range(n0, n1):
+            key = (tuple(node_pb[i]), tuple(node_pc[i]))
+            if key not in seen:
+                seen[key] = len(pbase)
+                pbase.extend(node_pb[i])
+                pcol.extend(node_pc[i])
+            poff[i] = seen[key]
+        pranges.append((start, len(pbase) - start))
     chain_top, chain_len, chain_ptop, chain_cptr, chain_child = [], [], [], [0], []
     level_ptr: List[int] = []
     blocks = []
@@ -326,8 +363,9 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64) -> Lo
             for k in kids:
                 chain_child.append(chains[k][0])
             chain_cptr.append(len(chain_child))
+        bi = len(blocks)
         blocks.append([n0, n1 - n0, int(soff[n0]), int(soff[n1] - soff[n0]), chain0, len(cids),
-                       level0, nlev, int(poff[n0]), int(poff[n1] - poff[n0]), 0, 0])
+                       level0, nlev, pranges[bi][0], pranges[bi][1], 0, 0])
 
     # ---- stimulus CSR (internal node -> stimulus columns) ----
     stim_inds = np.asarray(p.stim_inds, dtype=np.int64)
@@ -362,6 +400,20 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64) -> Lo
     def i32(x):
         return np.ascontiguousarray(np.asarray(x, dtype=np.int32))
 
+    # ---- parent / children in internal order (for the delta form of the step) ----
+    par_int = np.full(n, -1, dtype=np.int64)
+    ps = np.asarray(parent_solve, dtype=np.int64)[order]
+    has_par = ps >= 0
+    par_int[has_par] = solve2int[ps[has_par]]
+    kid_lists: List[List[int]] = [[] for _ in range(n)]
+    for i in range(n):
+        if par_int[i] >= 0:
+            kid_lists[int(par_int[i])].append(i)
+    kid_ptr = np.zeros(n + 1, dtype=np.int32)
+    for i in range(n):
+        kid_ptr[i + 1] = kid_ptr[i] + len(kid_lists[i])
+    kid = np.asarray([c for lst in kid_lists for c in lst], dtype=np.int32)
+
     return Lowered(
         n_nodes=n,
         batch=B,
@@ -382,6 +434,7 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64) -> Lo
         pcol=i32(pcol),
         pscale=np.ascontiguousarray(pscale),
         col_info=col_info,
+        col_members=[sorted(m) for m in col_members],
         chain_top=i32(chain_top),
         chain_len=i32(chain_len),
         chain_ptop=i32(chain_ptop),
@@ -392,6 +445,9 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64) -> Lo
         stim_ptr=stim_ptr,
         stim_idx=stim_idx,
         stim=stim,
+        parent=i32(par_int),
+        kid_ptr=kid_ptr,
+        kid=kid,
         rec_ptr=rec_ptr,
         rec_slot=rec_slot,
         rec_col=rec_col,

@@ -36,7 +36,7 @@ class DeviceModel:
     """A lowered model resident on one GPU."""
 
     def __init__(self, low: Lowered, dtype: torch.dtype = torch.float32, device="cuda",
-                 rows_per_item: int = 1):
+                 rows_per_item: int = 1, threads: int = 256):
         self.low = low
         self.dtype = dtype
         self.device = torch.device(device)
@@ -60,12 +60,22 @@ class DeviceModel:
             "chain_child": i(low.chain_child) if len(low.chain_child) else i(np.zeros(1)),
             "level_ptr": i(low.level_ptr), "stim_ptr": i(low.stim_ptr),
             "stim_idx": i(low.stim_idx) if len(low.stim_idx) else i(np.zeros(1)),
-            "rec_ptr": i(low.rec_ptr),
+            "rec_ptr": i(low.rec_ptr), "parent": i(low.parent), "kid_ptr": i(low.kid_ptr),
+            "kid": i(low.kid) if len(low.kid) else i(np.zeros(1)),
             "rec_slot": i(low.rec_slot) if len(low.rec_slot) else i(np.zeros(1)),
             "rec_col": i(low.rec_col) if len(low.rec_col) else i(np.zeros(1)),
         }
         self.pscale = f(low.pscale)
         self.stim = f(low.stim) if low.stim is not None else None
+        blocks = low.blocks
+        self.max_nodes = int(blocks[:, 1].max())
+        self.max_slots = int(blocks[:, 3].max())
+        self.max_chains = int(blocks[:, 5].max())
+        self.max_levels = int(blocks[:, 7].max())
+        self.max_pslots = max(1, int(blocks[:, 9].max()))
+        cp = low.chain_cptr
+        self.max_child = int(max(cp[b[4] + b[5]] - cp[b[4]] for b in blocks))
+        self.threads = threads
         self.set_rows_per_item(rows_per_item)
 
     def set_rows_per_item(self, rows: int) -> None:
@@ -87,7 +97,7 @@ class DeviceModel:
     def args(self, state: torch.Tensor, n_steps: int, t0: int, rec_out: Optional[torch.Tensor],
              mode: int = 0, ckpt=None, ckpt_every: int = 0, ckpt_base: int = 0, traj=None,
              pscale: Optional[torch.Tensor] = None, syn_lin=None, syn_const=None,
-             adj=None, rec_grad=None, pgrad=None) -> _lib.JxbSimArgs:
+             adj=None, rec_grad=None, pgrad=None, items=None) -> _lib.JxbSimArgs:
         low, t = self.low, self.t
         a = _lib.JxbSimArgs()
         a.dtype = self.code
@@ -100,15 +110,22 @@ class DeviceModel:
         a.n_steps = n_steps
         a.t0 = t0
         a.max_rows = self.rows_per_item
-        a.max_nodes = int(low.blocks[:, 1].max())
-        a.max_slots = int(low.blocks[:, 3].max())
+        a.max_nodes = self.max_nodes
+        a.max_slots = self.max_slots
+        a.max_chains = self.max_chains
+        a.max_child = self.max_child
+        a.max_levels = self.max_levels
+        a.max_pslots = self.max_pslots
+        a.threads = self.threads
         a.dt = low.dt
         for k in ["node_class", "soff", "poff", "a_low", "a_up", "gsum", "cm", "cls_ptr",
                   "cls_comp", "entries", "pbase", "pcol", "blocks", "chain_top", "chain_len",
                   "chain_ptop", "chain_cptr", "chain_child", "level_ptr", "stim_ptr", "stim_idx",
-                  "area", "rec_ptr", "rec_slot", "rec_col"]:
+                  "area", "rec_ptr", "rec_slot", "rec_col", "parent", "kid_ptr", "kid"]:
             setattr(a, k, t[k].data_ptr())
-        a.items = self.items.data_ptr()
+        a.items = (items if items is not None else self.items).data_ptr()
+        if items is not None:
+            a.n_items = int(items.shape[0])
         a.n_classes = len(low.cls_comp)
         a.n_entries = int(low.entries.shape[0])
         a.pscale = (pscale if pscale is not None else self.pscale).data_ptr()
@@ -150,32 +167,104 @@ class Simulation:
     """`jx.integrate` for a `Problem` on the CUDA kernels.
 
     `segment` is the number of steps per launch (1 = the plain per-step drop-in;
-    `None` = the whole horizon in one persistent launch).
+    `None` = the whole horizon in one persistent launch). `checkpoint` is the number
+    of steps between stored states for the adjoint (each backward launch recomputes
+    one such segment).
     """
 
     def __init__(self, problem: Problem, dtype=torch.float32, device="cuda",
                  max_block_nodes: int = 4096, rows_per_item: int = 1,
                  segment: Optional[int] = None, init_steady: bool = False,
-                 low: Optional[Lowered] = None):
+                 low: Optional[Lowered] = None, checkpoint: int = 100, threads: int = 256,
+                 keep_currents: bool = True):
         self.problem = problem
-        self.low = low if low is not None else lower(problem, max_block_nodes=max_block_nodes)
-        self.model = DeviceModel(self.low, dtype, device, rows_per_item)
+        self.low = low if low is not None else lower(problem, max_block_nodes=max_block_nodes,
+                                                     keep_currents=keep_currents)
+        self.model = DeviceModel(self.low, dtype, device, rows_per_item, threads=threads)
         self.segment = segment
         self.init_steady = init_steady
+        self.checkpoint = int(checkpoint)
 
-    def run(self, n_steps: Optional[int] = None, pscale: Optional[torch.Tensor] = None,
-            return_state: bool = False):
+    def n_steps(self, n_steps: Optional[int] = None) -> int:
+        return self.low.n_steps if n_steps is None else int(n_steps)
+
+    def forward_raw(self, pscale: torch.Tensor, T: int, ckpt: Optional[torch.Tensor] = None):
+        """Runs the forward pass; returns `(rec (T+1, B, n_rec), final state)`."""
         m = self.model
         low = self.low
-        T = low.n_steps if n_steps is None else int(n_steps)
         state = m.initial_state()
         rec = torch.zeros((T + 1, low.batch, low.n_rec), dtype=m.dtype, device=m.device)
         m.launch_forward(m.args(state, 0, 0, rec, mode=2 if self.init_steady else 1, pscale=pscale))
         seg = T if not self.segment else int(self.segment)
+        if ckpt is not None:
+            seg = min(seg, self.checkpoint) if self.segment else self.checkpoint * max(1, seg // self.checkpoint)
         t = 0
         while t < T:
             k = min(seg, T - t)
-            m.launch_forward(m.args(state, k, t, rec, pscale=pscale))
+            m.launch_forward(m.args(state, k, t, rec, pscale=pscale, ckpt=ckpt,
+                                    ckpt_every=self.checkpoint if ckpt is not None else 0))
             t += k
+        return rec, state
+
+    def backward_raw(self, pscale: torch.Tensor, T: int, ckpt: torch.Tensor,
+                     rec_grad: torch.Tensor) -> torch.Tensor:
+        """Adjoint of the recordings' gradient `rec_grad (T+1, B, n_rec)`: returns
+        d loss / d pscale, float64 `(B, n_cols)`."""
+        m = self.model
+        low = self.low
+        K = self.checkpoint
+        nseg = (T + K - 1) // K
+        adj = torch.zeros((low.batch, low.n_slots), dtype=m.dtype, device=m.device)
+        pgrad = torch.zeros((low.batch, low.n_cols), dtype=torch.float64, device=m.device)
+        traj = torch.empty((min(K, T), low.batch, low.n_slots), dtype=m.dtype, device=m.device)
+        rec_grad = rec_grad.contiguous()
+        for sgi in range(nseg - 1, -1, -1):
+            t0 = sgi * K
+            k = min(K, T - t0)
+            a = m.args(ckpt[sgi], k, t0, None, pscale=pscale, traj=traj, adj=adj,
+                       rec_grad=rec_grad, pgrad=pgrad)
+            a.ckpt = ckpt[sgi].data_ptr()
+            m.launch_backward(a)
+        return pgrad
+
+    def run(self, n_steps: Optional[int] = None, pscale: Optional[torch.Tensor] = None,
+            return_state: bool = False):
+        """Recordings `(B, n_rec, T + 1)`; differentiable with respect to `pscale`
+        (the per-row scales of the parameter columns) when it requires grad."""
+        T = self.n_steps(n_steps)
+        if pscale is None:
+            pscale = self.model.pscale
+        if pscale.requires_grad and torch.is_grad_enabled():
+            out = _IntegrateFn.apply(pscale, self, T)
+            return out
+        rec, state = self.forward_raw(pscale.detach().contiguous(), T)
         out = rec.permute(1, 2, 0)
         return (out, state) if return_state else out
+
+
+class _IntegrateFn(torch.autograd.Function):
+    """Forward: the fused step kernels with a checkpoint every `sim.checkpoint` steps.
+    Backward: the adjoint kernel per segment, in reverse order (recompute + reverse
+    sweep), instead of autograd through every operation of every step."""
+
+    @staticmethod
+    def forward(ctx, pscale, sim, T):
+        low = sim.low
+        K = sim.checkpoint
+        nseg = (T + K - 1) // K
+        ps = pscale.detach().to(sim.model.dtype).contiguous()
+        ckpt = torch.empty((nseg, low.batch, low.n_slots), dtype=sim.model.dtype,
+                           device=sim.model.device)
+        rec, _ = sim.forward_raw(ps, T, ckpt=ckpt)
+        ctx.sim, ctx.T = sim, T
+        ctx.save_for_backward(ps, ckpt)
+        ctx.in_dtype = pscale.dtype
+        return rec.permute(1, 2, 0)
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        ps, ckpt = ctx.saved_tensors
+        sim = ctx.sim
+        rec_grad = grad_out.to(sim.model.dtype).permute(2, 0, 1).contiguous()
+        pgrad = sim.backward_raw(ps, ctx.T, ckpt, rec_grad)
+        return pgrad.to(ctx.in_dtype), None, None

@@ -1,0 +1,383 @@
+"""Seeded synthetic problems of the benchmark configurations (no dataset involved).
+
+`morphology()` builds what `jx.Cell(branches, parents)` builds (modules/cell.py,
+`_init_comp_graph`): cylindrical compartments, one branchpoint node at the end of
+every branch that has children, compartment edges of the five reference types and
+their axial conductances (utils/morph_attributes.py:315-436, restated below). The
+nodes are numbered in a breadth-first solve order (parents before children), so
+`to_solve` is the identity.
+
+Configurations (sizes from the benchmark description):
+
+* `config_small`: 1 branch x 8 compartments, HH, step current at compartment 0,
+  401 steps, float64, forward only.
+* `config_l5pc_tree`: a near-balanced random binary tree of 300 branches x 4
+  compartments (1200 compartments + branchpoints, height 35-45), branch lengths
+  lognormal(ln 30 um, 0.5), radii tapering 2 -> 0.3 um with branch depth, the L5PC
+  channel set (soma: NaTs2T, SKv3_1, SKE2, CaNernstReversal, CaPump, CaHVA, CaLVA;
+  dendrites: NaTs2T, SKv3_1, M, H; Leak everywhere) with every conductance scaled by
+  U[0.5, 1.5] per parameter set; batch 256, dt 0.025 ms, 4000 steps.
+* `config_uneven`: 4096 cells of log-uniform(4, 3000) compartments and depth 1-60,
+  HH or L5PC, each with its own step current.
+"""
+from __future__ import annotations
+
+from typing import Dict, List, Optional, Sequence, Tuple
+
+import numpy as np
+
+from .channels import SPECS, ChannelInstance, make_instance
+from .problem import Problem, SynapseType
+
+PI = np.pi
+
+
+def morphology(branch_parents: Sequence[int], ncomp: Sequence[int], comp_radius: Sequence[np.ndarray],
+               comp_length: Sequence[np.ndarray], r_a: float = 5000.0, cm: float = 1.0):
+    """Nodes and the tree system of one cell. Returns a dict of node-order arrays
+    (node order = solve order) and the compartment index of every (branch, comp)."""
+    nb = len(branch_parents)
+    children: List[List[int]] = [[] for _ in range(nb)]
+    for b in range(1, nb):
+        children[int(branch_parents[b])].append(b)
+    # Breadth-first numbering over (branch, compartment) and branchpoint nodes.
+    order: List[Tuple[str, int, int]] = []  # ("c", branch, comp) or ("bp", branch, -1)
+    parent: List[int] = []
+    queue = [(0, -1)]
+    qi = 0
+    comp_node: Dict[Tuple[int, int], int] = {}
+    bp_node: Dict[int, int] = {}
+    while qi < len(queue):
+        b, pnode = queue[qi]
+        qi += 1
+        prev = pnode
+        for k in range(int(ncomp[b])):
+            comp_node[(b, k)] = len(order)
+            order.append(("c", b, k))
+            parent.append(prev)
+            prev = comp_node[(b, k)]
+        if children[b]:
+            bp_node[b] = len(order)
+            order.append(("bp", b, -1))
+            parent.append(prev)
+            for c in children[b]:
+                queue.append((c, bp_node[b]))
+    n = len(order)
+    is_comp = np.array([o[0] == "c" for o in order])
+    radius = np.ones(n)
+    length = np.ones(n)
+    for j, (kind, b, k) in enumerate(order):
+        if kind == "c":
+            radius[j] = comp_radius[b][k]
+            length[j] = comp_length[b][k]
+    area = 2 * PI * radius * length
+    rl = (length / 2) / (radius**2 * PI)  # resistive load of half a compartment
+    ra = np.full(n, float(r_a))
+    cmv = np.full(n, float(cm))
+    parent = np.asarray(parent, dtype=np.int64)
+    # Axial conductances per directed edge (sink row), utils/morph_attributes.py:380-433.
+    g_low = np.zeros(n)  # sink = node j, source = parent
+    g_up = np.zeros(n)  # sink = parent, source = node j
+    for j in range(1, n):
+        p = parent[j]
+        if is_comp[j] and is_comp[p]:  # compartment to compartment
+            r = rl[p] * ra[p] + rl[j] * ra[j]
+            g_low[j] = 1 / r / area[j] / cmv[j] * 1e7
+            g_up[j] = 1 / r / area[p] / cmv[p] * 1e7
+        elif not is_comp[j]:  # j is a branchpoint, parent compartment
+            r = rl[p] * ra[p]
+            g_low[j] = 1 / r  # c2bp: not divided by area
+            g_up[j] = 1 / r / area[p] / cmv[p] * 1e7  # bp2c
+        else:  # compartment whose parent is a branchpoint
+            r = rl[j] * ra[j]
+            g_low[j] = 1 / r / area[j] / cmv[j] * 1e7  # bp2c
+            g_up[j] = 1 / r  # c2bp
+    depth_of_branch = np.zeros(nb, dtype=np.int64)
+    for b in range(1, nb):
+        depth_of_branch[b] = depth_of_branch[branch_parents[b]] + 1
+    return {
+        "n": n, "parent": parent, "is_comp": is_comp, "area": area, "cm": cmv,
+        "radius": radius, "length": length, "g_low": g_low, "g_up": g_up,
+        "comp_node": comp_node, "order": order, "branch_depth": depth_of_branch,
+    }
+
+
+def _edges(parent: np.ndarray, g_low: np.ndarray, g_up: np.ndarray):
+    """Compartment-edge arrays (sinks, axial) and the lower/upper maps."""
+    n = len(parent)
+    nonroot = np.nonzero(parent >= 0)[0]
+    m = len(nonroot)
+    sinks = np.concatenate([nonroot, parent[nonroot]])
+    axial = np.concatenate([g_low[nonroot], g_up[nonroot]])
+    map_lower = np.zeros(n, dtype=np.int64)
+    map_upper = np.zeros(n, dtype=np.int64)
+    map_lower[nonroot] = np.arange(m)
+    map_upper[nonroot] = m + np.arange(m)
+    return sinks, axial, map_lower, map_upper
+
+
+def assemble(cells: List[dict], channels_per_cell: List[List[Tuple[str, np.ndarray, str, Dict[str, object]]]],
+             batch: int, dt: float, n_steps: int, v0: float = -70.0,
+             stim: Optional[List[Tuple[int, Tuple[int, int], np.ndarray]]] = None,
+             recordings: Optional[List[Tuple[str, int, Tuple[int, int]]]] = None) -> Problem:
+    """Concatenate cells into one problem (a network without synapses).
+
+    `channels_per_cell[c]` lists `(type, local node indices, instance name,
+    {param name: value (scalar, (n_local,), or (batch, n_local))})` in insertion order;
+    channels with the same instance name across cells are merged, as the reference
+    merges equally named channels of a network. `stim` holds
+    `(cell, (branch, comp), samples (batch or 1, steps))`, `recordings`
+    `(state, cell, (branch, comp))`.
+    """
+    offs = np.cumsum([0] + [c["n"] for c in cells])
+    N = int(offs[-1])
+    parent = np.concatenate([np.where(c["parent"] >= 0, c["parent"] + o, -1) for c, o in zip(cells, offs)])
+    g_low = np.concatenate([c["g_low"] for c in cells])
+    g_up = np.concatenate([c["g_up"] for c in cells])
+    sinks, axial, map_lower, map_upper = _edges(parent, g_low, g_up)
+    is_comp = np.concatenate([c["is_comp"] for c in cells])
+    params: Dict[str, np.ndarray] = {
+        "capacitance": np.concatenate([c["cm"] for c in cells]),
+        "area": np.concatenate([c["area"] for c in cells]),
+        "radius": np.concatenate([c["radius"] for c in cells]),
+        "length": np.concatenate([c["length"] for c in cells]),
+    }
+    states: Dict[str, np.ndarray] = {"v": np.full(N, float(v0))}
+    inst: Dict[str, ChannelInstance] = {}
+    order: List[str] = []
+    pending: Dict[str, List[Tuple[np.ndarray, Dict[str, object]]]] = {}
+    for c, chans in enumerate(channels_per_cell):
+        for type_name, local, name, values in chans:
+            glob = np.asarray(local, dtype=np.int64) + offs[c]
+            if name not in inst:
+                inst[name] = make_instance(type_name, np.zeros(0, np.int64), name=name,
+                                           constants=values.get("__constants__"))
+                order.append(name)
+                pending[name] = []
+            pending[name].append((glob, values))
+    current_names: List[str] = []
+    for name in order:
+        ch = inst[name]
+        spec = SPECS[ch.type_name]
+        inds = np.concatenate([g for g, _ in pending[name]])
+        ch.inds = inds
+        for (suffix, default), pname in zip(spec.params, ch.params):
+            if pname not in params:
+                params[pname] = np.full(N, float(default))
+        for (suffix, default), sname in zip(spec.states, ch.states):
+            if sname not in states:
+                states[sname] = np.full(N, np.nan)
+            states[sname][inds] = np.where(np.isnan(states[sname][inds]), float(default),
+                                           states[sname][inds])
+        for glob, values in pending[name]:
+            for key, val in values.items():
+                if key == "__constants__":
+                    continue
+                val = np.asarray(val, dtype=np.float64)
+                if val.ndim == 2 or params[key].ndim == 2:
+                    if params[key].ndim == 1:
+                        params[key] = np.broadcast_to(params[key], (batch, N)).copy()
+                    params[key][:, glob] = np.broadcast_to(val, (batch, len(glob)))
+                else:
+                    params[key][glob] = val
+        if ch.current not in current_names:
+            current_names.append(ch.current)
+    for cn in current_names:
+        states[cn] = np.zeros(N)
+    for k in list(states):
+        states[k] = np.where(np.isnan(states[k]), 0.0, states[k])
+    stim_inds, stim_arr = np.zeros(0, np.int64), None
+    if stim:
+        stim_inds = np.asarray([offs[c] + cells[c]["comp_node"][bc] for c, bc, _ in stim], dtype=np.int64)
+        rows = max(np.atleast_2d(s).shape[0] for _, _, s in stim)
+        stim_arr = np.zeros((rows, len(stim), n_steps))
+        for q, (_, _, s) in enumerate(stim):
+            s = np.atleast_2d(np.asarray(s, dtype=np.float64))
+            L = min(n_steps, s.shape[1])
+            stim_arr[:, q, :L] = s[:, :L]
+    recs = []
+    for name, c, bc in recordings or []:
+        recs.append((name, int(offs[c] + cells[c]["comp_node"][bc])))
+    return Problem(
+        n_nodes=N, comp_inds=np.nonzero(is_comp)[0], sinks=sinks, axial=axial,
+        parent_lookup=parent, to_solve=np.arange(N), map_lower=map_lower, map_upper=map_upper,
+        channels=[inst[n] for n in order], params=params, states=states, dt=float(dt),
+        n_steps=int(n_steps), stim_inds=stim_inds, stim=stim_arr, recordings=recs,
+        batch=int(batch), current_names=current_names,
+    )
+
+
+def step_current(i_delay: float, i_dur: float, i_amp, delta_t: float, t_max: float) -> np.ndarray:
+    """Step current of `int(t_max // delta_t) + 2` samples (stimulus.py:8-36)."""
+    n = int(t_max // delta_t) + 2
+    t = np.arange(n) * delta_t
+    amp = np.asarray(i_amp, dtype=np.float64).reshape(-1, 1)
+    on = ((t >= i_delay) & (t < i_delay + i_dur)).astype(np.float64)
+    return amp * on[None]
+
+
+def config_small() -> Problem:
+    cell = morphology([-1], [8], [np.full(8, 1.0)], [np.full(8, 10.0)])
+    nodes = np.arange(cell["n"])
+    prob = assemble([cell], [[("HH", nodes, "HH", {})]], batch=1, dt=0.025, n_steps=401,
+                    stim=[(0, (0, 0), step_current(1.0, 1.0, 0.1, 0.025, 10.0))],
+                    recordings=[("v", 0, (0, 0))])
+    return prob
+
+
+def balanced_random_tree(n_branches: int, rng: np.random.Generator, skew: float = 0.7) -> List[int]:
+    """A random binary tree of `n_branches` branches, grown by attaching every new
+    branch to an open slot: with probability `skew` to a slot of the shallowest
+    branches, else to any open slot."""
+    parents = [-1]
+    depth = [0]
+    nchild = [0]
+    for b in range(1, n_branches):
+        open_ = [q for q in range(b) if nchild[q] < 2]
+        if rng.random() < skew:
+            dmin = min(depth[q] for q in open_)
+            cand = [q for q in open_ if depth[q] == dmin]
+        else:
+            cand = open_
+        p = int(rng.choice(cand))
+        parents.append(p)
+        depth.append(depth[p] + 1)
+        nchild[p] += 1
+        nchild.append(0)
+    return parents
+
+
+def tree_height(parent: np.ndarray) -> int:
+    n = len(parent)
+    h = np.zeros(n, dtype=np.int64)
+    for j in range(n - 1, 0, -1):
+        p = parent[j]
+        h[p] = max(h[p], h[j] + 1)
+    return int(h.max()) if n else 0
+
+
+L5PC_SOMA = [
+    ("NaTs2T", "somatic_NaTs2T", {"somatic_NaTs2T_gNaTs2T": 0.983955}),
+    ("SKv3_1", "somatic_SKv3_1", {"somatic_SKv3_1_gSKv3_1": 0.303472}),
+    ("SKE2", "somatic_SKE2", {"somatic_SKE2_gSKE2": 0.008407}),
+    ("CaNernstReversal", "CaNernstReversal", {"__constants__": {"T": 307.15}}),
+    ("CaPump", "somatic_CaPump", {"somatic_CaPump_gamma": 0.000609, "somatic_CaPump_decay": 210.485291}),
+    ("CaHVA", "somatic_CaHVA", {"somatic_CaHVA_gCaHVA": 0.000994}),
+    ("CaLVA", "somatic_CaLVA", {"somatic_CaLVA_gCaLVA": 0.000333}),
+]
+L5PC_DEND = [
+    ("NaTs2T", "apical_NaTs2T", {"apical_NaTs2T_gNaTs2T": 0.026145}),
+    ("SKv3_1", "apical_SKv3_1", {"apical_SKv3_1_gSKv3_1": 0.004226}),
+    ("M", "apical_M", {"apical_M_gM": 0.000143}),
+    ("H", "apical_H", {"apical_H_gH": 8e-5}),
+]
+# Parameters that every parameter set scales by U[0.5, 1.5].
+L5PC_SCALED = [
+    "somatic_NaTs2T_gNaTs2T", "somatic_SKv3_1_gSKv3_1", "somatic_SKE2_gSKE2",
+    "somatic_CaHVA_gCaHVA", "somatic_CaLVA_gCaLVA", "apical_NaTs2T_gNaTs2T",
+    "apical_SKv3_1_gSKv3_1", "apical_M_gM", "apical_H_gH", "Leak_gLeak",
+]
+
+
+def l5pc_channels(cell: dict, scales: Optional[Dict[str, np.ndarray]] = None, ncomp_soma: int = 4):
+    """Channel list of one L5PC-like cell: soma = the first branch's compartments."""
+    soma = np.asarray([cell["comp_node"][(0, k)] for k in range(ncomp_soma)])
+    comps = np.nonzero(cell["is_comp"])[0]
+    dend = np.setdiff1d(comps, soma)
+    scales = scales or {}
+
+    def vals(d):
+        out = {}
+        for k, v in d.items():
+            if k == "__constants__":
+                out[k] = v
+            elif k in scales:
+                out[k] = np.asarray(v) * np.asarray(scales[k])[:, None]
+            else:
+                out[k] = v
+        return out
+
+    chans = [(t, soma, name, vals(v)) for t, name, v in L5PC_SOMA]
+    chans += [(t, dend, name, vals(v)) for t, name, v in L5PC_DEND]
+    leak = {"Leak_gLeak": 3e-05, "Leak_eLeak": -75.0}
+    chans.append(("Leak", comps, "Leak", vals(leak)))
+    return chans
+
+
+def config_l5pc_tree(batch: int = 256, n_branches: int = 300, ncomp: int = 4, n_steps: int = 4000,
+                     seed: int = 0, height_range=(35, 45), stim_amp: float = 0.3,
+                     scale_seed: int = 1) -> Problem:
+    rng = np.random.default_rng(seed)
+    for _ in range(1000):
+        parents = balanced_random_tree(n_branches, rng)
+        lengths = rng.lognormal(np.log(30.0), 0.5, size=n_branches)
+        depth = np.zeros(n_branches, dtype=np.int64)
+        for b in range(1, n_branches):
+            depth[b] = depth[parents[b]] + 1
+        dmax = max(int(depth.max()), 1)
+        radius = 2.0 - (2.0 - 0.3) * depth / dmax
+        cell = morphology(parents, [ncomp] * n_branches,
+                          [np.full(ncomp, r) for r in radius],
+                          [np.full(ncomp, L / ncomp) for L in lengths], r_a=100.0)
+        h = tree_height(cell["parent"])
+        if height_range[0] <= h <= height_range[1]:
+            break
+    else:
+        raise RuntimeError("no tree within the height range")
+    srng = np.random.default_rng(scale_seed)
+    scales = {k: srng.uniform(0.5, 1.5, size=batch) for k in L5PC_SCALED}
+    chans = l5pc_channels(cell, scales, ncomp_soma=ncomp)
+    t_max = n_steps * 0.025
+    prob = assemble([cell], [chans], batch=batch, dt=0.025, n_steps=n_steps, v0=-65.0,
+                    stim=[(0, (0, 0), step_current(10.0, 80.0, stim_amp, 0.025, t_max))],
+                    recordings=[("v", 0, (0, 0))])
+    prob.states.setdefault("CaCon_e", np.full(prob.n_nodes, 2.0))
+    prob.states["CaCon_i"] = np.where(prob.states.get("CaCon_i", np.zeros(prob.n_nodes)) == 0,
+                                      5e-05, prob.states["CaCon_i"])
+    prob.states["CaCon_e"] = np.where(prob.states["CaCon_e"] == 0, 2.0, prob.states["CaCon_e"])
+    for k in ["eNa", "eK"]:
+        if k in prob.params:
+            prob.params[k] = np.full(prob.n_nodes, 50.0 if k == "eNa" else -85.0)
+    prob.meta = {"height": h, "scales": scales}
+    return prob
+
+
+def config_uneven(n_cells: int = 4096, seed: int = 0, n_steps: int = 2000, min_comp: int = 4,
+                  max_comp: int = 3000, max_depth: int = 60, l5pc_fraction: float = 0.5) -> Problem:
+    """Cells of log-uniform compartment counts and bounded depth, HH or L5PC."""
+    rng = np.random.default_rng(seed)
+    cells, chans, stims, recs = [], [], [], []
+    t_max = n_steps * 0.025
+    for c in range(n_cells):
+        ncomp_total = int(round(np.exp(rng.uniform(np.log(min_comp), np.log(max_comp)))))
+        ncomp = 4 if ncomp_total >= 4 else ncomp_total
+        nb = max(1, ncomp_total // ncomp)
+        depth_cap = int(rng.integers(1, max_depth + 1))
+        parents = [-1]
+        bdepth = [0]
+        for b in range(1, nb):
+            cand = [q for q in range(max(0, b - 64), b) if bdepth[q] < depth_cap]
+            p = int(rng.choice(cand)) if cand else 0
+            parents.append(p)
+            bdepth.append(bdepth[p] + 1)
+        lengths = rng.lognormal(np.log(30.0), 0.5, size=nb)
+        radius = np.clip(2.0 - 0.05 * np.asarray(bdepth), 0.3, 2.0)
+        cell = morphology(parents, [ncomp] * nb, [np.full(ncomp, r) for r in radius],
+                          [np.full(ncomp, L / ncomp) for L in lengths], r_a=100.0)
+        cells.append(cell)
+        if rng.random() < l5pc_fraction and nb > 1:
+            chans.append(l5pc_channels(cell, None, ncomp_soma=ncomp))
+        else:
+            comps = np.nonzero(cell["is_comp"])[0]
+            chans.append([("HH", comps, "HH", {})])
+        delay = float(rng.uniform(1, 5))
+        amp = float(rng.uniform(0.05, 0.5))
+        stims.append((c, (0, 0), step_current(delay, 1.0, amp, 0.025, t_max)))
+        recs.append(("v", c, (0, 0)))
+    prob = assemble(cells, chans, batch=1, dt=0.025, n_steps=n_steps, v0=-65.0, stim=stims,
+                    recordings=recs)
+    if "CaCon_i" in prob.states:
+        prob.states["CaCon_i"] = np.where(prob.states["CaCon_i"] == 0, 5e-05, prob.states["CaCon_i"])
+    if "CaCon_e" in prob.states:
+        prob.states["CaCon_e"] = np.where(prob.states["CaCon_e"] == 0, 2.0, prob.states["CaCon_e"])
+    return prob

@@ -489,6 +489,28 @@ class _Stepper:
         self.axial = np.broadcast_to(ax, (B, ax.shape[-1])) if ax.ndim == 2 else ax[None]
         self.cur_names = list(problem.current_names)
 
+    def channel_currents(self, st, v):
+        """Currents with the finite-difference slope (modules/base.py:3445-3542); also
+        writes the current states. Returns `(lin, const)` in uA/cm^2."""
+        p, B, n = self.p, self.B, self.n
+        lin = np.zeros((B, n))
+        const = np.zeros((B, n))
+        cur_states = {k: np.zeros((B, n)) for k in self.cur_names}
+        for ch, prm in zip(p.channels, self.ch_params):
+            inds = np.asarray(ch.inds)
+            chs = {k: st[k][:, inds] for k in ch.states}
+            vv = v[:, inds]
+            i0 = np.broadcast_to(channel_current(ch, chs, vv, prm), vv.shape)
+            i1 = np.broadcast_to(channel_current(ch, chs, vv + DIFF, prm), vv.shape)
+            voltage_term = (i1 - i0) / DIFF
+            constant_term = i0 - voltage_term * vv
+            np.add.at(lin.T, inds, voltage_term.T)
+            np.add.at(const.T, inds, (-constant_term).T)
+            np.add.at(cur_states[ch.current].T, inds, i0.T)
+        for k in self.cur_names:
+            st[k] = cur_states[k]
+        return lin * 1000.0, const * 1000.0
+
     def step(self, st: Dict[str, np.ndarray], t: int) -> Dict[str, np.ndarray]:
         p, B, n, dt = self.p, self.B, self.n, self.p.dt
         st = dict(st)
@@ -509,25 +531,7 @@ class _Stepper:
                 arr = st[key].copy()
                 arr[:, inds] = val
                 st[key] = arr
-        # Currents with the finite-difference slope (modules/base.py:3445-3542).
-        lin = np.zeros((B, n))
-        const = np.zeros((B, n))
-        cur_states = {k: np.zeros((B, n)) for k in self.cur_names}
-        for ch, prm in zip(p.channels, self.ch_params):
-            inds = np.asarray(ch.inds)
-            chs = {k: st[k][:, inds] for k in ch.states}
-            vv = v[:, inds]
-            i0 = np.broadcast_to(channel_current(ch, chs, vv, prm), vv.shape)
-            i1 = np.broadcast_to(channel_current(ch, chs, vv + DIFF, prm), vv.shape)
-            voltage_term = (i1 - i0) / DIFF
-            constant_term = i0 - voltage_term * vv
-            np.add.at(lin.T, inds, voltage_term.T)
-            np.add.at(const.T, inds, (-constant_term).T)
-            np.add.at(cur_states[ch.current].T, inds, i0.T)
-        for k in self.cur_names:
-            st[k] = cur_states[k]
-        lin = lin * 1000.0
-        const = const * 1000.0
+        lin, const = self.channel_currents(st, v)
         # Synapses (modules/network.py:350-478).
         syn_lin = np.zeros((B, n))
         syn_const = np.zeros((B, n))
@@ -578,9 +582,14 @@ class _Stepper:
         return out
 
 
-def integrate(problem, n_steps: Optional[int] = None, return_states: bool = False):
+def integrate(problem, n_steps: Optional[int] = None, return_states: bool = False,
+              init_steady: bool = False):
     """`jx.integrate` for a `Problem` (integrate.py:396-666): recordings of shape
-    `(B, n_rec, n_steps + 1)`, the first sample being the initial state."""
+    `(B, n_rec, n_steps + 1)`, the first sample being the initial state.
+
+    The initial channel currents are recomputed from the initial states
+    (`_append_currents_with_plan`, modules/base.py:2375-2383); with `init_steady`,
+    every channel first goes to its steady state (`Module.init_states`)."""
     B = problem.batch
     n = problem.n_nodes
     T = problem.n_steps if n_steps is None else n_steps
@@ -593,6 +602,9 @@ def integrate(problem, n_steps: Optional[int] = None, return_states: bool = Fals
         if syn.current is not None:
             st[f"i_{syn.name}"] = _bn(syn.current, B, len(syn.pre))
     stepper = _Stepper(problem, B)
+    if init_steady:
+        st = init_steady_states(problem, st)
+    stepper.channel_currents(st, st["v"])
 
     def record(s):
         return np.stack([s[name][:, idx] for name, idx in problem.recordings], axis=1)

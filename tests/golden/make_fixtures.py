@@ -230,8 +230,86 @@ def synapse_net():
 
 
 if __name__ == "__main__":
-    which = sys.argv[1:] or ["golden", "small", "tree", "l5pc", "forest", "synapse"]
+    which = [w for w in sys.argv[1:] if w != "synth"] if sys.argv[1:] else ["golden", "small", "tree", "l5pc", "forest", "synapse", "synth"]
     fns = {"golden": golden_cases, "small": config_small, "tree": hh_tree, "l5pc": l5pc_cell,
            "forest": hh_forest, "synapse": synapse_net}
     for w in which:
-        fns[w]()
+        if w in fns:
+            fns[w]()
+
+
+def synth_check():
+    """A small tree from `jaxley_pytorch_b200.synth` rebuilt with the reference's own
+    `jx.Cell`: checks the synthetic morphology, conductances and channel setup."""
+    from jaxley_pytorch_b200 import synth
+
+    nb, ncomp, B = 15, 4, 2
+    rng = np.random.default_rng(11)
+    parents = synth.balanced_random_tree(nb, rng)
+    lengths = rng.lognormal(np.log(30.0), 0.5, size=nb)
+    depth = np.zeros(nb, dtype=np.int64)
+    for b in range(1, nb):
+        depth[b] = depth[parents[b]] + 1
+    radius = 2.0 - (2.0 - 0.3) * depth / max(int(depth.max()), 1)
+    cellm = synth.morphology(parents, [ncomp] * nb, [np.full(ncomp, r) for r in radius],
+                             [np.full(ncomp, L / ncomp) for L in lengths], r_a=100.0)
+    scales = {k: np.linspace(0.6, 1.4, B) for k in synth.L5PC_SCALED}
+    chans = synth.l5pc_channels(cellm, scales, ncomp_soma=ncomp)
+    n_steps = 600
+    prob = synth.assemble([cellm], [chans], batch=B, dt=0.025, n_steps=n_steps, v0=-65.0,
+                          stim=[(0, (0, 0), synth.step_current(2.0, 10.0, 0.3, 0.025, n_steps * 0.025))],
+                          recordings=[("v", 0, (0, 0)), ("v", 0, (nb - 1, 3))])
+    for k in ["eNa", "eK"]:
+        prob.params[k] = np.full(prob.n_nodes, 50.0 if k == "eNa" else -85.0)
+
+    cell = jx.Cell([jx.Branch(jx.Compartment(), ncomp)] * nb, parents=parents)
+    for b in range(nb):
+        cell.branch(b).set("radius", float(radius[b]))
+        cell.branch(b).set("length", float(lengths[b] / ncomp))
+    cell.set("axial_resistivity", 100.0)
+    classes = {"NaTs2T": NaTs2T, "SKv3_1": SKv3_1, "SKE2": SKE2, "CaPump": CaPump, "CaHVA": CaHVA,
+               "CaLVA": CaLVA, "M": M, "H": H}
+    for t, name, vals in synth.L5PC_SOMA:
+        if t == "CaNernstReversal":
+            ch = CaNernstReversal()
+            ch.channel_constants["T"] = 307.15
+        else:
+            ch = classes[t]().change_name(name)
+        cell.branch(0).insert(ch)
+    cell.branch(0).set("CaCon_i", 5e-05)
+    cell.branch(0).set("CaCon_e", 2.0)
+    for b in range(1, nb):
+        for t, name, vals in synth.L5PC_DEND:
+            cell.branch(b).insert(classes[t]().change_name(name))
+    cell.insert(Leak())
+    for t, name, vals in synth.L5PC_SOMA + synth.L5PC_DEND + [("Leak", "Leak", {"Leak_gLeak": 3e-05, "Leak_eLeak": -75.0})]:
+        for k, v in vals.items():
+            if k != "__constants__":
+                cell.set(k, v)
+    cell.set("eNa", 50.0)
+    cell.set("eK", -85.0)
+    cell.set("v", -65.0)
+    cell.init_states()
+    cell.branch(0).loc(0.0).record()
+    cell.branch(nb - 1).comp(3).record()
+    cell.branch(0).loc(0.0).stimulate(jx.step_current(2.0, 10.0, 0.3, 0.025, n_steps * 0.025))
+    pstate = None
+    soma_vals = {k: v for _, _, d in synth.L5PC_SOMA for k, v in d.items() if k != "__constants__"}
+    dend_vals = {k: v for _, _, d in synth.L5PC_DEND for k, v in d.items()}
+    for k in synth.L5PC_SCALED:
+        vals = torch.tensor(scales[k])[:, None]
+        if k in soma_vals:
+            pstate = cell.branch(0).data_set(k, vals * soma_vals[k], pstate)
+        elif k in dend_vals:
+            view = cell.branch(list(range(1, nb)))
+            pstate = view.data_set(k, vals * dend_vals[k], pstate)
+        else:
+            pstate = cell.data_set(k, vals * 3e-05, pstate)
+    ref = jx.integrate(cell, param_state=pstate, delta_t=0.025, t_max=(n_steps - 1) * 0.025).detach().numpy()
+    path = os.path.join(HERE, "synth_l5pc_15x4.npz")
+    save_problem(prob, path, ref=ref, init_steady=1)
+    print("synth_l5pc_15x4", ref.shape, prob.n_nodes)
+
+
+if __name__ == "__main__" and "synth" in sys.argv[1:]:
+    synth_check()

@@ -19,7 +19,7 @@ def test_oracle_matches_reference_golden_vectors(name):
 @pytest.mark.parametrize("name", fixture_names())
 def test_oracle_matches_reference_run(name):
     prob, extra = load_fixture(name)
-    out = oracle.integrate(prob)
+    out = oracle.integrate(prob, init_steady=bool(extra.get("init_steady", 0)))
     ref = extra["ref"].reshape(out.shape)
     scale = max(1.0, np.max(np.abs(ref)))
     assert np.max(np.abs(out - ref)) <= 1e-9 * scale

@@ -19,7 +19,8 @@ def test_fp64_matches_reference(cuda_device, name, segment):
     prob, extra = load_fixture(name)
     if prob.synapses:
         pytest.skip("synapse problems run through the network path")
-    sim = Simulation(prob, dtype=torch.float64, device=cuda_device, segment=segment)
+    steady = bool(extra.get("init_steady", 0))
+    sim = Simulation(prob, dtype=torch.float64, device=cuda_device, segment=segment, init_steady=steady)
     out = sim.run().cpu().numpy()
     ref = extra["ref"].reshape(out.shape)
     scale = max(1.0, np.abs(ref).max())
