@@ -1,0 +1,357 @@
+#!/usr/bin/env python
+"""Benchmark of the per-timestep hot path: compartment-steps/s, forward + adjoint.
+
+Workload (per GPU): the synthetic L5PC-like tree (300 branches x 4 compartments, 1200
+compartments + branchpoints, near-balanced, height 35-45), 256 parameter sets with
+every conductance scaled by U[0.5, 1.5], float32, dt = 0.025 ms, 4000 steps; one
+bench step = the simulation of all 256 rows, the MSE to a seeded target trace and its
+gradient with respect to the 256 x 10 conductance scales through the adjoint
+(checkpoint every 100 steps). Compartment-steps count compartments x rows x steps
+(branchpoints excluded, every simulated step once).
+
+`--impl reference` times the CPU restatement of the reference's torch path (eager
+autograd) on the host cores, on a bounded sample of the same workload.
+
+Multi-GPU (torchrun): every rank simulates its own 256 parameter sets (weak scaling,
+no collective in the data path); the timing is the maximum over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+from datetime import timedelta
+
+import numpy as np
+
+REPO = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, REPO)
+
+METRIC = "compartment-steps/s fwd+bwd on 1 B200 vs plain kernels; p50/p99 request latency"
+UNIT = "compartment-steps/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--batch", type=int, default=256)
+    ap.add_argument("--tsteps", type=int, default=4000)
+    ap.add_argument("--checkpoint", type=int, default=100)
+    ap.add_argument("--threads", type=int, default=512)
+    ap.add_argument("--rows", type=int, default=1)
+    ap.add_argument("--cpu-batch", type=int, default=16)
+    ap.add_argument("--cpu-tsteps", type=int, default=200)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+class ClockSampler:
+    """Samples SM clocks and throttle reasons with nvidia-smi during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_peak_hbm():
+    path = os.path.join(REPO, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def traffic_from_profiles(kernel: str):
+    """DRAM bytes per launch of `kernel` from the committed ncu summary, if any."""
+    path = os.path.join(REPO, "profiles", "dram_traffic.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return d.get(kernel)
+    return None
+
+
+def workload(rank: int, batch: int, tsteps: int):
+    from jaxley_pytorch_b200 import synth
+
+    prob = synth.config_l5pc_tree(batch=batch, n_steps=tsteps, seed=0, scale_seed=1 + rank)
+    held_out = synth.config_l5pc_tree(batch=1, n_steps=tsteps, seed=0, scale_seed=10_000)
+    return prob, held_out
+
+
+def algorithmic_bytes(low, itemsize: int):
+    """Per compartment-step: S = state slots per compartment, P = batch-varying
+    parameters per compartment (conductances); forward s(2S+P), adjoint launch
+    (recompute with trajectory store + reverse pass) s(6S+2P)."""
+    comps = [i for i in range(low.n_nodes) if low.cls_comp[low.node_class[i]]]
+    S = float(np.mean([low.soff[i + 1] - low.soff[i] for i in comps]))
+    cls_np = {}
+    P_list = []
+    for i in comps:
+        po = low.poff[i]
+        cls = low.node_class[i]
+        n_par = 0
+        for e in low.entries[low.cls_ptr[cls]:low.cls_ptr[cls + 1]]:
+            n_par += int(e[2])
+        P_list.append(int(np.count_nonzero(low.pcol[po:po + n_par])))
+    P = float(np.mean(P_list))
+    return S, P, itemsize * (2 * S + P), itemsize * (6 * S + 2 * P)
+
+
+def run_ours(args, rank, world, device):
+    import torch
+
+    from jaxley_pytorch_b200.sim import Simulation
+
+    torch.cuda.set_device(device)
+    prob, held = workload(rank, args.batch, args.tsteps)
+    T = prob.n_steps
+    kw = dict(dtype=torch.float32, device=device, checkpoint=args.checkpoint, init_steady=True,
+              keep_currents=False, threads=args.threads, rows_per_item=args.rows)
+    sim = Simulation(prob, **kw)
+    tsim = Simulation(held, **kw)
+    with torch.no_grad():
+        target = tsim.run()[0, 0].detach()
+    low = sim.low
+    n_comp = int(len(prob.comp_inds))
+    B = low.batch
+    ps0 = sim.model.pscale.clone()
+
+    def train_step(ps):
+        rec = sim.run(pscale=ps)
+        loss = ((rec[:, 0, :] - target) ** 2).mean()
+        (g,) = torch.autograd.grad(loss, ps)
+        return loss, g
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if world == 1:
+            return x
+        t = torch.tensor([x], device=device, dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        return float(t.item())
+
+    ps = ps0.clone().requires_grad_(True)
+    for _ in range(args.warmup):
+        train_step(ps)
+    torch.cuda.synchronize()
+    # Timed region: device timing with CUDA events; inputs resident in HBM.
+    sim.model.events = []
+    sim.model.timed_kind = "backward"
+    launches0 = sim.model.launches
+    barrier()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with ClockSampler(torch.cuda.current_device()) as clocks:
+        e0.record()
+        for _ in range(args.steps):
+            loss, g = train_step(ps)
+        e1.record()
+        torch.cuda.synchronize()
+    barrier()
+    launches = sim.model.launches - launches0
+    ms = max_over_ranks(e0.elapsed_time(e1))
+    bwd = [(a.elapsed_time(b), k) for a, b, k in sim.model.events]
+    sim.model.timed_kind = None
+    # Forward launch durations (one extra measured pass, outside the timed region).
+    sim.model.events = []
+    sim.model.timed_kind = "forward"
+    train_step(ps)
+    torch.cuda.synchronize()
+    fwd = [(a.elapsed_time(b), k) for a, b, k in sim.model.events if k > 0]
+    sim.model.timed_kind = None
+
+    comp_steps = n_comp * B * T * args.steps * world
+    value = comp_steps / (ms / 1e3)
+
+    # End to end through the public API: pinned host inputs in, loss and gradient out.
+    ps_host = ps0.detach().cpu().pin_memory()
+    loss_host = torch.empty((), dtype=torch.float32).pin_memory()
+    g_host = torch.empty_like(ps_host).pin_memory()
+    barrier()
+    torch.cuda.synchronize()
+    f0 = torch.cuda.Event(enable_timing=True)
+    f1 = torch.cuda.Event(enable_timing=True)
+    f0.record()
+    for _ in range(args.steps):
+        psd = ps_host.to(device, non_blocking=True).requires_grad_(True)
+        loss, g = train_step(psd)
+        loss_host.copy_(loss.detach(), non_blocking=True)
+        g_host.copy_(g, non_blocking=True)
+    f1.record()
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1))
+    e2e = {"value": comp_steps / (e2e_ms / 1e3), "unit": UNIT,
+           "h2d_bytes_per_step": int(ps_host.numel() * ps_host.element_size()),
+           "d2h_bytes_per_step": int(loss_host.element_size() + g_host.numel() * g_host.element_size())}
+
+    S, P, fwd_b, bwd_b = algorithmic_bytes(low, 4)
+    peak, peak_kind = measured_peak_hbm()
+    bwd_ms = float(np.mean([t for t, _ in bwd])) if bwd else None
+    fwd_ms = float(np.mean([t for t, _ in fwd])) if fwd else None
+    bwd_total = sum(t for t, _ in bwd)
+    fwd_total = sum(t for t, _ in fwd) * args.steps
+    if bwd_total >= fwd_total and bwd:
+        kern, k_steps, dur, per = "sim_backward_kernel", bwd[0][1], bwd_ms, bwd_b
+    else:
+        kern, k_steps, dur, per = "sim_forward_kernel", fwd[0][1], fwd_ms, fwd_b
+    bytes_launch = per * n_comp * B * k_steps
+    achieved = bytes_launch / (dur / 1e3) / 1e9
+    traffic = traffic_from_profiles(kern)
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "traffic": traffic, "kernel": kern,
+                "peak_source": peak_kind, "avg_launch_ms": dur,
+                "algorithmic_bytes_per_comp_step": per, "state_slots_per_comp": S,
+                "batched_params_per_comp": P, "fwd_launch_ms": fwd_ms, "bwd_launch_ms": bwd_ms}
+    out = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": {"workload": "l5pc_tree_300x4_b256_t4000_fwd_adjoint", "compartments": n_comp,
+                   "nodes": prob.n_nodes, "tree_height": prob.meta["height"], "batch": B,
+                   "time_steps": T, "checkpoint": args.checkpoint,
+                   "threads_per_cta": args.threads, "rows_per_cta": args.rows,
+                   "l2": "working set larger than L2 (trajectory buffer %d MB)"
+                         % (args.checkpoint * B * low.n_slots * 4 // 2**20),
+                   "loss": "MSE of the somatic voltage to a held-out parameter set's trace"},
+        "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
+        "clocks": clocks.summary(), "loss": float(loss.detach()),
+    }
+    return out
+
+
+def cpu_sample(batch: int, tsteps: int, reps: int = 1):
+    """Times the torch CPU restatement of the reference path (forward + autograd
+    backward) on `batch` rows x `tsteps` steps of the workload."""
+    import torch
+
+    from jaxley_pytorch_b200 import synth
+    from oracle import torch_port
+
+    cores = os.cpu_count() or 1
+    torch.set_num_threads(cores)
+    prob = synth.config_l5pc_tree(batch=batch, n_steps=tsteps, seed=0, scale_seed=1)
+    held = synth.config_l5pc_tree(batch=1, n_steps=tsteps, seed=0, scale_seed=10_000)
+    with torch.no_grad():
+        target = torch_port.integrate(held, {}, dtype=torch.float32, init_steady=True)[0, 0]
+    names = synth.L5PC_SCALED
+    params = {k: torch.as_tensor(np.asarray(prob.params[k]), dtype=torch.float32).requires_grad_(True)
+              for k in names}
+    n_comp = len(prob.comp_inds)
+    times = []
+    for r in range(reps + 1):
+        t0 = time.perf_counter()
+        rec = torch_port.integrate(prob, params, dtype=torch.float32, init_steady=True)
+        loss = ((rec[:, 0, :] - target) ** 2).mean()
+        loss.backward()
+        times.append(time.perf_counter() - t0)
+    t = float(np.median(times[1:])) if reps > 0 else times[0]
+    return n_comp * batch * tsteps / t, cores, t
+
+
+def main():
+    args = parse()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        if rank != 0:
+            return 0
+        vals = []
+        for _ in range(args.warmup):
+            cpu_sample(args.cpu_batch, args.cpu_tsteps, reps=0)
+        for _ in range(args.steps):
+            v, cores, t = cpu_sample(args.cpu_batch, args.cpu_tsteps, reps=0)
+            vals.append(v)
+        value = float(np.median(vals))
+        sample = f"{args.cpu_batch} of 256 rows x {args.cpu_tsteps} of 4000 steps per step, fwd+bwd"
+        out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
+               "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+               "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+               "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+               "config": {"workload": "l5pc_tree_300x4_b256_t4000_fwd_adjoint"},
+               "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                                "sample": sample},
+               "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
+                       "d2h_bytes_per_step": 0}}
+        print(json.dumps(out))
+        return 0
+    import torch
+
+    if world > 1:
+        torch.distributed.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                             device_id=torch.device("cuda", local))
+    device = torch.device("cuda", local)
+    out = run_ours(args, rank, world, device)
+    if rank == 0:
+        if world == 1 and not args.no_cpu_baseline:
+            v, cores, t = cpu_sample(args.cpu_batch, args.cpu_tsteps, reps=0)
+            out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                                   "sample": f"{args.cpu_batch} of 256 rows x {args.cpu_tsteps} of "
+                                             f"4000 steps, fwd+bwd, {t:.1f} s"}
+        print(json.dumps(out))
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -38,7 +38,10 @@ __device__ __forceinline__ bool gate_is_alpha_beta(int g) {
 
 template <typename S> struct Pair { S a, b; };
 
-// Rates of every gate: (alpha, beta) or (x_inf, tau).
+// Rates of every gate: (alpha, beta) for the alpha/beta gates, (x_inf, 1/tau) for the
+// x_inf/tau gates. Each is the reference's expression with divisions by constants
+// turned into products and u / (1 - exp(-u/k)) written as x_over_expm1(-u, k)
+// (equal values; finite at u = 0 where the reference divides 0 by 0).
 template <typename S>
 __device__ __forceinline__ Pair<S> gate_rates(int g, S v) {
   typedef typename Base<S>::type B;
@@ -47,115 +50,119 @@ __device__ __forceinline__ Pair<S> gate_rates(int g, S v) {
   switch (g) {
     case G_HH_M:  // channels/hh.py:88-92
       r.a = B(0.1) * x_over_expm1(-(v + B(40)), B(10));
-      r.b = B(4.0) * save_exp(-(v + B(65)) / B(18));
+      r.b = B(4.0) * save_exp(-(v + B(65)) * B(1.0 / 18.0));
       break;
     case G_HH_H:  // channels/hh.py:94-98
-      r.a = B(0.07) * save_exp(-(v + B(65)) / B(20));
-      r.b = B(1.0) / (save_exp(-(v + B(35)) / B(10)) + B(1));
+      r.a = B(0.07) * save_exp(-(v + B(65)) * B(1.0 / 20.0));
+      r.b = rcp(save_exp(-(v + B(35)) * B(0.1)) + B(1));
       break;
     case G_HH_N:  // channels/hh.py:100-104
       r.a = B(0.01) * x_over_expm1(-(v + B(55)), B(10));
-      r.b = B(0.125) * save_exp(-(v + B(65)) / B(80));
+      r.b = B(0.125) * save_exp(-(v + B(65)) * B(1.0 / 80.0));
       break;
     case G_NATAT_M:
     case G_NATS2T_M: {  // l5pc.py:95-103, 177-185
-      B off = g == G_NATAT_M ? B(38) : B(32);
-      S alpha = (B(0.182) * (v + off + B(1e-6))) / (B(1) - save_exp(-(v + off + B(1e-6)) / B(6)));
-      S beta = (B(0.124) * (-v - off + B(1e-6))) / (B(1) - save_exp(-(-v - off + B(1e-6)) / B(6)));
-      r.a = alpha / (alpha + beta);
-      r.b = B(1) / (alpha + beta) / qt;
+      const B off = g == G_NATAT_M ? B(38) : B(32);
+      S alpha = B(0.182) * x_over_expm1(-(v + off + B(1e-6)), B(6));
+      S beta = B(0.124) * x_over_expm1(-(-v - off + B(1e-6)), B(6));
+      S sum = alpha + beta;
+      r.a = fdiv(alpha, sum);
+      r.b = sum * qt;
       break;
     }
     case G_NATAT_H:
     case G_NATS2T_H: {  // l5pc.py:105-113, 187-195
-      B off = g == G_NATAT_H ? B(66) : B(60);
-      S alpha = (B(-0.015) * (v + off + B(1e-6))) / (B(1) - save_exp((v + off + B(1e-6)) / B(6)));
-      S beta = (B(-0.015) * (-v - off + B(1e-6))) / (B(1) - save_exp((-v - off + B(1e-6)) / B(6)));
-      r.a = alpha / (alpha + beta);
-      r.b = B(1) / (alpha + beta) / qt;
+      const B off = g == G_NATAT_H ? B(66) : B(60);
+      S alpha = B(0.015) * x_over_expm1(v + off + B(1e-6), B(6));
+      S beta = B(0.015) * x_over_expm1(-v - off + B(1e-6), B(6));
+      S sum = alpha + beta;
+      r.a = fdiv(alpha, sum);
+      r.b = sum * qt;
       break;
     }
     case G_NAP_M: {  // l5pc.py:268-276
-      S alpha = (B(0.182) * (v + B(38) + B(1e-6))) / (B(1) - save_exp(-(v + B(38) + B(1e-6)) / B(6)));
-      S beta = (B(0.124) * (-v - B(38) + B(1e-6))) / (B(1) - save_exp(-(-v - B(38) + B(1e-6)) / B(6)));
-      r.b = B(6) / (alpha + beta) / qt;
-      r.a = B(1.0) / (B(1) + save_exp((v + B(52.6)) / B(-4.6)));
+      S alpha = B(0.182) * x_over_expm1(-(v + B(38) + B(1e-6)), B(6));
+      S beta = B(0.124) * x_over_expm1(-(-v - B(38) + B(1e-6)), B(6));
+      r.b = (alpha + beta) * (qt * B(1.0 / 6.0));
+      r.a = rcp(B(1) + save_exp((v + B(52.6)) * B(-1.0 / 4.6)));
       break;
     }
     case G_NAP_H: {  // l5pc.py:278-289
-      S alpha = (B(-2.88e-6) * (v + B(17) + B(1e-6))) / (B(1) - save_exp((v + B(17) + B(1e-6)) / B(4.63)));
-      S beta = (B(6.94e-6) * (v + B(64.4) + B(1e-6))) /
-               (B(1) - save_exp((-(v + B(64.4)) + B(1e-6)) / B(2.63)));
-      r.b = B(1) / (alpha + beta) / qt;
-      r.a = B(1.0) / (B(1) + save_exp((v + B(48.8)) / B(10)));
+      S alpha = B(2.88e-6) * x_over_expm1(v + B(17) + B(1e-6), B(4.63));
+      S w = -(v + B(64.4)) + B(1e-6);
+      S beta = fdiv(B(-6.94e-6) * (v + B(64.4) + B(1e-6)), exm1(clamp20(w * B(1.0 / 2.63))));
+      r.b = (alpha + beta) * qt;
+      r.a = rcp(B(1) + save_exp((v + B(48.8)) * B(0.1)));
       break;
     }
     case G_KPST_M: {  // l5pc.py:355-369
       S va = v + B(10);
-      r.a = B(1) / (B(1) + save_exp(-(va + B(1)) / B(12)));
+      r.a = rcp(B(1) + save_exp(-(va + B(1)) * B(1.0 / 12.0)));
       if (val(va) < B(-50.0))
-        r.b = (B(1.25) + B(175.03) * save_exp(va * B(0.026))) / qt;
+        r.b = fdiv(S(qt), B(1.25) + B(175.03) * save_exp(va * B(0.026)));
       else
-        r.b = (B(1.25) + B(13) * save_exp(-va * B(0.026))) / qt;
+        r.b = fdiv(S(qt), B(1.25) + B(13) * save_exp(-va * B(0.026)));
       break;
     }
     case G_KPST_H: {  // l5pc.py:371-381
       S va = v + B(10);
-      r.a = B(1) / (B(1) + save_exp(-(va + B(54)) / B(-11)));
-      S q = (va + B(75)) / B(48);
-      r.b = (B(360) + (B(1010) + B(24) * (va + B(55))) * save_exp(-(q * q))) / qt;
+      r.a = rcp(B(1) + save_exp((va + B(54)) * B(1.0 / 11.0)));
+      S q = (va + B(75)) * B(1.0 / 48.0);
+      r.b = fdiv(S(qt), B(360) + (B(1010) + B(24) * (va + B(55))) * save_exp(-(q * q)));
       break;
     }
     case G_KTST_M: {  // l5pc.py:444-451
       S va = v + B(10);
-      r.a = B(1) / (B(1) + save_exp(-(va + B(0)) / B(19)));
-      S q = (va + B(71)) / B(59);
-      r.b = (B(0.34) + B(0.92) * save_exp(-(q * q))) / qt;
+      r.a = rcp(B(1) + save_exp(-(va + B(0)) * B(1.0 / 19.0)));
+      S q = (va + B(71)) * B(1.0 / 59.0);
+      r.b = fdiv(S(qt), B(0.34) + B(0.92) * save_exp(-(q * q)));
       break;
     }
     case G_KTST_H: {  // l5pc.py:453-460
       S va = v + B(10);
-      r.a = B(1) / (B(1) + save_exp(-(va + B(66)) / B(-10)));
-      S q = (va + B(73)) / B(23);
-      r.b = (B(8) + B(49) * save_exp(-(q * q))) / qt;
+      r.a = rcp(B(1) + save_exp((va + B(66)) * B(0.1)));
+      S q = (va + B(73)) * B(1.0 / 23.0);
+      r.b = fdiv(S(qt), B(8) + B(49) * save_exp(-(q * q)));
       break;
     }
     case G_SKV31_M:  // l5pc.py:585-590
-      r.a = B(1) / (B(1) + save_exp((v - B(18.7)) / B(-9.7)));
-      r.b = B(0.2) * B(20.0) / (B(1) + save_exp((v + B(46.56)) / B(-44.14)));
+      r.a = rcp(B(1) + save_exp((v - B(18.7)) * B(-1.0 / 9.7)));
+      r.b = (B(1) + save_exp((v + B(46.56)) * B(-1.0 / 44.14))) * B(1.0 / (0.2 * 20.0));
       break;
     case G_M_M: {  // l5pc.py:653-661
       S ma = B(3.3e-3) * save_exp(B(2.5) * B(0.04) * (v + B(35)));
       S mb = B(3.3e-3) * save_exp(B(-2.5) * B(0.04) * (v + B(35)));
-      r.a = ma / (ma + mb);
-      r.b = (B(1) / (ma + mb)) / qt;
+      S sum = ma + mb;
+      r.a = fdiv(ma, sum);
+      r.b = sum * qt;
       break;
     }
     case G_CAHVA_M:  // l5pc.py:723-727
-      r.a = (B(0.055) * (B(-27) - v + B(1e-6))) / (save_exp((B(-27.0) - v + B(1e-6)) / B(3.8)) - B(1.0));
-      r.b = B(0.94) * save_exp((B(-75.0) - v + B(1e-6)) / B(17.0));
+      r.a = B(0.055) * x_over_expm1(B(-27) - v + B(1e-6), B(3.8));
+      r.b = B(0.94) * save_exp((B(-75.0) - v + B(1e-6)) * B(1.0 / 17.0));
       break;
     case G_CAHVA_H:  // l5pc.py:729-734
-      r.a = B(0.000457) * save_exp((B(-13.0) - v) / B(50.0));
-      r.b = B(0.0065) / (save_exp((-v - B(15.0)) / B(28.0)) + B(1.0));
+      r.a = B(0.000457) * save_exp((B(-13.0) - v) * B(1.0 / 50.0));
+      r.b = fdiv(S(B(0.0065)), save_exp((-v - B(15.0)) * B(1.0 / 28.0)) + B(1.0));
       break;
     case G_CALVA_M: {  // l5pc.py:795-802
       S vs = v + B(10);
-      r.a = B(1.0) / (B(1) + save_exp((vs + B(30)) / B(-6)));
-      r.b = (B(5.0) + B(20.0) / (B(1) + save_exp((vs + B(25)) / B(5)))) / qt;
+      r.a = rcp(B(1) + save_exp((vs + B(30)) * B(-1.0 / 6.0)));
+      r.b = fdiv(S(qt), B(5.0) + B(20.0) * rcp(B(1) + save_exp((vs + B(25)) * B(0.2))));
       break;
     }
     case G_CALVA_H: {  // l5pc.py:804-811
       S vs = v + B(10);
-      r.a = B(1.0) / (B(1) + save_exp((vs + B(80)) / B(6.4)));
-      r.b = (B(20.0) + B(50.0) / (B(1) + save_exp((vs + B(40)) / B(7)))) / qt;
+      r.a = rcp(B(1) + save_exp((vs + B(80)) * B(1.0 / 6.4)));
+      r.b = fdiv(S(qt), B(20.0) + B(50.0) * rcp(B(1) + save_exp((vs + B(40)) * B(1.0 / 7.0))));
       break;
     }
     default: {  // G_H_M, l5pc.py:973-984
-      S ma = B(0.001) * B(6.43) * (v + B(154.9) + B(1e-6)) / (save_exp((v + B(154.9) + B(1e-6)) / B(11.9)) - B(1));
-      S mb = B(0.001) * B(193) * save_exp(v / B(33.1));
-      r.a = ma / (ma + mb);
-      r.b = B(1) / (ma + mb);
+      S ma = B(0.001 * 6.43) * x_over_expm1(v + B(154.9) + B(1e-6), B(11.9));
+      S mb = B(0.001 * 193) * save_exp(v * B(1.0 / 33.1));
+      S sum = ma + mb;
+      r.a = fdiv(ma, sum);
+      r.b = sum;
       break;
     }
   }
@@ -173,13 +180,12 @@ template <typename S, typename B>
 __device__ __forceinline__ S gate_step(int g, S v, B x, B dt, B* e_out) {
   Pair<S> r = gate_rates<S>(g, v);
   S xinf, em1;
-  if (gate_is_alpha_beta(g)) {  // solver_gate.py:45-64
-    S tau = B(1) / (r.a + r.b);
-    xinf = r.a * tau;
-    em1 = save_expm1(-dt / tau);
-  } else {  // solver_gate.py:67-87
-    S slope = B(-1.0) / r.b;
-    em1 = save_expm1(slope * dt);
+  if (gate_is_alpha_beta(g)) {  // solver_gate.py:45-53: tau = 1/(a+b), x_inf = a*tau
+    S sum = r.a + r.b;
+    xinf = fdiv(r.a, sum);
+    em1 = save_expm1(-dt * sum);
+  } else {  // solver_gate.py:67-87: slope = -1/tau
+    em1 = save_expm1(-r.b * dt);
     xinf = r.a;
   }
   if (e_out) *e_out = B(1) + val(em1);
@@ -190,7 +196,7 @@ __device__ __forceinline__ S gate_step(int g, S v, B x, B dt, B* e_out) {
 template <typename B>
 __device__ __forceinline__ B gate_steady(int g, B v) {
   Pair<B> r = gate_rates<B>(g, v);
-  if (gate_is_alpha_beta(g)) return r.a / (r.a + r.b);
+  if (gate_is_alpha_beta(g)) return fdiv(r.a, r.a + r.b);
   return r.a;
 }
 
@@ -199,7 +205,7 @@ template <typename S>
 __device__ __forceinline__ S ske2_zinf(S cai) {
   typedef typename Base<S>::type B;
   if (val(cai) < B(1e-7)) cai = cai + B(1e-7);
-  return B(1) / (B(1) + pw(B(0.00043) / cai, B(4.8)));
+  return rcp(B(1) + pw(fdiv(S(B(0.00043)), cai), B(4.8)));
 }
 
 // Gate ids and exponents of the gated ohmic channels.

@@ -6,7 +6,10 @@
 
 namespace jxb {
 
-__device__ __forceinline__ float ex(float x) { return expf(x); }
+// float32 uses the hardware approximations (exp2-based exponential, approximate
+// reciprocal and division: a few ulp, well inside the float32 tolerance of the
+// simulator); float64 stays correctly rounded.
+__device__ __forceinline__ float ex(float x) { return __expf(x); }
 __device__ __forceinline__ double ex(double x) { return exp(x); }
 __device__ __forceinline__ float exm1(float x) { return expm1f(x); }
 __device__ __forceinline__ double exm1(double x) { return expm1(x); }
@@ -16,7 +19,12 @@ __device__ __forceinline__ float pw(float x, float y) { return powf(x, y); }
 __device__ __forceinline__ double pw(double x, double y) { return pow(x, y); }
 __device__ __forceinline__ float fab(float x) { return fabsf(x); }
 __device__ __forceinline__ double fab(double x) { return fabs(x); }
+__device__ __forceinline__ float fdiv(float a, float b) { return __fdividef(a, b); }
+__device__ __forceinline__ double fdiv(double a, double b) { return a / b; }
+__device__ __forceinline__ float rcp(float b) { return __fdividef(1.0f, b); }
+__device__ __forceinline__ double rcp(double b) { return 1.0 / b; }
 
+// (rcp/fdiv for float/double are defined above.)
 // Dual number a + b*eps (eps^2 = 0): `d` carries the derivative with respect to
 // one seeded input.
 template <typename T>
@@ -31,8 +39,9 @@ template <typename T> __device__ __forceinline__ Dual<T> operator-(Dual<T> a, Du
 template <typename T> __device__ __forceinline__ Dual<T> operator-(Dual<T> a) { return Dual<T>(-a.v, -a.d); }
 template <typename T> __device__ __forceinline__ Dual<T> operator*(Dual<T> a, Dual<T> b) { return Dual<T>(a.v * b.v, a.d * b.v + a.v * b.d); }
 template <typename T> __device__ __forceinline__ Dual<T> operator/(Dual<T> a, Dual<T> b) {
-  T q = a.v / b.v;
-  return Dual<T>(q, (a.d - q * b.d) / b.v);
+  T ib = rcp(b.v);
+  T q = a.v * ib;
+  return Dual<T>(q, (a.d - q * b.d) * ib);
 }
 template <typename T> __device__ __forceinline__ Dual<T> operator+(Dual<T> a, T b) { return Dual<T>(a.v + b, a.d); }
 template <typename T> __device__ __forceinline__ Dual<T> operator+(T a, Dual<T> b) { return Dual<T>(a + b.v, b.d); }
@@ -42,8 +51,9 @@ template <typename T> __device__ __forceinline__ Dual<T> operator*(Dual<T> a, T 
 template <typename T> __device__ __forceinline__ Dual<T> operator*(T a, Dual<T> b) { return Dual<T>(a * b.v, a * b.d); }
 template <typename T> __device__ __forceinline__ Dual<T> operator/(Dual<T> a, T b) { return Dual<T>(a.v / b, a.d / b); }
 template <typename T> __device__ __forceinline__ Dual<T> operator/(T a, Dual<T> b) {
-  T q = a / b.v;
-  return Dual<T>(q, -q * b.d / b.v);
+  T ib = rcp(b.v);
+  T q = a * ib;
+  return Dual<T>(q, -q * b.d * ib);
 }
 template <typename T> __device__ __forceinline__ Dual<T> ex(Dual<T> a) { T e = ex(a.v); return Dual<T>(e, e * a.d); }
 template <typename T> __device__ __forceinline__ Dual<T> exm1(Dual<T> a) { return Dual<T>(exm1(a.v), ex(a.v) * a.d); }
@@ -53,6 +63,8 @@ template <typename T> __device__ __forceinline__ Dual<T> pw(Dual<T> a, T y) {
   return Dual<T>(p, y * pw(a.v, y - T(1)) * a.d);
 }
 template <typename T> __device__ __forceinline__ Dual<T> fab(Dual<T> a) { return a.v < T(0) ? -a : a; }
+template <typename T> __device__ __forceinline__ Dual<T> fdiv(Dual<T> a, Dual<T> b) { return a / b; }
+template <typename T> __device__ __forceinline__ Dual<T> rcp(Dual<T> b) { return T(1) / b; }
 
 template <typename T> __device__ __forceinline__ T val(T a) { return a; }
 template <typename T> __device__ __forceinline__ T val(Dual<T> a) { return a.v; }
@@ -73,10 +85,10 @@ template <typename S> __device__ __forceinline__ S save_exp(S x) { return ex(cla
 // solver_gate.py:14-30: x / (exp(x/y) - 1), series y*(1 - z/2 + z^2/12) for |z| < 1e-4.
 template <typename S, typename T> __device__ __forceinline__ S x_over_expm1(S x, T y) {
   typedef typename Base<S>::type B;
-  S z = clamp20(x / y);
+  S z = clamp20(x * (B(1) / B(y)));
   bool small = fab(val(z)) < B(1e-4);
-  if (small) return y * (B(1) - z / B(2) + z * z / B(12));
-  return x / exm1(z);
+  if (small) return y * (B(1) - z * B(0.5) + z * z * B(1.0 / 12.0));
+  return fdiv(x, exm1(z));
 }
 
 }  // namespace jxb

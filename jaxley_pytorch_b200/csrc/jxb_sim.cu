@@ -217,20 +217,23 @@ __device__ void block_solve(const JxbBlock& blk, const SimSmem<T>& sm, int rows,
       T* Sr = sm.S + (size_t)r * nn;
       const int top = sm.ctop[c];
       const int bot = top + sm.clen[c] - 1;
+      // D receives the reciprocal of every eliminated pivot.
       T d = Dr[bot], s = Sr[bot];
       for (int k = sm.ccp[c]; k < sm.ccp[c + 1]; ++k) {
         const int ct = sm.cchild[k];
-        const T f = au[ct] / Dr[ct];
+        const T f = au[ct] * Dr[ct];
         d -= al[ct] * f;
         s -= Sr[ct] * f;
       }
-      Dr[bot] = d;
+      T id = rcp(d);
+      Dr[bot] = id;
       Sr[bot] = s;
       for (int j = bot - 1; j >= top; --j) {
-        const T f = au[j + 1] / d;
+        const T f = au[j + 1] * id;
         d = Dr[j] - al[j + 1] * f;
         s = Sr[j] - s * f;
-        Dr[j] = d;
+        id = rcp(d);
+        Dr[j] = id;
         Sr[j] = s;
       }
     }
@@ -250,7 +253,7 @@ __device__ void block_solve(const JxbBlock& blk, const SimSmem<T>& sm, int rows,
       T xp = pt >= 0 ? Sr[pt] : T(0);
       T* Vr = V ? V + (size_t)r * nn : nullptr;
       for (int j = top; j <= bot; ++j) {
-        const T x = (Sr[j] - al[j] * xp) / Dr[j];
+        const T x = (Sr[j] - al[j] * xp) * Dr[j];
         Sr[j] = x;
         xp = x;
         if (Vr) Vr[j] += x;
@@ -388,8 +391,8 @@ __device__ void run_steps(const JxbSimArgs& a, const JxbBlock& blk, int row0, in
   __syncthreads();
 }
 
-template <typename T>
-__global__ void sim_forward_kernel(JxbSimArgs a) {
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) sim_forward_kernel(JxbSimArgs a) {
   extern __shared__ __align__(16) char smem_raw[];
   SimSmem<T> sm;
   sim_smem_layout<T>(a, false, &sm, smem_raw);
@@ -464,15 +467,15 @@ __device__ __forceinline__ void node_adjoint(const SimSmem<T>& sm, int j, T* x, 
   }
 }
 
-template <typename T>
-__global__ void sim_backward_kernel(JxbSimArgs a) {
+template <typename T, int NT>
+__global__ void __launch_bounds__(NT) sim_backward_kernel(JxbSimArgs a) {
   extern __shared__ __align__(16) char smem_raw[];
   SimSmem<T> sm;
   sim_smem_layout<T>(a, true, &sm, smem_raw);
   const JxbItem item = a.items[blockIdx.x];
   const JxbBlock blk = a.blocks[item.block];
   const int rows = item.n_rows, row0 = item.row0;
-  const int tid = threadIdx.x, NT = blockDim.x;
+  const int tid = threadIdx.x, nthr = blockDim.x;
   const int nn = blk.n_nodes, ns = blk.n_slots, np = blk.n_pslots;
   const T dt = T(a.dt);
   const int K = a.n_steps;
@@ -490,7 +493,7 @@ __global__ void sim_backward_kernel(JxbSimArgs a) {
     const int t = a.t0 + step;
     // Phase 1: state before the step, recording gradients at t + 1, the diagonal of
     // the step's matrix and the right-hand side of the transposed solve.
-    for (int w = tid; w < total; w += NT) {
+    for (int w = tid; w < total; w += nthr) {
       const int r = w / nn, j = w - r * nn;
       const int i = blk.node0 + j;
       const int b = row0 + r;
@@ -516,7 +519,7 @@ __global__ void sim_backward_kernel(JxbSimArgs a) {
     // lambda_r = A^{-T} lambda_v'  (solver_voltage.py:168-187).
     block_solve<T>(blk, sm, rows, sm.au, sm.al);
     // Phase 4: vector-Jacobian products of the step.
-    for (int w = tid; w < total; w += NT) {
+    for (int w = tid; w < total; w += nthr) {
       const int r = w / nn, j = w - r * nn;
       const int b = row0 + r;
       T* x = sm.st + (size_t)r * ns + sm.soff[j];
@@ -543,9 +546,9 @@ __global__ void sim_backward_kernel(JxbSimArgs a) {
   for (int r = 0; r < rows; ++r) {
     T* ga = (T*)a.adj + (size_t)(row0 + r) * a.n_slots + blk.slot0;
     const T* sa = sm.adj + (size_t)r * ns;
-    for (int q = tid; q < ns; q += NT) ga[q] = sa[q];
+    for (int q = tid; q < ns; q += nthr) ga[q] = sa[q];
   }
-  for (int q = tid; q < rows * a.n_cols; q += NT) {
+  for (int q = tid; q < rows * a.n_cols; q += nthr) {
     const int r = q / a.n_cols, c = q % a.n_cols;
     const double gv = sm.pg[q];
     if (c != 0 && gv != 0.0) atomicAdd(a.pgrad + (size_t)(row0 + r) * a.n_cols + c, gv);
@@ -564,7 +567,14 @@ int launch_sim(const JxbSimArgs& a, bool backward, cudaStream_t stream) {
     snprintf(g_err, sizeof(g_err), "threads must be a multiple of 32 up to 1024");
     return JXB_ERR_ARG;
   }
-  auto kern = backward ? sim_backward_kernel<T> : sim_forward_kernel<T>;
+  // Register budget by launch size: up to 256 threads, 512, 1024.
+  void (*kern)(JxbSimArgs);
+  if (threads <= 256)
+    kern = backward ? sim_backward_kernel<T, 256> : sim_forward_kernel<T, 256>;
+  else if (threads <= 512)
+    kern = backward ? sim_backward_kernel<T, 512> : sim_forward_kernel<T, 512>;
+  else
+    kern = backward ? sim_backward_kernel<T, 1024> : sim_forward_kernel<T, 1024>;
   cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) {
     set_err("cudaFuncSetAttribute", e);

@@ -76,6 +76,9 @@ class DeviceModel:
         cp = low.chain_cptr
         self.max_child = int(max(cp[b[4] + b[5]] - cp[b[4]] for b in blocks))
         self.threads = threads
+        self.launches = 0  # launches issued through this model (both kernels)
+        self.timed_kind: Optional[str] = None  # "forward"/"backward": record events
+        self.events: List = []
         self.set_rows_per_item(rows_per_item)
 
     def set_rows_per_item(self, rows: int) -> None:
@@ -149,18 +152,32 @@ class DeviceModel:
         a.mode = mode
         return a
 
+    def _launch(self, kind: str, fn, args, stream) -> None:
+        st = torch.cuda.current_stream(self.device)
+        s = stream if stream is not None else st.cuda_stream
+        timed = self.timed_kind == kind and stream is None
+        if timed:
+            e0 = torch.cuda.Event(enable_timing=True)
+            e0.record(st)
+        _lib.check(fn(C.byref(args), C.c_void_p(s)), f"jxb_sim_{kind}")
+        self.launches += 1
+        if timed:
+            e1 = torch.cuda.Event(enable_timing=True)
+            e1.record(st)
+            self.events.append((e0, e1, args.n_steps))
+
     def launch_forward(self, args: _lib.JxbSimArgs, stream=None) -> None:
-        lib = _lib.load()
-        s = stream if stream is not None else torch.cuda.current_stream(self.device).cuda_stream
-        _lib.check(lib.jxb_sim_forward(C.byref(args), C.c_void_p(s)), "jxb_sim_forward")
+        self._launch("forward", _lib.load().jxb_sim_forward, args, stream)
 
     def launch_backward(self, args: _lib.JxbSimArgs, stream=None) -> None:
-        lib = _lib.load()
-        s = stream if stream is not None else torch.cuda.current_stream(self.device).cuda_stream
-        _lib.check(lib.jxb_sim_backward(C.byref(args), C.c_void_p(s)), "jxb_sim_backward")
+        self._launch("backward", _lib.load().jxb_sim_backward, args, stream)
 
     def initial_state(self) -> torch.Tensor:
-        return torch.as_tensor(self.low.state0, dtype=self.dtype, device=self.device).contiguous()
+        """A fresh copy of the initial state (uploaded once, copied on the device)."""
+        if getattr(self, "_state0", None) is None:
+            self._state0 = torch.as_tensor(self.low.state0, dtype=self.dtype,
+                                           device=self.device).contiguous()
+        return self._state0.clone()
 
 
 class Simulation:

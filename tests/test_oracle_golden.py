@@ -53,3 +53,18 @@ def test_x_over_expm1_against_float64_reference():
     got = oracle.x_over_expm1(x, y)
     np.testing.assert_allclose(got, ref, rtol=1e-6)
     assert oracle.x_over_expm1(np.array(0.0), 10.0) == 10.0
+
+
+@pytest.mark.parametrize("name", ["cell_8comp_hh", "hh_tree_15x3", "l5pc_7x4_batch3", "hh_forest_6"])
+def test_torch_port_matches_oracle(name):
+    """The torch restatement used as the timed CPU baseline computes what the numpy
+    oracle computes (float64)."""
+    import torch
+
+    from oracle import torch_port
+
+    prob, extra = load_fixture(name)
+    prob.n_steps = min(prob.n_steps, 200)
+    ref = oracle.integrate(prob)
+    out = torch_port.integrate(prob, {}, dtype=torch.float64).numpy()
+    np.testing.assert_allclose(out, ref, rtol=1e-10, atol=1e-9)
