@@ -155,14 +155,16 @@ namespace jxb {
 
 template <typename T>
 struct PGradSink {
-  // Accumulates d loss / d parameter value times the parameter base, i.e. the
-  // gradient of the column scale, in float64; column 0 (fixed parameters) is skipped.
+  // Accumulates d loss / d parameter value times the parameter base (the gradient of
+  // the column scale) into the node's own slot of every trainable parameter
+  // (gk >= 0), in the precision of the run; fixed parameters are skipped. No two
+  // threads share a slot; the slots are folded into float64 columns once per launch.
   const T* base;
-  const int* col;
-  double* acc;  // per-column accumulator of this row (shared memory)
+  const int* gk;
+  T* acc;  // the node's gradient slots (shared memory)
   __device__ __forceinline__ void add(int k, T g) const {
-    int c = col[k];
-    if (c != 0) atomicAdd(acc + c, (double)(g * base[k]));
+    const int q = gk[k];
+    if (q >= 0) acc[q] += g * base[k];
   }
 };
 

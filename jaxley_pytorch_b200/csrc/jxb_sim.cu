@@ -51,6 +51,9 @@ struct SimSmem {
   int* cptr;                 // n_classes + 1 (entries of every node class)
   T* pb;                     // n_pslots (parameter bases)
   int* pc;                   // n_pslots (parameter columns)
+  int* gk;                   // n_pslots (gradient rank or -1)
+  int* gbase;                // n_nodes (first gradient slot)
+  T* gacc;                   // rows * max_gslots (adjoint only)
   // per row
   T *st, *D, *S, *pv;        // rows * (n_slots | n_nodes | n_nodes | n_pslots)
   T* V;                      // rows * n_nodes: voltages during the segment
@@ -83,6 +86,7 @@ __host__ __device__ inline size_t sim_smem_layout(const JxbSimArgs& a, bool back
   s.V = (T*)take(sizeof(T) * R * nn);
   s.X1 = backward ? (T*)take(sizeof(T) * R * nn) : nullptr;
   s.pv = (T*)take(sizeof(T) * R * np);
+  s.gacc = backward ? (T*)take(sizeof(T) * R * (size_t)a.max_gslots) : nullptr;
   s.al = (T*)take(sizeof(T) * nn);
   s.au = (T*)take(sizeof(T) * nn);
   s.dg = (T*)take(sizeof(T) * nn);
@@ -90,6 +94,8 @@ __host__ __device__ inline size_t sim_smem_layout(const JxbSimArgs& a, bool back
   s.pb = (T*)take(sizeof(T) * np);
   s.soff = (int*)take(sizeof(int) * nn);
   s.pc = (int*)take(sizeof(int) * np);
+  s.gk = (int*)take(sizeof(int) * np);
+  s.gbase = (int*)take(sizeof(int) * nn);
   s.ccp = (int*)take(sizeof(int) * (nc + 1));
   s.lp = (int*)take(sizeof(int) * (nl + 1));
   s.ents = (ChanEntry*)take(sizeof(ChanEntry) * ne);
@@ -130,6 +136,7 @@ __device__ void stage_item(const JxbSimArgs& a, const JxbBlock& blk, int row0, i
     sm.soff[j] = a.soff[i] - blk.slot0;
     sm.cls[j] = (short)cls;
     sm.poff[j] = (short)(a.poff[i] - blk.pslot0);
+    sm.gbase[j] = a.gbase[i];
     unsigned char f = comp ? FLAG_COMP : 0;
     if (a.stim_ptr[i + 1] > a.stim_ptr[i]) f |= FLAG_STIM;
     if (a.n_rec > 0 && a.rec_ptr[i + 1] > a.rec_ptr[i]) f |= FLAG_REC;
@@ -167,6 +174,7 @@ __device__ void stage_item(const JxbSimArgs& a, const JxbBlock& blk, int row0, i
   for (int q = tid; q < np; q += NT) {
     sm.pb[q] = pbase[blk.pslot0 + q];
     sm.pc[q] = a.pcol[blk.pslot0 + q];
+    sm.gk[q] = a.gk[blk.pslot0 + q];
   }
   for (int w = tid; w < rows * np; w += NT) {
     const int r = w / np, q = w % np;
@@ -185,6 +193,7 @@ __device__ void stage_item(const JxbSimArgs& a, const JxbBlock& blk, int row0, i
   }
   if (sm.pg) {
     for (int q = tid; q < rows * a.n_cols; q += NT) sm.pg[q] = 0.0;
+    for (int q = tid; q < rows * a.max_gslots; q += NT) sm.gacc[q] = T(0);
   }
 }
 
@@ -421,13 +430,14 @@ __global__ void __launch_bounds__(NT) sim_forward_kernel(JxbSimArgs a) {
 // reverse), then applies the VJPs of the currents and of every update.
 template <typename T>
 __device__ __forceinline__ void node_adjoint(const SimSmem<T>& sm, int j, T* x, T* lam,
-                                             const T* pv, double* pg, T dt, T lr, T x1,
+                                             const T* pv, T* gacc, T dt, T lr, T x1,
                                              T& lv) {
   const int cls = sm.cls[j];
   const int e0 = sm.cptr[cls], e1 = sm.cptr[cls + 1];
   const T* pn = pv + sm.poff[j];
   const T* pb = sm.pb + sm.poff[j];
-  const int* pc = sm.pc + sm.poff[j];
+  const int* pk = sm.gk + sm.poff[j];
+  T* ga = gacc + sm.gbase[j];
   const T v = x[0];
   T undo[kMaxWrites];
   short uslot[kMaxWrites];
@@ -447,7 +457,7 @@ __device__ __forceinline__ void node_adjoint(const SimSmem<T>& sm, int j, T* x, 
   // the adjoint of their previous values starts from zero.
   for (int q = e1 - 1; q >= e0; --q) {
     const ChanEntry& e = sm.ents[q];
-    PGradSink<T> G{pb + e.p[0], pc + e.p[0], pg};
+    PGradSink<T> G{pb + e.p[0], pk + e.p[0], ga};
     channel_current_vjp<T>(e, x, lam, Prm<T>{pn + e.p[0]}, G, v, lr, x1, lv);
   }
   for (int q = e0; q < e1; ++q) {
@@ -462,7 +472,7 @@ __device__ __forceinline__ void node_adjoint(const SimSmem<T>& sm, int j, T* x, 
       --nu;
       x[uslot[nu]] = undo[nu];
     }
-    PGradSink<T> G{pb + e.p[0], pc + e.p[0], pg};
+    PGradSink<T> G{pb + e.p[0], pk + e.p[0], ga};
     channel_update_vjp<T>(e, x, lam, Prm<T>{pn + e.p[0]}, G, v, dt, lv);
   }
 }
@@ -535,13 +545,27 @@ __global__ void __launch_bounds__(NT) sim_backward_kernel(JxbSimArgs a) {
       const T lrs = T(1000.0) * dt * lr / sm.cm[j];
       T lv = comp ? lr : T(0);
       lam[0] = T(0);
-      node_adjoint<T>(sm, j, x, lam, sm.pv + (size_t)r * np, sm.pg + (size_t)r * a.n_cols, dt,
-                      lrs, xnew, lv);
+      node_adjoint<T>(sm, j, x, lam, sm.pv + (size_t)r * np,
+                      sm.gacc + (size_t)r * a.max_gslots, dt, lrs, xnew, lv);
       lam[0] = lv;
       sm.X1[(size_t)r * nn + j] = x[0];
     }
     __syncthreads();
   }
+  // Fold the nodes' gradient slots into the columns (float64), once per launch.
+  for (int w = tid; w < total; w += nthr) {
+    const int r = w / nn, j = w - r * nn;
+    const int cls = sm.cls[j];
+    int npar = 0;
+    for (int q = sm.cptr[cls]; q < sm.cptr[cls + 1]; ++q) npar += sm.ents[q].np;
+    const int po = sm.poff[j];
+    const T* ga = sm.gacc + (size_t)r * a.max_gslots + sm.gbase[j];
+    for (int k = 0; k < npar; ++k) {
+      const int q = sm.gk[po + k];
+      if (q >= 0 && ga[q] != T(0)) atomicAdd(sm.pg + (size_t)r * a.n_cols + sm.pc[po + k], (double)ga[q]);
+    }
+  }
+  __syncthreads();
   // Adjoint of the segment's initial state, and the parameter gradients.
   for (int r = 0; r < rows; ++r) {
     T* ga = (T*)a.adj + (size_t)(row0 + r) * a.n_slots + blk.slot0;
@@ -597,7 +621,7 @@ static int check_sim_args(const JxbSimArgs* a, bool backward) {
       !a->cls_ptr || !a->cls_comp || !a->entries || !a->pbase || !a->pcol || !a->pscale ||
       !a->blocks || !a->items || !a->chain_top || !a->chain_len || !a->chain_ptop ||
       !a->chain_cptr || !a->level_ptr || !a->stim_ptr || !a->state || !a->area ||
-      !a->parent || !a->kid_ptr || !a->kid) {
+      !a->parent || !a->kid_ptr || !a->kid || !a->gk || !a->gbase) {
     snprintf(g_err, sizeof(g_err), "null pointer in JxbSimArgs");
     return JXB_ERR_ARG;
   }

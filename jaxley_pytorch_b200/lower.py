@@ -62,6 +62,9 @@ class Lowered:
     stim_ptr: np.ndarray
     stim_idx: np.ndarray
     stim: Optional[np.ndarray]  # (steps, rows, n_stim) time-major
+    gk: np.ndarray  # (n_pslots,) rank of a trainable parameter in its run, -1 if fixed
+    gbase: np.ndarray  # (n_nodes,) first gradient slot of a node (block-relative)
+    max_gslots: int  # largest number of gradient slots of a block
     parent: np.ndarray  # (n_nodes,) parent in internal order, -1 for roots
     kid_ptr: np.ndarray  # (n_nodes+1,) children CSR (internal order)
     kid: np.ndarray
@@ -400,6 +403,35 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
     def i32(x):
         return np.ascontiguousarray(np.asarray(x, dtype=np.int32))
 
+    # ---- gradient slots: every node owns one float32 accumulator per trainable
+    # parameter (column != 0) for the adjoint kernel ----
+    pcol_arr = np.asarray(pcol, dtype=np.int64)
+    gk = np.full(len(pcol_arr), -1, dtype=np.int32)
+    run_len = np.zeros(n, dtype=np.int64)
+    for i in range(n):
+        run_len[i] = len(node_pb[i])
+    done_runs = set()
+    for i in range(n):
+        st0 = int(poff[i])
+        key = (st0, int(run_len[i]))  # empty runs share their start with the next run
+        if key in done_runs:
+            continue
+        done_runs.add(key)
+        rk = 0
+        for q in range(st0, st0 + int(run_len[i])):
+            if pcol_arr[q] != 0:
+                gk[q] = rk
+                rk += 1
+    gbase = np.zeros(n, dtype=np.int32)
+    max_gslots = 0
+    for (n0, n1) in blocks_nodes:
+        acc = 0
+        for i in range(n0, n1):
+            gbase[i] = acc
+            st0 = int(poff[i])
+            acc += int(np.count_nonzero(pcol_arr[st0:st0 + int(run_len[i])]))
+        max_gslots = max(max_gslots, acc)
+
     # ---- parent / children in internal order (for the delta form of the step) ----
     par_int = np.full(n, -1, dtype=np.int64)
     ps = np.asarray(parent_solve, dtype=np.int64)[order]
@@ -445,6 +477,9 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
         stim_ptr=stim_ptr,
         stim_idx=stim_idx,
         stim=stim,
+        gk=gk,
+        gbase=gbase,
+        max_gslots=int(max_gslots),
         parent=i32(par_int),
         kid_ptr=kid_ptr,
         kid=kid,

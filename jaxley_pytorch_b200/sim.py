@@ -60,6 +60,7 @@ class DeviceModel:
             "chain_child": i(low.chain_child) if len(low.chain_child) else i(np.zeros(1)),
             "level_ptr": i(low.level_ptr), "stim_ptr": i(low.stim_ptr),
             "stim_idx": i(low.stim_idx) if len(low.stim_idx) else i(np.zeros(1)),
+            "gk": i(low.gk) if len(low.gk) else i(np.zeros(1)), "gbase": i(low.gbase),
             "rec_ptr": i(low.rec_ptr), "parent": i(low.parent), "kid_ptr": i(low.kid_ptr),
             "kid": i(low.kid) if len(low.kid) else i(np.zeros(1)),
             "rec_slot": i(low.rec_slot) if len(low.rec_slot) else i(np.zeros(1)),
@@ -120,11 +121,13 @@ class DeviceModel:
         a.max_levels = self.max_levels
         a.max_pslots = self.max_pslots
         a.threads = self.threads
+        a.max_gslots = max(1, low.max_gslots)
         a.dt = low.dt
         for k in ["node_class", "soff", "poff", "a_low", "a_up", "gsum", "cm", "cls_ptr",
                   "cls_comp", "entries", "pbase", "pcol", "blocks", "chain_top", "chain_len",
                   "chain_ptop", "chain_cptr", "chain_child", "level_ptr", "stim_ptr", "stim_idx",
-                  "area", "rec_ptr", "rec_slot", "rec_col", "parent", "kid_ptr", "kid"]:
+                  "area", "rec_ptr", "rec_slot", "rec_col", "parent", "kid_ptr", "kid",
+                  "gk", "gbase"]:
             setattr(a, k, t[k].data_ptr())
         a.items = (items if items is not None else self.items).data_ptr()
         if items is not None:

@@ -59,3 +59,17 @@ def test_library_exports_every_declared_symbol():
     lib = ctypes.CDLL(_lib.LIB_PATH)
     for name in declared:
         assert hasattr(lib, name), name
+
+
+@pytest.mark.parametrize("name", fixture_names())
+def test_every_batched_parameter_has_a_gradient_slot(name):
+    prob, _ = load_fixture(name)
+    low = lower(prob)
+    for i in range(low.n_nodes):
+        cls = low.node_class[i]
+        npar = sum(int(e[2]) for e in low.entries[low.cls_ptr[cls]:low.cls_ptr[cls + 1]])
+        run = slice(low.poff[i], low.poff[i] + npar)
+        cols, gk = low.pcol[run], low.gk[run]
+        assert np.all((cols != 0) == (gk >= 0))
+        if npar:
+            assert sorted(gk[gk >= 0].tolist()) == list(range(int(np.count_nonzero(cols))))
