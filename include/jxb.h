@@ -173,6 +173,7 @@ typedef struct {
   void* ckpt;                 /* optional (n_ckpt, batch, n_slots): state at t0 + m*ckpt_every */
   int32_t ckpt_every, ckpt_base;  /* ckpt index of t0 is (t0 - ckpt_base) / ckpt_every */
   void* traj;                 /* optional (n_steps, batch, n_slots): state before each step */
+  void* traj_piv;             /* adjoint: (n_steps, batch, n_nodes) reciprocal pivots */
   /* adjoint */
   void* adj;                  /* (batch, n_slots) adjoint of the state, updated in place */
   const void* rec_grad;       /* (T + 1, batch, n_rec) gradient of the recordings */

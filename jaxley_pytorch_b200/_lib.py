@@ -66,7 +66,7 @@ class JxbSimArgs(C.Structure):
         ("n_rec", C.c_int32), ("pad1", C.c_int32),
         ("state", _p), ("ckpt", _p),
         ("ckpt_every", C.c_int32), ("ckpt_base", C.c_int32),
-        ("traj", _p),
+        ("traj", _p), ("traj_piv", _p),
         ("adj", _p), ("rec_grad", _p), ("pgrad", _p),
         ("mode", C.c_int32), ("pad2", C.c_int32),
     ]

@@ -352,3 +352,108 @@ __device__ __forceinline__ int update_writes(const ChanEntry& e, short* out) {
 }
 
 }  // namespace jxb
+
+namespace jxb {
+
+// Undo log of one node's channel updates for the adjoint: the slot, its value before
+// the update, d new / d old and d new / d (v or the second input).
+template <typename T, int N>
+struct UndoLog {
+  T old[N], dx[N], dy[N];
+  short slot[N];
+  int n = 0;
+  __device__ __forceinline__ void push(short s, T o, T a, T b) {
+    if (n < N) {
+      slot[n] = s;
+      old[n] = o;
+      dx[n] = a;
+      dy[n] = b;
+      ++n;
+    }
+  }
+};
+
+// Gate step with its derivatives (dual number in v), logged.
+template <typename T, int N>
+__device__ __forceinline__ void gate_logged(int g, T v, T* x, short s, T dt, UndoLog<T, N>& L) {
+  T e;
+  Dual<T> xn = gate_step<Dual<T>, T>(g, Dual<T>(v, T(1)), x[s], dt, &e);
+  L.push(s, x[s], e, xn.d);
+  x[s] = xn.v;
+}
+
+// `channel_update` that logs every overwritten slot with the partial derivatives
+// the reverse pass needs, so that the rate functions are evaluated once per step.
+template <typename T, int N>
+__device__ __forceinline__ void channel_update_logged(const ChanEntry& e, T* x, const Prm<T>& P,
+                                                      T v, T dt, UndoLog<T, N>& L) {
+  switch (e.type) {
+    case CH_HH:
+      gate_logged<T, N>(G_HH_M, v, x, e.s[0], dt, L);
+      gate_logged<T, N>(G_HH_H, v, x, e.s[1], dt, L);
+      gate_logged<T, N>(G_HH_N, v, x, e.s[2], dt, L);
+      break;
+    case CH_LEAK:
+      break;
+    case CH_SKE2: {
+      const T em1 = save_expm1(T(-1.0) / T(1.0) * dt);
+      Dual<T> zi = ske2_zinf<Dual<T>>(Dual<T>(x[e.s[1]], T(1)));
+      const T z = x[e.s[0]];
+      L.push(e.s[0], z, T(1) + em1, -em1 * zi.d);
+      x[e.s[0]] = z + (z - zi.v) * em1;
+      break;
+    }
+    case CH_CAPUMP:
+    case CH_CANERNST:
+      L.push(e.s[0], x[e.s[0]], T(0), T(0));
+      channel_update<T>(e, x, P, v, dt);
+      break;
+    default: {
+      GateLayout gl = gate_layout(e.type);
+      gate_logged<T, N>(gl.g0, v, x, e.s[0], dt, L);
+      if (gl.g1 >= 0) gate_logged<T, N>(gl.g1, v, x, e.s[1], dt, L);
+      break;
+    }
+  }
+}
+
+// Reverse of `channel_update_logged`: restores the entry's slots from the log and
+// applies its vector-Jacobian product.
+template <typename T, int N>
+__device__ __forceinline__ void channel_update_vjp_logged(const ChanEntry& e, T* x, T* lam,
+                                                          const Prm<T>& P, const PGradSink<T>& G,
+                                                          T v, T dt, T& lv, UndoLog<T, N>& L) {
+  switch (e.type) {
+    case CH_LEAK:
+      break;
+    case CH_SKE2: {
+      --L.n;
+      x[L.slot[L.n]] = L.old[L.n];
+      const T lz = lam[e.s[0]];
+      lam[e.s[0]] = L.dx[L.n] * lz;
+      lam[e.s[1]] += L.dy[L.n] * lz;
+      break;
+    }
+    case CH_CAPUMP:
+    case CH_CANERNST:
+      --L.n;
+      x[L.slot[L.n]] = L.old[L.n];
+      channel_update_vjp<T>(e, x, lam, P, G, v, dt, lv);
+      break;
+    default: {
+      // Gates: pop in reverse order of the pushes.
+      int ng = e.type == CH_HH ? 3 : (gate_layout(e.type).g1 >= 0 ? 2 : 1);
+      for (int k = 0; k < ng; ++k) {
+        --L.n;
+        const short s = L.slot[L.n];
+        x[s] = L.old[L.n];
+        const T ln = lam[s];
+        lam[s] = L.dx[L.n] * ln;
+        lv += L.dy[L.n] * ln;
+      }
+      break;
+    }
+  }
+}
+
+}  // namespace jxb

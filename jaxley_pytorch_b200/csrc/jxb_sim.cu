@@ -335,7 +335,7 @@ __device__ __forceinline__ void record_node(const JxbSimArgs& a, int i, const T*
 template <typename T>
 __device__ void run_steps(const JxbSimArgs& a, const JxbBlock& blk, int row0, int rows,
                           const SimSmem<T>& sm, T dt, int t0, int nsteps, int mode, bool record,
-                          bool ckpt, T* traj, T* X1) {
+                          bool ckpt, T* traj, T* X1, T* piv = nullptr) {
   const int tid = threadIdx.x, NT = blockDim.x;
   const int nn = blk.n_nodes, ns = blk.n_slots, np = blk.n_pslots;
   const int total = nn * rows;
@@ -350,6 +350,8 @@ __device__ void run_steps(const JxbSimArgs& a, const JxbBlock& blk, int row0, in
       const unsigned char f = sm.flags[j];
       const T* Vr = sm.V + (size_t)r * nn;
       if (step > 0) x[0] = Vr[j];
+      if (piv && step > 0)  // reciprocal pivots of the previous step's elimination
+        piv[((size_t)(step - 1) * a.batch + b) * a.n_nodes + i] = sm.D[(size_t)r * nn + j];
       if (record && step > 0 && (f & FLAG_REC)) record_node<T>(a, i, x, b, t);
       if (step == nsteps) {
         if (mode != 0) {
@@ -426,8 +428,10 @@ __global__ void __launch_bounds__(NT) sim_forward_kernel(JxbSimArgs a) {
 }
 
 // Adjoint of one node and row for one step: replays the channel updates from the
-// pre-step state `x` (restored afterwards from the undo log, one entry at a time, in
-// reverse), then applies the VJPs of the currents and of every update.
+// pre-step state `x`, logging every overwritten slot with its partial derivatives
+// (one evaluation of the rate functions, in dual arithmetic), then applies the VJPs
+// of the currents at the updated state and of the updates in reverse order,
+// restoring `x` from the log.
 template <typename T>
 __device__ __forceinline__ void node_adjoint(const SimSmem<T>& sm, int j, T* x, T* lam,
                                              const T* pv, T* gacc, T dt, T lr, T x1,
@@ -439,41 +443,77 @@ __device__ __forceinline__ void node_adjoint(const SimSmem<T>& sm, int j, T* x, 
   const int* pk = sm.gk + sm.poff[j];
   T* ga = gacc + sm.gbase[j];
   const T v = x[0];
-  T undo[kMaxWrites];
-  short uslot[kMaxWrites];
-  int nu = 0;
+  UndoLog<T, kMaxWrites> L;
   for (int q = e0; q < e1; ++q) {
     const ChanEntry& e = sm.ents[q];
-    short w[4];
-    const int nw = update_writes(e, w);
-    for (int k = 0; k < nw && nu < kMaxWrites; ++k) {
-      uslot[nu] = w[k];
-      undo[nu] = x[w[k]];
-      ++nu;
-    }
-    channel_update<T>(e, x, Prm<T>{pn + e.p[0]}, v, dt);
+    channel_update_logged<T, kMaxWrites>(e, x, Prm<T>{pn + e.p[0]}, v, dt, L);
   }
-  // Currents at the updated state; their slots were overwritten by the step, so
-  // the adjoint of their previous values starts from zero.
   for (int q = e1 - 1; q >= e0; --q) {
     const ChanEntry& e = sm.ents[q];
     PGradSink<T> G{pb + e.p[0], pk + e.p[0], ga};
     channel_current_vjp<T>(e, x, lam, Prm<T>{pn + e.p[0]}, G, v, lr, x1, lv);
   }
+  // The step overwrote the current slots, so the adjoint of their previous values
+  // starts from zero.
   for (int q = e0; q < e1; ++q) {
     const int c = sm.ents[q].cur;
     if (c >= 0) lam[c] = T(0);
   }
   for (int q = e1 - 1; q >= e0; --q) {
     const ChanEntry& e = sm.ents[q];
-    short w[4];
-    const int nw = update_writes(e, w);
-    for (int k = nw - 1; k >= 0; --k) {
-      --nu;
-      x[uslot[nu]] = undo[nu];
-    }
     PGradSink<T> G{pb + e.p[0], pk + e.p[0], ga};
-    channel_update_vjp<T>(e, x, lam, Prm<T>{pn + e.p[0]}, G, v, dt, lv);
+    channel_update_vjp_logged<T, kMaxWrites>(e, x, lam, Prm<T>{pn + e.p[0]}, G, v, dt, lv, L);
+  }
+}
+
+// Transposed solve with the reciprocal pivots of the forward elimination (the
+// pivots of A and A^T coincide): only the right-hand side is eliminated.
+template <typename T>
+__device__ void block_solve_pivots(const JxbBlock& blk, const SimSmem<T>& sm, int rows,
+                                   const T* al, const T* au) {
+  const int tid = threadIdx.x, NT = blockDim.x;
+  const int nn = blk.n_nodes;
+  const int nlev = blk.n_levels;
+  for (int h = 0; h < nlev; ++h) {
+    const int c0 = sm.lp[h], nch = sm.lp[h + 1] - c0;
+    for (int w = tid; w < nch * rows; w += NT) {
+      const int c = c0 + w % nch;
+      const int r = w / nch;
+      const T* Dr = sm.D + (size_t)r * nn;
+      T* Sr = sm.S + (size_t)r * nn;
+      const int top = sm.ctop[c];
+      const int bot = top + sm.clen[c] - 1;
+      T s = Sr[bot];
+      for (int k = sm.ccp[c]; k < sm.ccp[c + 1]; ++k) {
+        const int ct = sm.cchild[k];
+        s -= Sr[ct] * (au[ct] * Dr[ct]);
+      }
+      Sr[bot] = s;
+      for (int j = bot - 1; j >= top; --j) {
+        s = Sr[j] - s * (au[j + 1] * Dr[j + 1]);
+        Sr[j] = s;
+      }
+    }
+    __syncthreads();
+  }
+  for (int h = nlev - 1; h >= 0; --h) {
+    const int c0 = sm.lp[h], nch = sm.lp[h + 1] - c0;
+    for (int w = tid; w < nch * rows; w += NT) {
+      const int c = c0 + w % nch;
+      const int r = w / nch;
+      const T* Dr = sm.D + (size_t)r * nn;
+      T* Sr = sm.S + (size_t)r * nn;
+      const int top = sm.ctop[c];
+      const int bot = top + sm.clen[c] - 1;
+      const int pt = sm.cptop[c];
+      T xp = pt >= 0 ? Sr[pt] : T(0);
+      for (int j = top; j <= bot; ++j) {
+        const T x = (Sr[j] - al[j] * xp) * Dr[j];
+        Sr[j] = x;
+        xp = x;
+      }
+    }
+    __syncthreads();
   }
 }
 
@@ -495,23 +535,20 @@ __global__ void __launch_bounds__(NT) sim_backward_kernel(JxbSimArgs a) {
   __syncthreads();
   init_voltages<T>(blk, sm, rows);
   __syncthreads();
-  run_steps<T>(a, blk, row0, rows, sm, dt, a.t0, K, 0, false, false, traj, sm.X1);
+  T* piv = (T*)a.traj_piv;
+  run_steps<T>(a, blk, row0, rows, sm, dt, a.t0, K, 0, false, false, traj, sm.X1, piv);
 
   const T* rec_grad = (const T*)a.rec_grad;
   const int total = nn * rows;
   for (int step = K - 1; step >= 0; --step) {
     const int t = a.t0 + step;
-    // Phase 1: state before the step, recording gradients at t + 1, the diagonal of
-    // the step's matrix and the right-hand side of the transposed solve.
+    // Phase 1: recording gradients at t + 1, the pivots of the step's matrix and the
+    // right-hand side of the transposed solve.
     for (int w = tid; w < total; w += nthr) {
       const int r = w / nn, j = w - r * nn;
       const int i = blk.node0 + j;
       const int b = row0 + r;
-      T* x = sm.st + (size_t)r * ns + sm.soff[j];
       T* lam = sm.adj + (size_t)r * ns + sm.soff[j];
-      const int nslot = (j + 1 < nn ? sm.soff[j + 1] : ns) - sm.soff[j];
-      const T* g = traj + ((size_t)step * a.batch + b) * a.n_slots + blk.slot0 + sm.soff[j];
-      for (int q = 0; q < nslot; ++q) x[q] = g[q];
       const unsigned char f = sm.flags[j];
       if (rec_grad && (f & FLAG_REC)) {
         for (int q = a.rec_ptr[i]; q < a.rec_ptr[i + 1]; ++q) {
@@ -519,15 +556,13 @@ __global__ void __launch_bounds__(NT) sim_backward_kernel(JxbSimArgs a) {
           if (sl >= 0) lam[sl] += rec_grad[((size_t)(t + 1) * a.batch + b) * a.n_rec + a.rec_col[q]];
         }
       }
-      T lin, cst;
-      node_channels<T>(sm, j, x, sm.pv + (size_t)r * np, dt, 0, lin, cst);
-      if (a.syn_lin) lin += ((const T*)a.syn_lin)[(size_t)b * a.n_nodes + i];
-      sm.D[(size_t)r * nn + j] = sm.dg[j] + dt * (lin / sm.cm[j]);
+      sm.D[(size_t)r * nn + j] = piv[((size_t)step * a.batch + b) * a.n_nodes + i];
       sm.S[(size_t)r * nn + j] = lam[0];
     }
     __syncthreads();
-    // lambda_r = A^{-T} lambda_v'  (solver_voltage.py:168-187).
-    block_solve<T>(blk, sm, rows, sm.au, sm.al);
+    // lambda_r = A^{-T} lambda_v'  (solver_voltage.py:168-187), with the pivots of
+    // the forward elimination.
+    block_solve_pivots<T>(blk, sm, rows, sm.au, sm.al);
     // Phase 4: vector-Jacobian products of the step.
     for (int w = tid; w < total; w += nthr) {
       const int r = w / nn, j = w - r * nn;
@@ -651,8 +686,9 @@ static int check_sim_args(const JxbSimArgs* a, bool backward) {
     return JXB_ERR_ARG;
   }
   if (backward) {
-    if (!a->ckpt || !a->traj || !a->adj || !a->pgrad || a->mode != 0 || a->n_steps <= 0) {
-      snprintf(g_err, sizeof(g_err), "adjoint needs ckpt, traj, adj, pgrad and n_steps > 0");
+    if (!a->ckpt || !a->traj || !a->traj_piv || !a->adj || !a->pgrad || a->mode != 0 ||
+        a->n_steps <= 0) {
+      snprintf(g_err, sizeof(g_err), "adjoint needs ckpt, traj, traj_piv, adj, pgrad and n_steps > 0");
       return JXB_ERR_ARG;
     }
   }

@@ -237,6 +237,7 @@ class Simulation:
         adj = torch.zeros((low.batch, low.n_slots), dtype=m.dtype, device=m.device)
         pgrad = torch.zeros((low.batch, low.n_cols), dtype=torch.float64, device=m.device)
         traj = torch.empty((min(K, T), low.batch, low.n_slots), dtype=m.dtype, device=m.device)
+        piv = torch.empty((min(K, T), low.batch, low.n_nodes), dtype=m.dtype, device=m.device)
         rec_grad = rec_grad.contiguous()
         for sgi in range(nseg - 1, -1, -1):
             t0 = sgi * K
@@ -244,6 +245,7 @@ class Simulation:
             a = m.args(ckpt[sgi], k, t0, None, pscale=pscale, traj=traj, adj=adj,
                        rec_grad=rec_grad, pgrad=pgrad)
             a.ckpt = ckpt[sgi].data_ptr()
+            a.traj_piv = piv.data_ptr()
             m.launch_backward(a)
         return pgrad
 
