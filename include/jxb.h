@@ -134,6 +134,7 @@ typedef struct {
   const void* cm;             /* (n_nodes,) capacitance */
   const int32_t* cls_ptr;     /* (n_classes+1,) entries of every node class */
   const int32_t* cls_comp;    /* (n_classes,) 1 for compartments, 0 for branchpoints */
+  const int32_t* cls_prog;    /* (n_classes,) compile-time program id, 0 = interpreted */
   const void* entries;        /* channel entries (16-bit fields, see jxb_channels.cuh) */
   int32_t n_classes, n_entries;
   const void* pbase;          /* (n_pslots,) */

@@ -51,7 +51,7 @@ class JxbSimArgs(C.Structure):
         ("dt", C.c_double),
         ("node_class", _p), ("soff", _p), ("poff", _p),
         ("a_low", _p), ("a_up", _p), ("gsum", _p), ("cm", _p),
-        ("cls_ptr", _p), ("cls_comp", _p), ("entries", _p),
+        ("cls_ptr", _p), ("cls_comp", _p), ("cls_prog", _p), ("entries", _p),
         ("n_classes", C.c_int32), ("n_entries", C.c_int32),
         ("pbase", _p), ("pcol", _p), ("pscale", _p),
         ("blocks", _p), ("items", _p),

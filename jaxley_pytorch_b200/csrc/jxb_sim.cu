@@ -23,6 +23,7 @@
 
 #include "jxb.h"
 #include "jxb_node.cuh"
+#include "jxb_prog.cuh"
 
 namespace jxb {
 
@@ -49,6 +50,7 @@ struct SimSmem {
   short *par, *kptr, *kids;  // parent, children CSR (block-relative)
   ChanEntry* ents;
   int* cptr;                 // n_classes + 1 (entries of every node class)
+  int* cprog;                // n_classes (compile-time program or PROG_GENERIC)
   T* pb;                     // n_pslots (parameter bases)
   int* pc;                   // n_pslots (parameter columns)
   int* gk;                   // n_pslots (gradient rank or -1)
@@ -100,6 +102,7 @@ __host__ __device__ inline size_t sim_smem_layout(const JxbSimArgs& a, bool back
   s.lp = (int*)take(sizeof(int) * (nl + 1));
   s.ents = (ChanEntry*)take(sizeof(ChanEntry) * ne);
   s.cptr = (int*)take(sizeof(int) * (a.n_classes + 1));
+  s.cprog = (int*)take(sizeof(int) * a.n_classes);
   s.cls = (short*)take(sizeof(short) * nn);
   s.poff = (short*)take(sizeof(short) * nn);
   s.ctop = (short*)take(sizeof(short) * nc);
@@ -168,6 +171,7 @@ __device__ void stage_item(const JxbSimArgs& a, const JxbBlock& blk, int row0, i
   const int nshort = a.n_entries * (int)(sizeof(ChanEntry) / sizeof(short));
   for (int q = tid; q < nshort; q += NT) dst[q] = src[q];
   for (int q = tid; q <= a.n_classes; q += NT) sm.cptr[q] = a.cls_ptr[q];
+  for (int q = tid; q < a.n_classes; q += NT) sm.cprog[q] = a.cls_prog ? a.cls_prog[q] : 0;
   const int np = blk.n_pslots;
   const T* pbase = (const T*)a.pbase;
   const T* pscale = (const T*)a.pscale;
@@ -283,6 +287,17 @@ __device__ __forceinline__ void node_channels(const SimSmem<T>& sm, int j, T* x,
   const T* pn = pv + sm.poff[j];
   const T v = x[0];
   lin = cst = T(0);
+  if (mode == 0) {
+    const int prog = sm.cprog[cls];
+    if (prog == PROG_L5PC_DEND) {
+      ProgL5pcDend<T>::forward(x, pn, dt, lin, cst);
+      return;
+    }
+    if (prog == PROG_HH) {
+      ProgHH<T>::forward(x, pn, dt, lin, cst);
+      return;
+    }
+  }
   if (mode == 2) {
     for (int q = e0; q < e1; ++q) channel_steady<T>(sm.ents[q], x, v);
     return;
@@ -442,6 +457,16 @@ __device__ __forceinline__ void node_adjoint(const SimSmem<T>& sm, int j, T* x, 
   const T* pb = sm.pb + sm.poff[j];
   const int* pk = sm.gk + sm.poff[j];
   T* ga = gacc + sm.gbase[j];
+  const int prog = sm.cprog[cls];
+  if (prog != PROG_GENERIC) {
+    AdjCtx<T> c{lam, pb, pk, ga, lr, x1, lv};
+    if (prog == PROG_L5PC_DEND)
+      ProgL5pcDend<T>::adjoint(x, pn, dt, c);
+    else
+      ProgHH<T>::adjoint(x, pn, dt, c);
+    lv = c.lv;
+    return;
+  }
   const T v = x[0];
   UndoLog<T, kMaxWrites> L;
   for (int q = e0; q < e1; ++q) {

@@ -44,6 +44,7 @@ class Lowered:
     poff: np.ndarray  # (n_nodes,) first parameter slot of every node (shared runs)
     cls_ptr: np.ndarray
     cls_comp: np.ndarray
+    cls_prog: np.ndarray  # (n_classes,) compile-time program id (0 = interpreted)
     entries: np.ndarray  # (n_entries, 18) int16
     pbase: np.ndarray
     pcol: np.ndarray
@@ -169,6 +170,32 @@ def pack_blocks(tree_ptr: np.ndarray, max_nodes: int, weights: Optional[np.ndarr
             s = a
     blocks.append((s, int(tree_ptr[-1])))
     return blocks
+
+
+# Compile-time programs of csrc/jxb_prog.cuh: channel type sequence -> id. A class
+# runs one only if its slots and parameters have the program's consecutive layout.
+PROGRAMS = {
+    (SPECS["HH"].type_id,): 1,
+    tuple(SPECS[t].type_id for t in ["NaTs2T", "SKv3_1", "M", "H", "Leak"]): 2,
+}
+
+
+def program_of(ents: np.ndarray) -> int:
+    if len(ents) == 0:
+        return 0
+    prog = PROGRAMS.get(tuple(int(e[0]) for e in ents), 0)
+    if not prog:
+        return 0
+    slot, par = 1, 0
+    for e in ents:
+        ns, npar, cur = int(e[1]), int(e[2]), int(e[3])
+        if cur >= 0 or int(e[10]) != par:
+            return 0
+        if any(int(e[4 + q]) != slot + q for q in range(ns)):
+            return 0
+        slot += ns
+        par += npar
+    return prog
 
 
 def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
@@ -303,6 +330,7 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
         node_pb.append(pbs)
         node_pc.append(pcs)
         slot_names.append(names)
+    cls_prog = np.asarray([program_of(e) for e in cls_entries], dtype=np.int32)
     cls_ptr = np.zeros(len(cls_entries) + 1, dtype=np.int32)
     for c, e in enumerate(cls_entries):
         cls_ptr[c + 1] = cls_ptr[c] + len(e)
@@ -461,6 +489,7 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
         poff=i32(poff),
         cls_ptr=i32(cls_ptr),
         cls_comp=i32(cls_comp),
+        cls_prog=cls_prog,
         entries=np.ascontiguousarray(entries),
         pbase=np.asarray(pbase, dtype=np.float64),
         pcol=i32(pcol),

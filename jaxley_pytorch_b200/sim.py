@@ -36,7 +36,7 @@ class DeviceModel:
     """A lowered model resident on one GPU."""
 
     def __init__(self, low: Lowered, dtype: torch.dtype = torch.float32, device="cuda",
-                 rows_per_item: int = 1, threads: int = 256):
+                 rows_per_item: int = 1, threads: int = 256, programs: bool = True):
         self.low = low
         self.dtype = dtype
         self.device = torch.device(device)
@@ -53,6 +53,7 @@ class DeviceModel:
             "node_class": i(low.node_class), "soff": i(low.soff), "poff": i(low.poff),
             "a_low": f(low.a_low), "a_up": f(low.a_up), "gsum": f(low.gsum), "cm": f(low.cm),
             "area": f(low.area), "cls_ptr": i(low.cls_ptr), "cls_comp": i(low.cls_comp),
+            "cls_prog": i(low.cls_prog),
             "entries": torch.as_tensor(low.entries.astype(np.int16), device=dev).contiguous(),
             "pbase": f(low.pbase), "pcol": i(low.pcol), "blocks": i(low.blocks),
             "chain_top": i(low.chain_top), "chain_len": i(low.chain_len),
@@ -66,6 +67,8 @@ class DeviceModel:
             "rec_slot": i(low.rec_slot) if len(low.rec_slot) else i(np.zeros(1)),
             "rec_col": i(low.rec_col) if len(low.rec_col) else i(np.zeros(1)),
         }
+        if not programs:
+            self.t["cls_prog"] = torch.zeros_like(self.t["cls_prog"])
         self.pscale = f(low.pscale)
         self.stim = f(low.stim) if low.stim is not None else None
         blocks = low.blocks
@@ -124,7 +127,7 @@ class DeviceModel:
         a.max_gslots = max(1, low.max_gslots)
         a.dt = low.dt
         for k in ["node_class", "soff", "poff", "a_low", "a_up", "gsum", "cm", "cls_ptr",
-                  "cls_comp", "entries", "pbase", "pcol", "blocks", "chain_top", "chain_len",
+                  "cls_comp", "cls_prog", "entries", "pbase", "pcol", "blocks", "chain_top", "chain_len",
                   "chain_ptop", "chain_cptr", "chain_child", "level_ptr", "stim_ptr", "stim_idx",
                   "area", "rec_ptr", "rec_slot", "rec_col", "parent", "kid_ptr", "kid",
                   "gk", "gbase"]:
@@ -196,11 +199,12 @@ class Simulation:
                  max_block_nodes: int = 4096, rows_per_item: int = 1,
                  segment: Optional[int] = None, init_steady: bool = False,
                  low: Optional[Lowered] = None, checkpoint: int = 100, threads: int = 256,
-                 keep_currents: bool = True):
+                 keep_currents: bool = True, programs: bool = True):
         self.problem = problem
         self.low = low if low is not None else lower(problem, max_block_nodes=max_block_nodes,
                                                      keep_currents=keep_currents)
-        self.model = DeviceModel(self.low, dtype, device, rows_per_item, threads=threads)
+        self.model = DeviceModel(self.low, dtype, device, rows_per_item, threads=threads,
+                                 programs=programs)
         self.segment = segment
         self.init_steady = init_steady
         self.checkpoint = int(checkpoint)

@@ -127,3 +127,27 @@ def test_fp32_spiking_error_is_bounded(cuda_device):
     assert vmax > 0.0
     assert dv <= 2.0, dv
     assert rel <= 5e-2, rel
+
+
+@pytest.mark.parametrize("name", ["cell_8comp_hh", "hh_tree_15x3", "hh_forest_6", "synth_l5pc_15x4",
+                                  "l5pc_7x4_batch3"])
+def test_compile_time_programs_match_interpreter(cuda_device, name):
+    """Node classes that run a compile-time channel program (csrc/jxb_prog.cuh) give
+    the interpreter's results, forward and adjoint (float64)."""
+    prob, extra = load_fixture(name)
+    prob.n_steps = min(prob.n_steps, 150)
+    steady = bool(extra.get("init_steady", 0))
+    res = []
+    for programs in (True, False):
+        sim = Simulation(prob, dtype=torch.float64, device=cuda_device, checkpoint=40,
+                         init_steady=steady, keep_currents=False, programs=programs)
+        W = torch.as_tensor(_loss_weights((prob.batch, sim.low.n_rec, prob.n_steps + 1), 2),
+                            device=cuda_device)
+        ps = sim.model.pscale.clone().requires_grad_(True)
+        out = sim.run(pscale=ps)
+        (out * W).sum().backward()
+        res.append((out.detach(), ps.grad))
+        if programs and name != "l5pc_7x4_batch3":
+            assert int(sim.low.cls_prog.max()) > 0  # the program path is exercised
+    torch.testing.assert_close(res[0][0], res[1][0], rtol=1e-12, atol=1e-10)
+    torch.testing.assert_close(res[0][1], res[1][1], rtol=1e-10, atol=1e-12)
