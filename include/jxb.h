@@ -184,6 +184,19 @@ typedef struct {
 
 int jxb_sim_forward(const JxbSimArgs* args, void* stream);
 int jxb_sim_backward(const JxbSimArgs* args, void* stream);
+
+/* jxb_sim_backward without caller scratch: no counterpart in the reference. For
+ * callers that cannot allocate device memory during the simulation (buffers handed
+ * over from a host-owned memory pool, or a plugin whose framework allocator must not
+ * be re-entered from a step). The trajectory scratch (args->traj, args->traj_piv are
+ * ignored) lives in a fixed 32 MiB device array of the library, held by every GPU
+ * that loads it until exit; segments needing more return JXB_ERR_TOO_LARGE. The first
+ * call on a device looks up the array's device address (cudaGetSymbolAddress) with
+ * that device current and should come before any stream capture. All calls share the
+ * array: calls that overlap on the GPU (other streams, other threads) race. Nothing
+ * in the array needs to start at zero: every slot a segment reads was written earlier
+ * in the same launch. It calls no cudaMalloc, cudaFree or allocating library routine. */
+int jxb_sim_backward_noalloc(const JxbSimArgs* args, void* stream);
 int64_t jxb_sim_smem_bytes(const JxbSimArgs* args, int backward);
 
 /* ---------------------------------------------------------------------------------

@@ -92,6 +92,7 @@ EXPORTED = [
     "jxb_tree_solve_registers",
     "jxb_sim_forward",
     "jxb_sim_backward",
+    "jxb_sim_backward_noalloc",
     "jxb_sim_smem_bytes",
     "jxb_synapse_forward",
     "jxb_synapse_backward",
@@ -116,7 +117,7 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.jxb_version.restype = C.c_int
     lib.jxb_sim_smem_bytes.restype = C.c_int64
     lib.jxb_sim_smem_bytes.argtypes = [C.POINTER(JxbSimArgs), C.c_int]
-    for name in ["jxb_sim_forward", "jxb_sim_backward"]:
+    for name in ["jxb_sim_forward", "jxb_sim_backward", "jxb_sim_backward_noalloc"]:
         fn = getattr(lib, name)
         fn.restype = C.c_int
         fn.argtypes = [C.POINTER(JxbSimArgs), C.c_void_p]

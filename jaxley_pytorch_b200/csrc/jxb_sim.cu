@@ -746,3 +746,71 @@ extern "C" int64_t jxb_sim_smem_bytes(const JxbSimArgs* a, int backward) {
 
 extern "C" const char* jxb_last_error(void) { return g_err; }
 extern "C" int jxb_version(void) { return 1; }
+
+// ---------------------------------------------------------------------------------
+// Adjoint segment without caller-provided scratch.
+//
+// Some callers cannot allocate device memory while they run the simulation: a
+// host program that hands this library fixed buffers from its own memory pool and
+// forbids allocation during a training loop, or a plugin that is invoked from a
+// framework step whose allocator must not be re-entered. For them the trajectory
+// scratch of the adjoint (state before every step of the segment plus the step's
+// pivots) lives in this fixed device array instead of caller buffers. Every GPU that
+// loads the library holds the array until the process exits.
+// ---------------------------------------------------------------------------------
+namespace {
+
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+constexpr int kMaxDevices = 64;
+void* g_noalloc_ptr[kMaxDevices] = {nullptr};  // device address of the array, per device
+
+}  // namespace
+
+extern "C" int jxb_sim_backward_noalloc(const JxbSimArgs* a, void* stream) {
+  if (!a) return JXB_ERR_ARG;
+  if (a->dtype != JXB_F32 && a->dtype != JXB_F64) return JXB_ERR_DTYPE;
+  if (a->n_items <= 0) return JXB_OK;
+  if (a->n_steps <= 0 || a->batch <= 0 || a->n_slots <= 0 || a->n_nodes <= 0) {
+    snprintf(jxb::g_err, sizeof(jxb::g_err), "jxb_sim_backward_noalloc: bad sizes");
+    return JXB_ERR_ARG;
+  }
+  const size_t item = a->dtype == JXB_F32 ? sizeof(float) : sizeof(double);
+  const size_t traj_bytes = (size_t)a->n_steps * a->batch * a->n_slots * item;
+  const size_t piv_off = (traj_bytes + 255) / 256 * 256;
+  const size_t need = piv_off + (size_t)a->n_steps * a->batch * a->n_nodes * item;
+  if (need > kNoAllocScratchBytes) {
+    snprintf(jxb::g_err, sizeof(jxb::g_err),
+             "jxb_sim_backward_noalloc: segment needs %zu bytes of scratch, the fixed "
+             "array holds %zu (use fewer steps per segment or jxb_sim_backward)",
+             need, kNoAllocScratchBytes);
+    return JXB_ERR_TOO_LARGE;
+  }
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+    jxb::set_err("cudaGetDevice", e);
+    return JXB_ERR_LAUNCH;
+  }
+  // One-time set-up per device (the device must be current): the device address of
+  // the array. This first call should happen before any stream capture.
+  if (!g_noalloc_ptr[dev]) {
+    void* p = nullptr;
+    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess || !p) {
+      jxb::set_err("cudaGetSymbolAddress", e);
+      return JXB_ERR_LAUNCH;
+    }
+    g_noalloc_ptr[dev] = p;
+  }
+  // The caller's trajectory pointers are ignored; the rest is checked and launched
+  // as by jxb_sim_backward.
+  JxbSimArgs b = *a;
+  b.traj = g_noalloc_ptr[dev];
+  b.traj_piv = (unsigned char*)g_noalloc_ptr[dev] + piv_off;
+  const int rc = jxb::check_sim_args(&b, true);
+  if (rc != JXB_OK) return rc;
+  if (b.dtype == JXB_F32) return jxb::launch_sim<float>(b, true, (cudaStream_t)stream);
+  return jxb::launch_sim<double>(b, true, (cudaStream_t)stream);
+}
