@@ -62,7 +62,7 @@ typedef struct {
   int32_t max_levels;
   const int32_t* block_info;  /* (n_blocks, 4): node start, node count, chain start, level-ptr start */
   const int32_t* block_levels;/* (n_blocks,) number of chain levels */
-  const int32_t* perm;        /* (n_nodes,) chain-order position -> node index */
+  const int32_t* perm;        /* (n_nodes,) chain-order position -> node index (absolute) */
   const int32_t* chain_top;   /* (n_chains,) first node (chain-order position, block-relative) */
   const int32_t* chain_len;   /* (n_chains,) */
   const int32_t* chain_ptop;  /* (n_chains,) parent of the top (block-relative) or -1 */
@@ -83,9 +83,10 @@ typedef struct {
   int32_t n_blocks;
   int32_t regs_per_lane;      /* 1, 2, 4 or 8 */
   int32_t num_slots;          /* max children per node */
-  const int32_t* block_info;  /* (n_blocks, 4): start, length, levels (height), depth */
+  const int32_t* block_info;  /* (n_blocks, 4): start, length, height, depth of the block */
   const int32_t* rel_parent;  /* (n_blocks, 32*regs) parent (block-relative), self for roots */
   const int32_t* rel_height;  /* (n_blocks, 32*regs) height, -1 for padding */
+  const int32_t* rel_depth;   /* (n_blocks, 32*regs) depth, -1 for padding */
   const int32_t* rel_children;/* (n_blocks, num_slots, 32*regs) children or -1 */
 } JxbRegSchedule;
 

@@ -34,7 +34,8 @@ class JxbRegSchedule(C.Structure):
     _fields_ = [
         ("n_nodes", C.c_int32), ("n_blocks", C.c_int32), ("regs_per_lane", C.c_int32),
         ("num_slots", C.c_int32),
-        ("block_info", _p), ("rel_parent", _p), ("rel_height", _p), ("rel_children", _p),
+        ("block_info", _p), ("rel_parent", _p), ("rel_height", _p), ("rel_depth", _p),
+        ("rel_children", _p),
     ]
 
 

@@ -1,0 +1,391 @@
+"""Tree solve of the DHS voltage step on sm_100a: the drop-in for jaxley-pytorch's
+`kernels/tree_solve.py`.
+
+Same public surface as the reference module: `build_forest_schedule`,
+`build_level_schedule`, `TreeSolveKernel` / `LevelTreeSolveKernel` with `.solve()` and
+`.fused()`, `make_tree_solve_kernel(parent, device, mode)` honouring
+`JAXLEY_PYTORCH_TREE_KERNEL=auto|registers|levels` (`tree_solve.py:485-513`), the custom
+ops `tree_solve` / `tree_solve_levels` with the reference's argument lists and a
+backward that is the transposed solve (`tree_solve.py:516-630`), and
+`fused_tree_solve`. The schedule tensors are this implementation's own (chain
+schedule, warp-register blocks); the kernels are `jxb_tree_solve_levels` and
+`jxb_tree_solve_registers` of libjxb. There is no torch fallback: the reference
+returns `None` for orders it cannot handle, this module raises.
+
+The custom ops are registered as `jaxley_pytorch::tree_solve[_levels]` when that
+namespace is free, else (the reference's Triton module already registered it in the
+same process) as `jaxley_pytorch_b200::tree_solve[_levels]`.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import os
+from typing import Dict, Optional
+
+import numpy as np
+import torch
+
+from .. import _lib
+from ..lower import chain_levels, chain_order
+
+MAX_BLOCK = 256  # registers variant: 32 lanes x 8 registers
+LEVEL_BLOCK = 4096  # levels variant: nodes per block of trees (shared memory bound)
+
+
+def _forest(parent: np.ndarray):
+    parent = np.asarray(parent, dtype=np.int64)
+    n = len(parent)
+    roots = np.nonzero(parent < 0)[0]
+    if n == 0 or len(roots) == 0 or roots[0] != 0:
+        raise ValueError("the node order must start with a root")
+    ends = np.append(roots[1:], n)
+    tree_of = np.repeat(np.arange(len(roots)), ends - roots)
+    nonroot = parent >= 0
+    idx = np.arange(n)
+    if not (np.all(parent[nonroot] >= roots[tree_of[nonroot]]) and np.all(parent[nonroot] < idx[nonroot])):
+        raise ValueError("trees must be contiguous with parents before children")
+    return parent, roots, ends
+
+
+def _depth_height(parent: np.ndarray):
+    n = len(parent)
+    depth = np.zeros(n, dtype=np.int64)
+    for j in range(n):
+        if parent[j] >= 0:
+            depth[j] = depth[parent[j]] + 1
+    height = np.zeros(n, dtype=np.int64)
+    for j in range(n - 1, -1, -1):
+        p = parent[j]
+        if p >= 0:
+            height[p] = max(height[p], height[j] + 1)
+    return depth, height
+
+
+def _pack(roots, ends, max_nodes):
+    blocks, s = [], 0
+    for a, b in zip(roots, ends):
+        if b - s > max_nodes and a > s:
+            blocks.append((s, int(a)))
+            s = int(a)
+    blocks.append((s, int(ends[-1])))
+    return blocks
+
+
+def build_forest_schedule(parent: np.ndarray, max_block: int = MAX_BLOCK) -> Dict[str, np.ndarray]:
+    """Schedule of the registers variant: whole trees packed into blocks of at most
+    `max_block` (<= 256) nodes; per block the parent, height, depth and child slots of
+    every node (block-relative), cf. reference `tree_solve.py:45-138`."""
+    parent, roots, ends = _forest(parent)
+    if int((ends - roots).max()) > max_block:
+        raise ValueError(f"a tree has more than {max_block} nodes: use the levels variant")
+    depth, height = _depth_height(parent)
+    n = len(parent)
+    blocks = _pack(roots, ends, max_block)
+    size = max(b - a for a, b in blocks)
+    regs = 1
+    while 32 * regs < size:
+        regs *= 2
+    W = 32 * regs
+    kids = [[] for _ in range(n)]
+    for j in range(n):
+        if parent[j] >= 0:
+            kids[parent[j]].append(j)
+    num_slots = max(1, max(len(k) for k in kids))
+    nb = len(blocks)
+    rel_parent = np.tile(np.arange(W, dtype=np.int32), (nb, 1))
+    rel_height = -np.ones((nb, W), dtype=np.int32)
+    rel_depth = -np.ones((nb, W), dtype=np.int32)
+    rel_children = -np.ones((nb, num_slots, W), dtype=np.int32)
+    block_info = np.zeros((nb, 4), dtype=np.int32)
+    for b, (s, e) in enumerate(blocks):
+        ln = e - s
+        p = parent[s:e]
+        rel_parent[b, :ln] = np.where(p >= 0, p - s, np.arange(ln))
+        rel_height[b, :ln] = height[s:e]
+        rel_depth[b, :ln] = depth[s:e]
+        for j in range(s, e):
+            for k, c in enumerate(kids[j]):
+                rel_children[b, k, j - s] = c - s
+        block_info[b] = [s, ln, int(height[s:e].max()), int(depth[s:e].max())]
+    return {"parent": parent, "block_info": block_info, "rel_parent": rel_parent,
+            "rel_height": rel_height, "rel_depth": rel_depth, "rel_children": rel_children,
+            "block_size": W, "regs_per_lane": regs, "num_slots": num_slots, "num_nodes": n}
+
+
+def build_level_schedule(parent: np.ndarray, block_nodes: int = LEVEL_BLOCK) -> Dict[str, np.ndarray]:
+    """Schedule of the levels variant: trees packed into blocks of about
+    `block_nodes` nodes (a larger tree gets its own block), each block's nodes in
+    chain order with its chains sorted by level (cf. reference `tree_solve.py:142-224`)."""
+    parent, roots, ends = _forest(parent)
+    n = len(parent)
+    if int((ends - roots).max()) > 32767:
+        raise ValueError("trees of more than 32767 nodes are not supported")
+    order, tree_ptr, chains = chain_order(parent)
+    lev = chain_levels(chains)
+    blocks = _pack(roots, ends, block_nodes)
+    # chain_order keeps the trees in order, so a block is the same range in both orders.
+    tops = np.asarray([c[0] for c in chains], dtype=np.int64)
+    srt = np.argsort(tops, kind="stable")
+    tops_s = tops[srt]
+    chain_top, chain_len, chain_ptop, chain_cptr, chain_child = [], [], [], [0], []
+    level_ptr, block_info, block_levels = [], [], []
+    top_of = {}
+    for (n0, n1) in blocks:
+        lo, hi = np.searchsorted(tops_s, n0), np.searchsorted(tops_s, n1)
+        cids = srt[lo:hi]
+        cids = cids[np.argsort(lev[cids], kind="stable")]
+        nlev = int(lev[cids].max()) + 1 if len(cids) else 0
+        c0 = len(chain_top)
+        lp0 = len(level_ptr)
+        counts = np.bincount(lev[cids], minlength=nlev)
+        level_ptr.extend(np.concatenate([[0], np.cumsum(counts)]).tolist())
+        for c in cids:
+            top, ln, ptop, kids = chains[c]
+            chain_top.append(top - n0)
+            chain_len.append(ln)
+            chain_ptop.append(ptop - n0 if ptop >= 0 else -1)
+            for k in kids:
+                chain_child.append(chains[k][0] - n0)
+            chain_cptr.append(len(chain_child))
+        block_info.append([n0, n1 - n0, c0, lp0])
+        block_levels.append(nlev)
+    i32 = lambda x: np.ascontiguousarray(np.asarray(x, dtype=np.int32))  # noqa: E731
+    return {"parent": parent, "block_info": i32(block_info), "block_levels": i32(block_levels),
+            "perm": i32(order), "chain_top": i32(chain_top), "chain_len": i32(chain_len),
+            "chain_ptop": i32(chain_ptop), "chain_cptr": i32(chain_cptr),
+            "chain_child": i32(chain_child if chain_child else [0]), "level_ptr": i32(level_ptr),
+            "max_block_nodes": int(max(b - a for a, b in blocks)),
+            "max_levels": int(max(block_levels)), "num_nodes": n,
+            "num_slots": int(max(1, max(len(c[3]) for c in chains)))}
+
+
+def _code(t: torch.Tensor) -> int:
+    if t.dtype == torch.float32:
+        return _lib.F32
+    if t.dtype == torch.float64:
+        return _lib.F64
+    raise TypeError(f"unsupported dtype {t.dtype}")
+
+
+def _prep(diags, lowers, uppers, solves, n):
+    assert diags.shape[-1] == n, (diags.shape, n)
+    batch = torch.broadcast_shapes(diags.shape, lowers.shape, uppers.shape, solves.shape)[:-1]
+    ts = [torch.broadcast_to(t, (*batch, n)).reshape(-1, n).contiguous()
+          for t in (diags, lowers, uppers, solves)]
+    dt = ts[0].dtype
+    ts = [t.to(dt) for t in ts]
+    return batch, ts
+
+
+class TreeSolveKernel:
+    """Registers variant (blocks of small trees); schedule on the GPU."""
+
+    def __init__(self, schedule: Dict[str, np.ndarray], device):
+        self.device = torch.device(device)
+        dev = self.device
+        self.num_nodes = schedule["num_nodes"]
+        self.block_size = schedule["block_size"]
+        self.num_slots = schedule["num_slots"]
+        self.num_warps = schedule["regs_per_lane"]  # the op's third int: registers per lane
+        self.t = {k: torch.as_tensor(schedule[k], device=dev).contiguous()
+                  for k in ["block_info", "rel_parent", "rel_height", "rel_depth", "rel_children"]}
+        parents = np.asarray(schedule["parent"], dtype=np.int64)
+        self.has_parent = torch.as_tensor(parents >= 0, device=dev)
+        self.parent_safe = torch.as_tensor(np.where(parents >= 0, parents, 0), device=dev)
+        s = _lib.JxbRegSchedule()
+        s.n_nodes = self.num_nodes
+        s.n_blocks = int(schedule["block_info"].shape[0])
+        s.regs_per_lane = schedule["regs_per_lane"]
+        s.num_slots = self.num_slots
+        for k in ["block_info", "rel_parent", "rel_height", "rel_depth", "rel_children"]:
+            setattr(s, k, self.t[k].data_ptr())
+        self.sched = s
+
+    def raw(self, d, l, u, s):
+        x = torch.empty_like(s)
+        st = torch.cuda.current_stream(d.device).cuda_stream
+        rc = _lib.load().jxb_tree_solve_registers(_code(d), d.data_ptr(), l.data_ptr(), u.data_ptr(),
+                                                  s.data_ptr(), x.data_ptr(), d.shape[0],
+                                                  C.byref(self.sched), C.c_void_p(st))
+        _lib.check(rc, "jxb_tree_solve_registers")
+        return x
+
+    def solve(self, diags, lowers, uppers, solves):
+        """Solve; all inputs have shape `(..., num_nodes)` (broadcast)."""
+        batch, (d, l, u, s) = _prep(diags, lowers, uppers, solves, self.num_nodes)
+        return self.raw(d, l, u, s).reshape(*batch, self.num_nodes)
+
+    def fused(self, diags, lowers, uppers, solves):
+        """Differentiable solve (custom op)."""
+        _register(self)
+        return tree_solve_op(diags, lowers, uppers, solves, self.t["block_info"],
+                             self.t["rel_parent"], self.t["rel_height"], self.t["rel_children"],
+                             self.parent_safe, self.has_parent, self.block_size, self.num_slots,
+                             self.num_warps)
+
+
+class LevelTreeSolveKernel:
+    """Levels variant (chain schedule in shared memory); schedule on the GPU."""
+
+    W = 0  # kept for interface parity (the reference's chunk width); unused here
+
+    def __init__(self, schedule: Dict[str, np.ndarray], device):
+        self.device = torch.device(device)
+        dev = self.device
+        self.num_nodes = schedule["num_nodes"]
+        self.num_slots = schedule["num_slots"]
+        keys = ["block_info", "block_levels", "perm", "chain_top", "chain_len", "chain_ptop",
+                "chain_cptr", "chain_child", "level_ptr"]
+        self.t = {k: torch.as_tensor(schedule[k], device=dev).contiguous() for k in keys}
+        parents = np.asarray(schedule["parent"], dtype=np.int64)
+        self.has_parent = torch.as_tensor(parents >= 0, device=dev)
+        self.parent_safe = torch.as_tensor(np.where(parents >= 0, parents, 0), device=dev)
+        s = _lib.JxbTreeSchedule()
+        s.n_nodes = self.num_nodes
+        s.n_blocks = int(schedule["block_info"].shape[0])
+        s.max_block_nodes = schedule["max_block_nodes"]
+        s.max_levels = schedule["max_levels"]
+        for k in keys:
+            setattr(s, k, self.t[k].data_ptr())
+        self.sched = s
+        self.block_info = self.t["block_info"]
+
+    def raw(self, d, l, u, s):
+        x = torch.empty_like(s)
+        st = torch.cuda.current_stream(d.device).cuda_stream
+        rc = _lib.load().jxb_tree_solve_levels(_code(d), d.data_ptr(), l.data_ptr(), u.data_ptr(),
+                                               s.data_ptr(), x.data_ptr(), d.shape[0],
+                                               C.byref(self.sched), C.c_void_p(st))
+        _lib.check(rc, "jxb_tree_solve_levels")
+        return x
+
+    def solve(self, diags, lowers, uppers, solves):
+        batch, (d, l, u, s) = _prep(diags, lowers, uppers, solves, self.num_nodes)
+        return self.raw(d, l, u, s).reshape(*batch, self.num_nodes)
+
+    def fused(self, diags, lowers, uppers, solves):
+        _register(self)
+        t = self.t
+        return tree_solve_levels_op(diags, lowers, uppers, solves, t["block_info"], t["level_ptr"],
+                                    t["perm"], t["chain_ptop"], t["chain_child"], self.parent_safe,
+                                    self.has_parent, self.num_slots, 0)
+
+
+def make_tree_solve_kernel(parent: np.ndarray, device, mode: Optional[str] = None):
+    """The solver for the forest given by `parent` (solve order, -1 for roots).
+
+    `mode` (default: `JAXLEY_PYTORCH_TREE_KERNEL`, else `auto`): `registers` for
+    blocks of small trees held in warp registers, `levels` for any tree (chain
+    schedule), `auto` picks `registers` when every tree has at most 64 nodes."""
+    mode = mode or os.environ.get("JAXLEY_PYTORCH_TREE_KERNEL", "auto")
+    if mode not in ("auto", "registers", "levels"):
+        raise ValueError(f"JAXLEY_PYTORCH_TREE_KERNEL={mode}: expected auto, registers or levels")
+    parent, roots, ends = _forest(parent)
+    largest = int((ends - roots).max())
+    if mode == "auto":
+        mode = "registers" if largest <= 64 else "levels"
+    if mode == "registers":
+        return TreeSolveKernel(build_forest_schedule(parent), device)
+    return LevelTreeSolveKernel(build_level_schedule(parent), device)
+
+
+# ----------------------------------------------------------------------------------
+# Custom ops (registered on first use; the registry maps schedule tensors to kernels)
+# ----------------------------------------------------------------------------------
+_KERNELS: Dict[int, object] = {}
+_NS = None
+tree_solve_op = None
+tree_solve_levels_op = None
+
+
+def _register(kernel) -> None:
+    _KERNELS[kernel.t["block_info"].data_ptr()] = kernel
+    if _NS is None:
+        _define_ops()
+
+
+def _kernel_for(block_info: torch.Tensor):
+    k = _KERNELS.get(block_info.data_ptr())
+    if k is None:
+        raise RuntimeError("tree_solve: unknown schedule (build it with make_tree_solve_kernel)")
+    return k
+
+
+def _transposed_backward(kernel_op, ctx, grad_x, args_after):
+    diags, lowers, uppers, x, parent_safe, has_parent = ctx.saved_tensors
+    lam = kernel_op(diags, uppers, lowers, grad_x.contiguous(), *args_after)
+    g_diags = -lam * x
+    g_uppers = torch.where(has_parent, -lam[..., parent_safe] * x, torch.zeros_like(x))
+    g_lowers = torch.where(has_parent, -lam * x[..., parent_safe], torch.zeros_like(x))
+    return g_diags, g_lowers, g_uppers, lam
+
+
+def _define_ops():
+    global _NS, tree_solve_op, tree_solve_levels_op
+    for ns in ("jaxley_pytorch", "jaxley_pytorch_b200"):
+        try:
+            _define_in(ns)
+            _NS = ns
+            return
+        except RuntimeError:
+            continue
+    raise RuntimeError("could not register the tree-solve ops")
+
+
+def _define_in(ns: str):
+    global tree_solve_op, tree_solve_levels_op
+
+    @torch.library.custom_op(f"{ns}::tree_solve", mutates_args=())
+    def _tree_solve(diags: torch.Tensor, lowers: torch.Tensor, uppers: torch.Tensor,
+                    solves: torch.Tensor, block_info: torch.Tensor, rel_parent: torch.Tensor,
+                    rel_height: torch.Tensor, rel_children: torch.Tensor,
+                    parent_safe: torch.Tensor, has_parent: torch.Tensor, block_size: int,
+                    num_slots: int, num_warps: int) -> torch.Tensor:
+        """Registers-variant tree solve (reference `tree_solve.py:518-563`)."""
+        return _kernel_for(block_info).solve(diags, lowers, uppers, solves)
+
+    @_tree_solve.register_fake
+    def _(diags, lowers, uppers, solves, *args):
+        return torch.empty_like(solves)
+
+    def _setup(ctx, inputs, output):
+        ctx.save_for_backward(inputs[0], inputs[1], inputs[2], output, inputs[8], inputs[9])
+        ctx.rest = inputs[4:]
+
+    def _backward(ctx, grad_x):
+        g = _transposed_backward(_tree_solve, ctx, grad_x, ctx.rest)
+        return g + (None,) * 9
+
+    _tree_solve.register_autograd(_backward, setup_context=_setup)
+
+    @torch.library.custom_op(f"{ns}::tree_solve_levels", mutates_args=())
+    def _tree_solve_levels(diags: torch.Tensor, lowers: torch.Tensor, uppers: torch.Tensor,
+                           solves: torch.Tensor, block_info: torch.Tensor,
+                           level_ptr: torch.Tensor, ordered_nodes: torch.Tensor,
+                           ordered_parent: torch.Tensor, ordered_children: torch.Tensor,
+                           parent_safe: torch.Tensor, has_parent: torch.Tensor, num_slots: int,
+                           w: int) -> torch.Tensor:
+        """Levels-variant tree solve (reference `tree_solve.py:589-609`)."""
+        return _kernel_for(block_info).solve(diags, lowers, uppers, solves)
+
+    @_tree_solve_levels.register_fake
+    def _(diags, lowers, uppers, solves, *args):
+        return torch.empty_like(solves)
+
+    def _setup_l(ctx, inputs, output):
+        ctx.save_for_backward(inputs[0], inputs[1], inputs[2], output, inputs[9], inputs[10])
+        ctx.rest = inputs[4:]
+
+    def _backward_l(ctx, grad_x):
+        g = _transposed_backward(_tree_solve_levels, ctx, grad_x, ctx.rest)
+        return g + (None,) * 9
+
+    _tree_solve_levels.register_autograd(_backward_l, setup_context=_setup_l)
+    tree_solve_op = _tree_solve
+    tree_solve_levels_op = _tree_solve_levels
+
+
+def fused_tree_solve(kernel, diags, lowers, uppers, solves):
+    """Differentiable fused tree solve (reference `tree_solve.py:633-635`)."""
+    return kernel.fused(diags, lowers, uppers, solves)

@@ -1,0 +1,123 @@
+"""The standalone tree-solve drop-in (jaxley_pytorch_b200.kernels.tree_solve) against
+the oracle and a dense solve, as the reference's tests/test_kernels.py:63-136 and
+tests/test_solver.py:78-199 check its Triton kernels (float64 1e-12, float32 1e-4,
+gradients 1e-10, gradcheck)."""
+import numpy as np
+import pytest
+import torch
+
+import oracle
+from jaxley_pytorch_b200.kernels import tree_solve as ts
+
+
+def forests():
+    rng = np.random.default_rng(0)
+    out = {}
+    out["chain_12"] = [-1] + list(range(11))
+    out["star_8"] = [-1] + [0] * 8  # a node with 8 children (tests/test_kernels.py:25-33)
+    out["point_cells_5"] = [-1] * 5
+    out["ragged_4"] = [-1, 0, 0, 1]  # tests/test_solver.py:78-86
+    rnd = [-1] + [int(rng.integers(0, j)) for j in range(1, 40)]
+    out["random_40"] = rnd
+    # a forest of uneven trees
+    f = []
+    for sz in [1, 7, 30, 3, 60, 2]:
+        base = len(f)
+        f += [-1] + [base + int(rng.integers(0, j)) for j in range(1, sz)]
+    out["forest_mixed"] = f
+    deep = [-1] + [int(j - 1 if rng.random() < 0.8 else rng.integers(0, j)) for j in range(1, 600)]
+    out["deep_600"] = deep
+    return out
+
+
+def system(parent, B, dtype, seed=1):
+    rng = np.random.default_rng(seed)
+    n = len(parent)
+    parent = np.asarray(parent)
+    l = rng.uniform(-0.4, -0.05, (B, n))
+    u = rng.uniform(-0.4, -0.05, (B, n))
+    l[:, parent < 0] = 0
+    u[:, parent < 0] = 0
+    d = 1.0 + rng.uniform(0.5, 1.5, (B, n)) + np.abs(l)
+    for j in range(n):
+        if parent[j] >= 0:
+            d[:, parent[j]] += np.abs(u[:, j])
+    s = rng.normal(size=(B, n))
+    return d, l, u, s
+
+
+def test_schedules_on_cpu():
+    for name, parent in forests().items():
+        lv = ts.build_level_schedule(np.asarray(parent))
+        assert sorted(lv["perm"].tolist()) == list(range(len(parent)))
+        if max(np.diff(np.append(np.nonzero(np.asarray(parent) < 0)[0], len(parent)))) <= ts.MAX_BLOCK:
+            fs = ts.build_forest_schedule(np.asarray(parent))
+            assert fs["block_size"] % 32 == 0
+    with pytest.raises(ValueError):
+        ts.build_forest_schedule(np.asarray(forests()["deep_600"]))
+    with pytest.raises(ValueError):
+        ts.build_level_schedule(np.asarray([0, -1]))
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["registers", "levels"])
+@pytest.mark.parametrize("name", list(forests()))
+def test_tree_solve_matches_oracle(cuda_device, mode, name):
+    parent = np.asarray(forests()[name])
+    if mode == "registers" and name == "deep_600":
+        pytest.skip("tree larger than the registers variant")
+    kern = ts.make_tree_solve_kernel(parent, cuda_device, mode=mode)
+    assert isinstance(kern, ts.TreeSolveKernel if mode == "registers" else ts.LevelTreeSolveKernel)
+    d, l, u, s = system(parent, 6, np.float64)
+    ref = oracle.tree_solve(d, l, u, s, parent)
+    for dtype, tol in [(torch.float64, 1e-12), (torch.float32, 1e-4)]:
+        args = [torch.as_tensor(a, dtype=dtype, device=cuda_device) for a in (d, l, u, s)]
+        x = kern.solve(*args).double().cpu().numpy()
+        np.testing.assert_allclose(x, ref, rtol=tol, atol=tol)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["registers", "levels"])
+def test_tree_solve_gradients(cuda_device, mode):
+    parent = np.asarray(forests()["random_40"])
+    kern = ts.make_tree_solve_kernel(parent, cuda_device, mode=mode)
+    d, l, u, s = system(parent, 3, np.float64, seed=4)
+    args = [torch.as_tensor(a, device=cuda_device).requires_grad_(True) for a in (d, l, u, s)]
+    w = torch.randn(3, len(parent), dtype=torch.float64, device=cuda_device)
+    (ts.fused_tree_solve(kern, *args) * w).sum().backward()
+    # Dense reference: A x = s.
+    n = len(parent)
+    dn = [torch.as_tensor(a).requires_grad_(True) for a in (d, l, u, s)]
+    A = torch.diag_embed(dn[0])
+    idx = torch.arange(n)
+    par = torch.as_tensor(np.where(parent >= 0, parent, 0))
+    has = torch.as_tensor(parent >= 0)
+    bi = torch.arange(d.shape[0])[:, None]
+    rows, cols = idx[has][None, :], par[has][None, :]
+    A = A.index_put((bi, rows, cols), dn[1][:, has], accumulate=True)
+    A = A.index_put((bi, cols, rows), dn[2][:, has], accumulate=True)
+    x = torch.linalg.solve(A, dn[3])
+    (x * w.cpu()).sum().backward()
+    for g, r in zip(args, dn):
+        np.testing.assert_allclose(g.grad.cpu().numpy(), r.grad.numpy(), rtol=1e-10, atol=1e-10)
+
+
+@pytest.mark.gpu
+def test_tree_solve_gradcheck(cuda_device):
+    parent = np.asarray(forests()["ragged_4"])
+    kern = ts.make_tree_solve_kernel(parent, cuda_device, mode="levels")
+    d, l, u, s = system(parent, 2, np.float64, seed=5)
+    args = tuple(torch.as_tensor(a, device=cuda_device).requires_grad_(True) for a in (d, l, u, s))
+    assert torch.autograd.gradcheck(lambda *a: ts.fused_tree_solve(kern, *a), args)
+
+
+@pytest.mark.gpu
+def test_env_var_selects_variant(cuda_device, monkeypatch):
+    parent = np.asarray(forests()["random_40"])
+    monkeypatch.setenv("JAXLEY_PYTORCH_TREE_KERNEL", "levels")
+    assert isinstance(ts.make_tree_solve_kernel(parent, cuda_device), ts.LevelTreeSolveKernel)
+    monkeypatch.setenv("JAXLEY_PYTORCH_TREE_KERNEL", "registers")
+    assert isinstance(ts.make_tree_solve_kernel(parent, cuda_device), ts.TreeSolveKernel)
+    monkeypatch.setenv("JAXLEY_PYTORCH_TREE_KERNEL", "auto")
+    deep = np.asarray(forests()["deep_600"])
+    assert isinstance(ts.make_tree_solve_kernel(deep, cuda_device), ts.LevelTreeSolveKernel)
