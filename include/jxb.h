@@ -227,6 +227,7 @@ typedef struct {
   void* g_v;                  /* (batch, n_nodes), overwritten */
   void* g_params;             /* (n_need, n_syn), overwritten */
   void* g_pre;                /* (n_syn, batch) scratch for the presynaptic sum */
+  void* g_post;               /* (batch, n_syn / k) scratch for the postsynaptic sum */
   int32_t need;               /* bit mask of parameters that need gradients */
   int32_t inv_width, n_pre_nodes, pad;
   const int32_t* inv;         /* (n_pre_nodes, inv_width) synapses of every pre node */

@@ -82,7 +82,7 @@ class JxbSynArgs(C.Structure):
         ("p", _p * 6), ("area", _p), ("scalars", _p),
         ("s_new", _p), ("current", _p), ("lin", _p), ("cst", _p),
         ("g_s_new", _p), ("g_current", _p), ("g_lin", _p), ("g_const", _p),
-        ("g_s", _p), ("g_v", _p), ("g_params", _p), ("g_pre", _p),
+        ("g_s", _p), ("g_v", _p), ("g_params", _p), ("g_pre", _p), ("g_post", _p),
         ("need", C.c_int32), ("inv_width", C.c_int32), ("n_pre_nodes", C.c_int32), ("pad", C.c_int32),
         ("inv", _p), ("pre_nodes", _p),
     ]
