@@ -61,7 +61,6 @@ struct SimSmem {
   T* V;                      // rows * n_nodes: voltages during the segment
   // adjoint
   T *adj, *X1;               // rows * n_slots, rows * n_nodes
-  double* pg;                // rows * n_cols
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -70,8 +69,7 @@ template <typename T>
 __host__ __device__ inline size_t sim_smem_layout(const JxbSimArgs& a, bool backward, SimSmem<T>* o,
                                                   char* base) {
   const size_t R = a.max_rows, nn = a.max_nodes, ns = a.max_slots, nc = a.max_chains,
-               nk = a.max_child, nl = a.max_levels, np = a.max_pslots, ne = a.n_entries,
-               ncol = a.n_cols;
+               nk = a.max_child, nl = a.max_levels, np = a.max_pslots, ne = a.n_entries;
   size_t off = 0;
   auto take = [&](size_t bytes) {
     size_t r = off;
@@ -80,7 +78,6 @@ __host__ __device__ inline size_t sim_smem_layout(const JxbSimArgs& a, bool back
   };
   SimSmem<T> s;
   // 8-byte types first.
-  s.pg = backward ? (double*)take(sizeof(double) * R * ncol) : nullptr;
   s.st = (T*)take(sizeof(T) * R * ns);
   s.adj = backward ? (T*)take(sizeof(T) * R * ns) : nullptr;
   s.D = (T*)take(sizeof(T) * R * nn);
@@ -195,8 +192,7 @@ __device__ void stage_item(const JxbSimArgs& a, const JxbBlock& blk, int row0, i
       for (int q = tid; q < ns; q += NT) sa[q] = ga[q];
     }
   }
-  if (sm.pg) {
-    for (int q = tid; q < rows * a.n_cols; q += NT) sm.pg[q] = 0.0;
+  if (sm.gacc) {
     for (int q = tid; q < rows * a.max_gslots; q += NT) sm.gacc[q] = T(0);
   }
 }
@@ -612,7 +608,9 @@ __global__ void __launch_bounds__(NT) sim_backward_kernel(JxbSimArgs a) {
     }
     __syncthreads();
   }
-  // Fold the nodes' gradient slots into the columns (float64), once per launch.
+  // Fold the nodes' gradient slots into the columns (float64, global), once per
+  // launch: a shared per-column buffer would scale with the number of columns,
+  // which is large when every cell has its own trainable group.
   for (int w = tid; w < total; w += nthr) {
     const int r = w / nn, j = w - r * nn;
     const int cls = sm.cls[j];
@@ -620,22 +618,17 @@ __global__ void __launch_bounds__(NT) sim_backward_kernel(JxbSimArgs a) {
     for (int q = sm.cptr[cls]; q < sm.cptr[cls + 1]; ++q) npar += sm.ents[q].np;
     const int po = sm.poff[j];
     const T* ga = sm.gacc + (size_t)r * a.max_gslots + sm.gbase[j];
+    double* pg = a.pgrad + (size_t)(row0 + r) * a.n_cols;
     for (int k = 0; k < npar; ++k) {
       const int q = sm.gk[po + k];
-      if (q >= 0 && ga[q] != T(0)) atomicAdd(sm.pg + (size_t)r * a.n_cols + sm.pc[po + k], (double)ga[q]);
+      if (q >= 0 && ga[q] != T(0)) atomicAdd(pg + sm.pc[po + k], (double)ga[q]);
     }
   }
-  __syncthreads();
-  // Adjoint of the segment's initial state, and the parameter gradients.
+  // Adjoint of the segment's initial state.
   for (int r = 0; r < rows; ++r) {
     T* ga = (T*)a.adj + (size_t)(row0 + r) * a.n_slots + blk.slot0;
     const T* sa = sm.adj + (size_t)r * ns;
     for (int q = tid; q < ns; q += nthr) ga[q] = sa[q];
-  }
-  for (int q = tid; q < rows * a.n_cols; q += nthr) {
-    const int r = q / a.n_cols, c = q % a.n_cols;
-    const double gv = sm.pg[q];
-    if (c != 0 && gv != 0.0) atomicAdd(a.pgrad + (size_t)(row0 + r) * a.n_cols + c, gv);
   }
 }
 

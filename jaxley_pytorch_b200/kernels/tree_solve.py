@@ -27,7 +27,7 @@ import numpy as np
 import torch
 
 from .. import _lib
-from ..lower import chain_levels, chain_order
+from ..lower import block_schedule, chain_table
 
 MAX_BLOCK = 256  # registers variant: 32 lanes x 8 registers
 LEVEL_BLOCK = 4096  # levels variant: nodes per block of trees (shared memory bound)
@@ -121,43 +121,21 @@ def build_level_schedule(parent: np.ndarray, block_nodes: int = LEVEL_BLOCK) -> 
     n = len(parent)
     if int((ends - roots).max()) > 32767:
         raise ValueError("trees of more than 32767 nodes are not supported")
-    order, tree_ptr, chains = chain_order(parent)
-    lev = chain_levels(chains)
+    order, tree_ptr, chains = chain_table(parent)
     blocks = _pack(roots, ends, block_nodes)
-    # chain_order keeps the trees in order, so a block is the same range in both orders.
-    tops = np.asarray([c[0] for c in chains], dtype=np.int64)
-    srt = np.argsort(tops, kind="stable")
-    tops_s = tops[srt]
-    chain_top, chain_len, chain_ptop, chain_cptr, chain_child = [], [], [], [0], []
-    level_ptr, block_info, block_levels = [], [], []
-    top_of = {}
-    for (n0, n1) in blocks:
-        lo, hi = np.searchsorted(tops_s, n0), np.searchsorted(tops_s, n1)
-        cids = srt[lo:hi]
-        cids = cids[np.argsort(lev[cids], kind="stable")]
-        nlev = int(lev[cids].max()) + 1 if len(cids) else 0
-        c0 = len(chain_top)
-        lp0 = len(level_ptr)
-        counts = np.bincount(lev[cids], minlength=nlev)
-        level_ptr.extend(np.concatenate([[0], np.cumsum(counts)]).tolist())
-        for c in cids:
-            top, ln, ptop, kids = chains[c]
-            chain_top.append(top - n0)
-            chain_len.append(ln)
-            chain_ptop.append(ptop - n0 if ptop >= 0 else -1)
-            for k in kids:
-                chain_child.append(chains[k][0] - n0)
-            chain_cptr.append(len(chain_child))
-        block_info.append([n0, n1 - n0, c0, lp0])
-        block_levels.append(nlev)
+    # chain_table keeps the trees in order, so a block is the same range in both orders.
+    (chain_top, chain_len, chain_ptop, chain_cptr, chain_child, level_ptr,
+     per_block) = block_schedule(chains, blocks, relative=True)
+    block_info = [[n0, n1 - n0, pb[0], pb[2]] for (n0, n1), pb in zip(blocks, per_block)]
+    block_levels = [pb[3] for pb in per_block]
     i32 = lambda x: np.ascontiguousarray(np.asarray(x, dtype=np.int32))  # noqa: E731
     return {"parent": parent, "block_info": i32(block_info), "block_levels": i32(block_levels),
             "perm": i32(order), "chain_top": i32(chain_top), "chain_len": i32(chain_len),
             "chain_ptop": i32(chain_ptop), "chain_cptr": i32(chain_cptr),
-            "chain_child": i32(chain_child if chain_child else [0]), "level_ptr": i32(level_ptr),
+            "chain_child": i32(chain_child if len(chain_child) else [0]), "level_ptr": i32(level_ptr),
             "max_block_nodes": int(max(b - a for a, b in blocks)),
             "max_levels": int(max(block_levels)), "num_nodes": n,
-            "num_slots": int(max(1, max(len(c[3]) for c in chains)))}
+            "num_slots": int(max(1, np.diff(chains.kid_ptr).max(initial=0)))}
 
 
 def _code(t: torch.Tensor) -> int:

@@ -27,6 +27,48 @@ from .problem import Problem
 ENTRY_SHORTS = 18  # ChanEntry: type, ns, np, cur, s[6], p[8]
 
 
+class _SlotNames:
+    """Slot names of every internal node (shared per node group)."""
+
+    def __init__(self, grp_names, grp_int):
+        self.grp_names = grp_names
+        self.grp_int = grp_int
+
+    def __getitem__(self, i):
+        return self.grp_names[int(self.grp_int[i])]
+
+    def __len__(self):
+        return len(self.grp_int)
+
+
+class _ColMembers:
+    """`(param name, reference node, base value)` of every use of a column, built on
+    access (a column of a trainable group can have millions of uses)."""
+
+    def __init__(self, ncol, use_c, use_i, use_k, grp_pslots, grp_int, grp_base, row_in_grp,
+                 int2node):
+        self.ncol = ncol
+        order = np.argsort(use_c, kind="stable")
+        self.use_c = use_c[order]
+        self.use_i = use_i[order]
+        self.use_k = use_k[order]
+        self.ptr = np.searchsorted(self.use_c, np.arange(ncol + 1))
+        self.grp_pslots, self.grp_int, self.grp_base = grp_pslots, grp_int, grp_base
+        self.row_in_grp, self.int2node = row_in_grp, int2node
+
+    def __len__(self):
+        return self.ncol
+
+    def __getitem__(self, col):
+        out = set()
+        for q in range(self.ptr[col], self.ptr[col + 1]):
+            i, k = int(self.use_i[q]), int(self.use_k[q])
+            g = int(self.grp_int[i])
+            out.add((self.grp_pslots[g][k][1], int(self.int2node[i]),
+                     float(self.grp_base[g][self.row_in_grp[i], k])))
+        return sorted(out)
+
+
 @dataclass
 class Lowered:
     n_nodes: int
@@ -50,7 +92,7 @@ class Lowered:
     pcol: np.ndarray
     pscale: np.ndarray  # (B, n_cols)
     col_info: List[Tuple[str, int]]  # (param name, reference node of first use) per column
-    col_members: List[List[Tuple[str, int, float]]]  # (param name, node, base) per column
+    col_members: "_ColMembers"  # [col] -> (param name, node, base) of its uses
     # chains and blocks
     chain_top: np.ndarray
     chain_len: np.ndarray
@@ -75,7 +117,7 @@ class Lowered:
     n_rec: int
     # state
     state0: np.ndarray  # (B, n_slots)
-    slot_names: List[List[str]]  # per internal node
+    slot_names: "_SlotNames"  # [internal node] -> slot names
     dt: float
     n_steps: int
     max_levels: int = 0
@@ -94,68 +136,182 @@ class Lowered:
         return int(self.pscale.shape[1])
 
 
-def _children(parent: np.ndarray) -> List[List[int]]:
-    ch: List[List[int]] = [[] for _ in range(len(parent))]
-    for j, p in enumerate(parent):
-        if p >= 0:
-            ch[p].append(j)
-    return ch
+@dataclass
+class ChainTable:
+    """Chains of a forest in breadth-first chain order (arrays indexed by chain id)."""
+
+    top: np.ndarray  # first node (chain order)
+    length: np.ndarray
+    ptop: np.ndarray  # chain-order index of the parent chain's last node, -1 at a root
+    parent: np.ndarray  # parent chain id, -1 at a root
+    kid_ptr: np.ndarray  # (n_chains + 1,) child chains CSR
+    kid: np.ndarray
+    depth: np.ndarray  # chain depth from the root chain
+
+    def __len__(self):
+        return len(self.top)
+
+    def as_list(self):
+        """`(top, length, parent_top_node, child_chain_ids)` per chain."""
+        return [[int(self.top[c]), int(self.length[c]), int(self.ptop[c]),
+                 self.kid[self.kid_ptr[c]:self.kid_ptr[c + 1]].tolist()] for c in range(len(self.top))]
 
 
-def chain_order(parent: np.ndarray):
-    """Chain decomposition of a solve-order forest.
+def _unique_rows(a: np.ndarray):
+    """`np.unique(a, axis=0, return_index=True, return_inverse=True)` for a 2-D array,
+    with each distinct row's first index; sorts with `lexsort` over the columns."""
+    m = a.shape[0]
+    if m == 0:
+        return a[:0], np.zeros(0, np.int64), np.zeros(0, np.int64)
+    if a.shape[1] == 0:
+        return a[:1], np.zeros(1, np.int64), np.zeros(m, np.int64)
+    if a.shape[1] > 16:
+        u, first, inv = np.unique(a, axis=0, return_index=True, return_inverse=True)
+        return u, first, inv.reshape(-1)
+    srt = np.lexsort(a.T[::-1])  # stable: equal rows keep their index order
+    b = a[srt]
+    new = np.ones(m, dtype=bool)
+    new[1:] = np.any(b[1:] != b[:-1], axis=1)
+    grp = np.cumsum(new) - 1
+    inv = np.empty(m, dtype=np.int64)
+    inv[srt] = grp
+    return b[new], srt[new], inv
 
-    Returns `(order, trees, chains)`: `order[i]` is the solve index of chain-order
-    node `i`; `trees` the chain-order start of every tree (plus the end);
-    `chains` a list of `(top, length, parent_top_node, child_chain_ids)` in chain
-    order (node indices in chain order).
+
+def _pointer_jump(ptr: np.ndarray, dist: np.ndarray):
+    """List ranking: follow `ptr` to its fixed point, summing `dist` on the way."""
+    while True:
+        nxt = ptr[ptr]
+        if np.array_equal(nxt, ptr):
+            return ptr, dist
+        dist = dist + dist[ptr]
+        ptr = nxt
+
+
+def chain_table(parent: np.ndarray):
+    """Chain decomposition of a solve-order forest (vectorised).
+
+    A node continues its parent's chain when it is the parent's only child. The
+    chains of every tree are numbered breadth first (a chain's children in the order
+    of their first nodes) and their nodes laid out consecutively. Returns
+    `(order, trees, table)`: `order[i]` is the solve index of chain-order node `i`,
+    `trees` the chain-order start of every tree (plus the end).
     """
     parent = np.asarray(parent, dtype=np.int64)
     n = len(parent)
     roots = np.nonzero(parent < 0)[0]
     if n == 0 or len(roots) == 0 or roots[0] != 0:
         raise ValueError("the forest must start with a root")
-    starts = roots
     ends = np.append(roots[1:], n)
-    tree_of = np.repeat(np.arange(len(starts)), ends - starts)
+    tree_of = np.repeat(np.arange(len(roots)), ends - roots)
     nonroot = parent >= 0
     idx = np.arange(n)
-    if not (np.all(parent[nonroot] >= starts[tree_of[nonroot]]) and np.all(parent[nonroot] < idx[nonroot])):
+    if not (np.all(parent[nonroot] >= roots[tree_of[nonroot]]) and np.all(parent[nonroot] < idx[nonroot])):
         raise ValueError("every tree must be contiguous and parents must precede children")
-    kids = _children(parent)
-    order: List[int] = []
-    chains: List[list] = []  # [top, len, ptop(chain order), [child chain ids]]
-    trees = [0]
-    for r in roots:
-        queue = [(int(r), -1, -1)]  # (solve node, parent chain id, parent node chain order)
-        qi = 0
-        while qi < len(queue):
-            node, pc, ptop = queue[qi]
-            qi += 1
-            cid = len(chains)
-            top = len(order)
-            cur = node
-            order.append(cur)
-            while len(kids[cur]) == 1:
-                cur = kids[cur][0]
-                order.append(cur)
-            bot = len(order) - 1
-            chains.append([top, bot - top + 1, ptop, []])
-            if pc >= 0:
-                chains[pc][3].append(cid)
-            for c in kids[cur]:
-                queue.append((c, cid, bot))
-        trees.append(len(order))
-    return np.asarray(order, dtype=np.int64), np.asarray(trees, dtype=np.int64), chains
+    nkids = np.bincount(parent[nonroot], minlength=n)
+    is_head = ~nonroot
+    is_head[nonroot] = nkids[parent[nonroot]] != 1
+    head_of, pos = _pointer_jump(np.where(is_head, idx, parent), (~is_head).astype(np.int64))
+    heads = np.nonzero(is_head)[0]  # increasing node index
+    H = len(heads)
+    cid_of_head = np.full(n, -1, dtype=np.int64)
+    cid_of_head[heads] = np.arange(H)
+    ph = parent[heads]
+    pc = np.where(ph >= 0, cid_of_head[head_of[np.maximum(ph, 0)]], -1)
+    # breadth-first rank, one chain depth at a time
+    depth = np.full(H, -1, dtype=np.int64)
+    rank = np.zeros(H, dtype=np.int64)
+    cur = np.nonzero(pc < 0)[0]  # root chains, in tree order
+    depth[cur] = 0
+    rank[cur] = np.arange(len(cur))
+    d = 0
+    while len(cur):
+        at_d = np.zeros(H, dtype=bool)
+        at_d[cur] = True
+        nxt = np.nonzero((pc >= 0) & at_d[np.maximum(pc, 0)])[0]
+        nxt = nxt[np.lexsort((heads[nxt], rank[pc[nxt]]))]
+        d += 1
+        depth[nxt] = d
+        rank[nxt] = np.arange(len(nxt))
+        cur = nxt
+    bfs = np.lexsort((rank, depth, tree_of[heads]))  # chain ids in breadth-first order
+    new_id = np.empty(H, dtype=np.int64)
+    new_id[bfs] = np.arange(H)
+    length = np.bincount(head_of, minlength=n)[heads][bfs]
+    top = np.zeros(H, dtype=np.int64)
+    top[1:] = np.cumsum(length)[:-1]
+    order = np.empty(n, dtype=np.int64)
+    order[top[new_id[cid_of_head[head_of]]] + pos] = idx
+    cpar = np.where(pc[bfs] >= 0, new_id[np.maximum(pc[bfs], 0)], -1)
+    ptop = np.where(cpar >= 0, top[np.maximum(cpar, 0)] + length[np.maximum(cpar, 0)] - 1, -1)
+    child = np.nonzero(cpar >= 0)[0]
+    child = child[np.argsort(cpar[child], kind="stable")]
+    kid_ptr = np.zeros(H + 1, dtype=np.int64)
+    kid_ptr[1:] = np.cumsum(np.bincount(cpar[child], minlength=H))
+    trees = np.zeros(len(roots) + 1, dtype=np.int64)
+    trees[1:] = np.cumsum(ends - roots)
+    return order, trees, ChainTable(top, length, ptop, cpar, kid_ptr, child, depth[bfs])
+
+
+def chain_order(parent: np.ndarray):
+    """`chain_table` with the chains as a list of `(top, length, parent_top_node,
+    child_chain_ids)`."""
+    order, trees, table = chain_table(parent)
+    return order, trees, table.as_list()
 
 
 def chain_levels(chains) -> np.ndarray:
+    """Height of every chain above its deepest descendant chain (0 for a leaf chain)."""
+    if isinstance(chains, ChainTable):
+        lev = np.zeros(len(chains), dtype=np.int64)
+        for d in range(int(chains.depth.max(initial=0)), 0, -1):
+            c = np.nonzero(chains.depth == d)[0]
+            np.maximum.at(lev, chains.parent[c], lev[c] + 1)
+        return lev
     lev = np.zeros(len(chains), dtype=np.int64)
     for cid in range(len(chains) - 1, -1, -1):  # children come after parents
         kids = chains[cid][3]
         if kids:
             lev[cid] = 1 + max(lev[k] for k in kids)
     return lev
+
+
+def block_schedule(table: ChainTable, blocks_nodes, relative: bool = False):
+    """Chains of every block sorted by level (height), children CSR by first node.
+
+    Returns `(chain_top, chain_len, chain_ptop, chain_cptr, chain_child, level_ptr,
+    per_block)` with `per_block[b] = (chain0, n_chains, level0, n_levels)`; with
+    `relative` the node indices are relative to the block's first node.
+    """
+    lev = chain_levels(table)
+    perm_parts, lp_parts, per_block = [], [], []
+    n_ch = n_lp = 0
+    for (n0, n1) in blocks_nodes:
+        lo, hi = np.searchsorted(table.top, n0), np.searchsorted(table.top, n1)
+        cids = np.arange(lo, hi)
+        cids = cids[np.argsort(lev[cids], kind="stable")]
+        nlev = int(lev[cids].max()) + 1 if len(cids) else 0
+        counts = np.bincount(lev[cids], minlength=nlev)
+        lp_parts.append(np.concatenate([[0], np.cumsum(counts)]))
+        per_block.append((n_ch, len(cids), n_lp, nlev))
+        perm_parts.append(cids)
+        n_ch += len(cids)
+        n_lp += nlev + 1
+    perm = np.concatenate(perm_parts) if perm_parts else np.zeros(0, np.int64)
+    shift = np.zeros(len(table), dtype=np.int64)
+    if relative:
+        for (n0, n1), part in zip(blocks_nodes, perm_parts):
+            shift[part] = n0
+    nk = table.kid_ptr[perm + 1] - table.kid_ptr[perm]
+    cptr = np.zeros(len(perm) + 1, dtype=np.int64)
+    cptr[1:] = np.cumsum(nk)
+    kid_pos = np.repeat(table.kid_ptr[perm] - cptr[:-1], nk) + np.arange(int(cptr[-1]))
+    kids = table.kid[kid_pos]
+    child_top = table.top[kids] - np.repeat(shift[perm], nk)
+    ptop = table.ptop[perm]
+    ptop = np.where(ptop >= 0, ptop - shift[perm], -1)
+    return (table.top[perm] - shift[perm], table.length[perm], ptop, cptr, child_top,
+            np.concatenate(lp_parts) if lp_parts else np.zeros(0, np.int64), per_block)
 
 
 def pack_blocks(tree_ptr: np.ndarray, max_nodes: int, weights: Optional[np.ndarray] = None):
@@ -202,14 +358,18 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
           keep_currents: bool = True) -> Lowered:
     """Lower `problem`. With `keep_currents=False` a channel current gets a state slot
     only where a channel reads it (the calcium pump reads `i_Ca`) or it is recorded;
-    the other currents are not kept in the resident state."""
+    the other currents are not kept in the resident state.
+
+    The work is vectorised over groups of nodes with the same channels (and flags):
+    a group shares its slot layout and node class, and its parameters are gathered
+    as one `(nodes, slots)` matrix."""
     p = problem
     n = p.n_nodes
     B = p.batch
     parent_solve, g_low_s, g_up_s = p.solve_order_system()
     if np.asarray(g_low_s).ndim != 1:
         raise NotImplementedError("axial conductances with a batch dimension are not covered")
-    order, tree_ptr, chains = chain_order(parent_solve)
+    order, tree_ptr, chains = chain_table(parent_solve)
     int2node = np.asarray(p.to_solve, dtype=np.int64)[order]
     node2int = np.empty(n, dtype=np.int64)
     node2int[int2node] = np.arange(n)
@@ -235,55 +395,37 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
     is_comp = np.zeros(n, dtype=bool)
     is_comp[np.asarray(p.comp_inds, dtype=np.int64)] = True
 
-    # ---- node classes: channels, state slots and parameter slots of every node ----
-    chan_at: List[List[int]] = [[] for _ in range(n)]
+    # ---- node groups: nodes with the same channels (and flags) share a layout ----
+    C = len(p.channels)
+    ch_member = np.zeros((n, max(C, 1)), dtype=bool)
     for ci, ch in enumerate(p.channels):
-        for r in np.asarray(ch.inds, dtype=np.int64):
-            chan_at[int(r)].append(ci)
-
-    cols: Dict[bytes, int] = {}
-    col_vecs: List[np.ndarray] = [np.ones(B)]
-    col_info: List[Tuple[str, int]] = [("", -1)]
-    col_members: List[set] = [set()]
-
-    def pval(name: str, r: int) -> Tuple[float, int]:
-        a = np.asarray(p.params[name], dtype=np.float64)
-        if a.ndim == 1:
-            return float(a[r]), 0
-        vec = np.broadcast_to(a[:, r], (B,))
-        if np.all(vec == vec[0]):
-            return float(vec[0]), 0
-        base = float(vec[0]) if vec[0] != 0 else 1.0
-        prof = vec / base
-        key = name.encode() + b"|" + prof.tobytes()
-        if key not in cols:
-            cols[key] = len(col_vecs)
-            col_vecs.append(prof)
-            col_info.append((name, r))
-            col_members.append(set())
-        col_members[cols[key]].add((name, int(r), base))
-        return base, cols[key]
-
+        ch_member[np.asarray(ch.inds, dtype=np.int64), ci] = True
     recorded = {(name, int(r)) for name, r in p.recordings}
+    cur_names = sorted({ch.current for ch in p.channels})
+    rec_cur = np.zeros((n, max(len(cur_names), 1)), dtype=bool)
+    for name, r in p.recordings:
+        if name in cur_names:
+            rec_cur[int(r), cur_names.index(name)] = True
+    keymat = np.concatenate([is_comp[:, None], ch_member, rec_cur], axis=1)
+    _, grp_rep, grp_of_node = _unique_rows(np.packbits(keymat, axis=1))
     readers = {"CaPump"}  # channels whose update reads their current state
-
+    G = len(grp_rep)
+    first_int = np.full(G, n, dtype=np.int64)
+    np.minimum.at(first_int, grp_of_node[int2node], np.arange(n))
     classes: Dict[tuple, int] = {}
     cls_entries: List[np.ndarray] = []
     cls_comp: List[int] = []
-    cls_nslots: List[int] = []
-    node_class = np.zeros(n, dtype=np.int32)
-    soff = np.zeros(n + 1, dtype=np.int64)
-    node_pb: List[List[float]] = []
-    node_pc: List[List[int]] = []
-    slot_names: List[List[str]] = []
-    for i in range(n):
-        r = int(int2node[i])
-        chs = chan_at[r]
+    grp_class = np.zeros(G, dtype=np.int32)
+    grp_names: List[List[str]] = [[] for _ in range(G)]
+    grp_pslots: List[list] = [[] for _ in range(G)]
+    for g in np.argsort(first_int, kind="stable"):  # class ids in order of first use
+        r = int(grp_rep[g])
+        chs = [int(ci) for ci in np.nonzero(ch_member[r, :C])[0]]
         names = ["v"]
         for ci in chs:
-            for s in p.channels[ci].states:
-                if s not in names:
-                    names.append(s)
+            for st_name in p.channels[ci].states:
+                if st_name not in names:
+                    names.append(st_name)
         for ci in chs:
             cn = p.channels[ci].current
             need = (keep_currents or p.channels[ci].type_name in readers
@@ -292,10 +434,7 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
                            for cj in chs))
             if need and cn not in names:
                 names.append(cn)
-        ents = []
-        pk = 0
-        pbs: List[float] = []
-        pcs: List[int] = []
+        ents, pslots, pk = [], [], 0
         for ci in chs:
             ch = p.channels[ci]
             spec = SPECS[ch.type_name]
@@ -304,19 +443,12 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
             e[1] = len(ch.states)
             e[2] = len(ch.params) + len(ch.constants)
             e[3] = names.index(ch.current) if ch.current in names else -1
-            for q, s in enumerate(ch.states):
-                e[4 + q] = names.index(s)
-            e[10] = pk  # parameters are consecutive: p[0] is the first slot
-            for q in range(int(e[2])):
+            for q, st_name in enumerate(ch.states):
+                e[4 + q] = names.index(st_name)
+            for q in range(int(e[2])):  # parameters are consecutive
                 if 10 + q < ENTRY_SHORTS:
                     e[10 + q] = pk + q
-            for q, pn in enumerate(ch.params):
-                b, c = pval(pn, r)
-                pbs.append(b)
-                pcs.append(c)
-            for cval in ch.constants:
-                pbs.append(float(cval))
-                pcs.append(0)
+            pslots += [("p", pn) for pn in ch.params] + [("c", float(cv)) for cv in ch.constants]
             pk += int(e[2])
             ents.append(e)
         key = (bool(is_comp[r]), tuple(names), tuple(tuple(e.tolist()) for e in ents))
@@ -324,155 +456,236 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
             classes[key] = len(cls_entries)
             cls_entries.append(np.stack(ents) if ents else np.zeros((0, ENTRY_SHORTS), np.int16))
             cls_comp.append(int(is_comp[r]))
-            cls_nslots.append(len(names))
-        node_class[i] = classes[key]
-        soff[i + 1] = soff[i] + len(names)
-        node_pb.append(pbs)
-        node_pc.append(pcs)
-        slot_names.append(names)
+        grp_class[g] = classes[key]
+        grp_names[g] = names
+        grp_pslots[g] = pslots
+    grp_int = grp_of_node[int2node]  # group of every internal node
+    node_class = grp_class[grp_int]
+    nslots_g = np.asarray([len(nm) for nm in grp_names], dtype=np.int64)
+    soff = np.zeros(n + 1, dtype=np.int64)
+    soff[1:] = np.cumsum(nslots_g[grp_int])
     cls_prog = np.asarray([program_of(e) for e in cls_entries], dtype=np.int32)
     cls_ptr = np.zeros(len(cls_entries) + 1, dtype=np.int32)
     for c, e in enumerate(cls_entries):
         cls_ptr[c + 1] = cls_ptr[c] + len(e)
     entries = (np.concatenate(cls_entries) if len(cls_entries) else np.zeros((0, ENTRY_SHORTS))).astype(np.int16)
+    grp_nodes = [np.nonzero(grp_int == g)[0] for g in range(G)]  # internal nodes, increasing
+    row_in_grp = np.zeros(n, dtype=np.int64)
+    for g in range(G):
+        row_in_grp[grp_nodes[g]] = np.arange(len(grp_nodes[g]))
+
+    # ---- parameter values and columns, per group (vectorised over its nodes) ----
+    # A parameter that varies over the batch gets one column per distinct batch
+    # profile (value / row-0 value); a node of a trainable group gets its group's
+    # column (one per distinct profile of the group). Columns are numbered at the
+    # end in order of first use (internal node, then parameter slot).
+    col_vecs: List[np.ndarray] = [np.ones(B)]
+    col_keys: Dict[bytes, int] = {}
+    tgroup_of: Dict[str, np.ndarray] = {}
+    for gi, (gname, gnodes) in enumerate(getattr(p, "trainable", []) or []):
+        if gname not in tgroup_of:
+            tgroup_of[gname] = np.full(n, -1, dtype=np.int64)
+        tgroup_of[gname][np.asarray(gnodes, dtype=np.int64)] = gi
+
+    def col_ids(prefix: bytes, rows: np.ndarray, tag: Optional[np.ndarray] = None) -> np.ndarray:
+        """Column of every row of `rows` (m, B): one column per distinct (tag, row)."""
+        keyed = rows if tag is None else np.concatenate([tag[:, None].astype(np.float64), rows], axis=1)
+        urows, _, inv = _unique_rows(keyed)
+        ids = np.empty(len(urows), dtype=np.int64)
+        for u, row in enumerate(urows):
+            pre = prefix if tag is None else prefix + str(int(row[0])).encode() + b"|"
+            vec = row if tag is None else row[1:]
+            kb = pre + np.ascontiguousarray(vec).tobytes()
+            if kb not in col_keys:
+                col_keys[kb] = len(col_vecs)
+                col_vecs.append(np.asarray(vec, dtype=np.float64))
+            ids[u] = col_keys[kb]
+        return ids[inv]
+
+    grp_base: List[np.ndarray] = []
+    grp_col: List[np.ndarray] = []
+    for g in range(G):
+        R = int2node[grp_nodes[g]]
+        m = len(R)
+        P = len(grp_pslots[g])
+        base = np.zeros((m, P))
+        colm = np.zeros((m, P), dtype=np.int64)
+        for k, (kind, val) in enumerate(grp_pslots[g]):
+            if kind == "c":
+                base[:, k] = val
+                continue
+            a = np.asarray(p.params[val], dtype=np.float64)
+            b0 = a[R] if a.ndim == 1 else a[0, R]
+            safe = np.where(b0 != 0, b0, 1.0)
+            tg = tgroup_of[val][R] if val in tgroup_of else np.full(m, -1, dtype=np.int64)
+            trained = tg >= 0
+            base[:, k] = b0
+            if a.ndim == 2:
+                vals = np.broadcast_to(a[:, R], (B, m))
+                vary = np.nonzero(~np.all(vals == vals[:1], axis=0) & ~trained)[0]
+                if len(vary):
+                    base[vary, k] = safe[vary]
+                    colm[vary, k] = col_ids(val.encode() + b"|", (vals[:, vary] / safe[vary]).T)
+            idx = np.nonzero(trained)[0]
+            if len(idx):
+                base[idx, k] = safe[idx]
+                prof = (np.ones((len(idx), B)) if a.ndim == 1
+                        else (np.broadcast_to(a[:, R[idx]], (B, len(idx))) / safe[idx]).T)
+                colm[idx, k] = col_ids(b"group|", prof, tag=tg[idx])
+        grp_base.append(base)
+        grp_col.append(colm)
+
+    # renumber the columns in order of first use
+    ncol = len(col_vecs)
+    Pmax = max([len(ps) for ps in grp_pslots] + [1])
+    first_use = np.full(ncol, np.iinfo(np.int64).max, dtype=np.int64)
+    first_use[0] = -1
+    use_i, use_k, use_c = [], [], []
+    for g in range(G):
+        ii, kk = np.nonzero(grp_col[g])
+        use_i.append(grp_nodes[g][ii])
+        use_k.append(kk)
+        use_c.append(grp_col[g][ii, kk])
+    use_i = np.concatenate(use_i) if use_i else np.zeros(0, np.int64)
+    use_k = np.concatenate(use_k) if use_k else np.zeros(0, np.int64)
+    use_c = np.concatenate(use_c) if use_c else np.zeros(0, np.int64)
+    np.minimum.at(first_use, use_c, use_i * Pmax + use_k)
+    new_of = np.empty(ncol, dtype=np.int64)
+    new_of[np.argsort(first_use, kind="stable")] = np.arange(ncol)
+    grp_col = [new_of[c] for c in grp_col]
+    old_of = np.argsort(new_of)
+    col_vecs = [col_vecs[c] for c in old_of]
     pscale = np.stack(col_vecs, axis=1) if B > 0 else np.ones((1, 1))
+    fu = first_use[old_of]
+    col_info: List[Tuple[str, int]] = [("", -1)]
+    for c in range(1, ncol):
+        i_f, k_f = int(fu[c] // Pmax), int(fu[c] % Pmax)
+        col_info.append((grp_pslots[grp_int[i_f]][k_f][1], int(int2node[i_f])))
+    col_members = _ColMembers(ncol, new_of[use_c], use_i, use_k, grp_pslots, grp_int,
+                              grp_base, row_in_grp, int2node)
 
     # ---- initial state ----
     L = int(soff[-1])
     state0 = np.zeros((B, L), dtype=np.float64)
-    for i in range(n):
-        r = int(int2node[i])
-        for k, nm in enumerate(slot_names[i]):
-            a = np.asarray(p.states[nm], dtype=np.float64) if nm in p.states else None
-            if a is None:
+    for g in range(G):
+        I = grp_nodes[g]
+        R = int2node[I]
+        for k, nm in enumerate(grp_names[g]):
+            if nm not in p.states:
                 continue
-            state0[:, soff[i] + k] = a[..., r] if a.ndim == 1 else np.broadcast_to(a[:, r], (B,))
+            a = np.asarray(p.states[nm], dtype=np.float64)
+            state0[:, soff[I] + k] = a[R][None, :] if a.ndim == 1 else np.broadcast_to(a[:, R], (B, len(R)))
 
-    # ---- blocks, chains ordered by level inside each block ----
-    lev = chain_levels(chains)
+    # ---- blocks: parameter runs, chains ordered by level inside each block ----
     blocks_nodes = pack_blocks(tree_ptr, max_block_nodes)
-    # Parameter blocks: nodes with identical parameters (values and columns) share
-    # one run of parameter slots inside their block of trees.
-    pbase: List[float] = []
-    pcol: List[int] = []
+    # Nodes of a block with identical parameters (values and columns) share one run
+    # of parameter slots; runs are laid out in order of first use inside the block.
+    pbase_parts: List[np.ndarray] = []
+    pcol_parts: List[np.ndarray] = []
+    gk_parts: List[np.ndarray] = []
     poff = np.zeros(n, dtype=np.int64)
     pranges = []
+    total = 0
     for (n0, n1) in blocks_nodes:
-        start = len(pbase)
-        seen: Dict[tuple, int] = {}
-        for i in range(n0, n1):
-            key = (tuple(node_pb[i]), tuple(node_pc[i]))
-            if key not in seen:
-                seen[key] = len(pbase)
-                pbase.extend(node_pb[i])
-                pcol.extend(node_pc[i])
-            poff[i] = seen[key]
-        pranges.append((start, len(pbase) - start))
-    chain_top, chain_len, chain_ptop, chain_cptr, chain_child = [], [], [], [0], []
-    level_ptr: List[int] = []
-    blocks = []
-    tops = np.asarray([c[0] for c in chains], dtype=np.int64)
-    cid_sorted = np.argsort(tops, kind="stable")
-    tops_sorted = tops[cid_sorted]
-    max_levels = 0
-    for (n0, n1) in blocks_nodes:
-        lo = np.searchsorted(tops_sorted, n0)
-        hi = np.searchsorted(tops_sorted, n1)
-        cids = cid_sorted[lo:hi]
-        cids = cids[np.argsort(lev[cids], kind="stable")]
-        nlev = int(lev[cids].max()) + 1 if len(cids) else 0
-        max_levels = max(max_levels, nlev)
-        chain0 = len(chain_top)
-        level0 = len(level_ptr)
-        counts = np.bincount(lev[cids], minlength=nlev)
-        level_ptr.extend(np.concatenate([[0], np.cumsum(counts)]).tolist())
-        for c in cids:
-            top, ln, ptop, kids = chains[c]
-            chain_top.append(top)
-            chain_len.append(ln)
-            chain_ptop.append(ptop)
-            for k in kids:
-                chain_child.append(chains[k][0])
-            chain_cptr.append(len(chain_child))
-        bi = len(blocks)
-        blocks.append([n0, n1 - n0, int(soff[n0]), int(soff[n1] - soff[n0]), chain0, len(cids),
-                       level0, nlev, pranges[bi][0], pranges[bi][1], 0, 0])
+        start = total
+        runs: Dict[bytes, list] = {}  # content -> [first node, base, col, node lists]
+        for g in np.unique(grp_int[n0:n1]):
+            gn = grp_nodes[g]
+            I = gn[np.searchsorted(gn, n0):np.searchsorted(gn, n1)]
+            P = len(grp_pslots[g])
+            rb = grp_base[g][row_in_grp[I]]
+            rc = grp_col[g][row_in_grp[I]]
+            rows = np.concatenate([rb, rc.astype(np.float64)], axis=1) if P else np.zeros((len(I), 1))
+            urows, ufirst, inv_r = _unique_rows(rows)
+            if len(urows) > 1:
+                srt = np.argsort(inv_r, kind="stable")
+                splits = np.split(I[srt], np.cumsum(np.bincount(inv_r, minlength=len(urows)))[:-1])
+            else:
+                splits = [I]
+            for u in range(len(urows)):
+                kb = (np.ascontiguousarray(rb[ufirst[u]]).tobytes() + b"|"
+                      + np.ascontiguousarray(rc[ufirst[u]]).tobytes())
+                if kb in runs:
+                    ent = runs[kb]
+                    ent[0] = min(ent[0], int(I[ufirst[u]]))
+                    ent[3].append(splits[u])
+                else:
+                    runs[kb] = [int(I[ufirst[u]]), rb[ufirst[u]], rc[ufirst[u]], [splits[u]]]
+        for first, rbase, rcol, node_lists in sorted(runs.values(), key=lambda e: e[0]):
+            for nl in node_lists:
+                poff[nl] = total
+            pbase_parts.append(rbase)
+            pcol_parts.append(rcol)
+            nzr = rcol != 0
+            gk_parts.append(np.where(nzr, np.cumsum(nzr) - 1, -1))
+            total += len(rbase)
+        pranges.append((start, total - start))
+    pbase = np.concatenate(pbase_parts) if pbase_parts else np.zeros(0)
+    pcol = np.concatenate(pcol_parts).astype(np.int64) if pcol_parts else np.zeros(0, dtype=np.int64)
+    gk = (np.concatenate(gk_parts) if gk_parts else np.zeros(0)).astype(np.int32)
+    (chain_top, chain_len, chain_ptop, chain_cptr, chain_child, level_ptr,
+     per_block) = block_schedule(chains, blocks_nodes)
+    max_levels = max([pb[3] for pb in per_block] + [0])
+    blocks = [[n0, n1 - n0, int(soff[n0]), int(soff[n1] - soff[n0]), pb[0], pb[1], pb[2], pb[3],
+               pr[0], pr[1], 0, 0] for (n0, n1), pb, pr in zip(blocks_nodes, per_block, pranges)]
 
     # ---- stimulus CSR (internal node -> stimulus columns) ----
     stim_inds = np.asarray(p.stim_inds, dtype=np.int64)
-    stim_lists: List[List[int]] = [[] for _ in range(n)]
-    for q, r in enumerate(stim_inds):
-        stim_lists[int(node2int[r])].append(q)
+    s_int = node2int[stim_inds] if len(stim_inds) else np.zeros(0, np.int64)
+    stim_idx = np.argsort(s_int, kind="stable").astype(np.int32)
     stim_ptr = np.zeros(n + 1, dtype=np.int32)
-    for i in range(n):
-        stim_ptr[i + 1] = stim_ptr[i] + len(stim_lists[i])
-    stim_idx = np.asarray([q for lst in stim_lists for q in lst], dtype=np.int32)
+    stim_ptr[1:] = np.cumsum(np.bincount(s_int, minlength=n))
     stim = None
     if p.stim is not None and len(stim_inds):
         stim = np.ascontiguousarray(np.transpose(np.asarray(p.stim, dtype=np.float64), (2, 0, 1)))
 
     # ---- recordings CSR ----
-    rec_lists: List[List[Tuple[int, int]]] = [[] for _ in range(n)]
-    for col, (name, r) in enumerate(p.recordings):
+    rec_int, rec_sl = [], []
+    for name, r in p.recordings:
         i = int(node2int[int(r)])
-        if name in slot_names[i]:
-            sl = slot_names[i].index(name)
+        names = grp_names[grp_int[i]]
+        if name in names:
+            sl = names.index(name)
         elif name in p.current_names or name in p.states:
             sl = -1
         else:
             raise NotImplementedError(f"recording of `{name}` is not covered")
-        rec_lists[i].append((sl, col))
+        rec_int.append(i)
+        rec_sl.append(sl)
+    rec_int = np.asarray(rec_int, dtype=np.int64)
+    r_order = np.argsort(rec_int, kind="stable")
+    rec_slot = np.asarray(rec_sl, dtype=np.int32)[r_order] if len(rec_sl) else np.zeros(0, np.int32)
+    rec_col = r_order.astype(np.int32)
     rec_ptr = np.zeros(n + 1, dtype=np.int32)
-    for i in range(n):
-        rec_ptr[i + 1] = rec_ptr[i] + len(rec_lists[i])
-    rec_slot = np.asarray([s for lst in rec_lists for s, _ in lst], dtype=np.int32)
-    rec_col = np.asarray([c for lst in rec_lists for _, c in lst], dtype=np.int32)
+    if len(rec_int):
+        rec_ptr[1:] = np.cumsum(np.bincount(rec_int, minlength=n))
 
     def i32(x):
         return np.ascontiguousarray(np.asarray(x, dtype=np.int32))
 
-    # ---- gradient slots: every node owns one float32 accumulator per trainable
-    # parameter (column != 0) for the adjoint kernel ----
-    pcol_arr = np.asarray(pcol, dtype=np.int64)
-    gk = np.full(len(pcol_arr), -1, dtype=np.int32)
-    run_len = np.zeros(n, dtype=np.int64)
-    for i in range(n):
-        run_len[i] = len(node_pb[i])
-    done_runs = set()
-    for i in range(n):
-        st0 = int(poff[i])
-        key = (st0, int(run_len[i]))  # empty runs share their start with the next run
-        if key in done_runs:
-            continue
-        done_runs.add(key)
-        rk = 0
-        for q in range(st0, st0 + int(run_len[i])):
-            if pcol_arr[q] != 0:
-                gk[q] = rk
-                rk += 1
+    # ---- gradient slots: every node owns one accumulator per trainable parameter
+    # (column != 0) of its run for the adjoint kernel (ranks in `gk`) ----
+    n_train = np.zeros(n, dtype=np.int64)
+    for g in range(G):
+        if len(grp_pslots[g]) and len(grp_nodes[g]):
+            n_train[grp_nodes[g]] = np.count_nonzero(grp_col[g], axis=1)
     gbase = np.zeros(n, dtype=np.int32)
     max_gslots = 0
-    for (n0, n1) in blocks_nodes:
-        acc = 0
-        for i in range(n0, n1):
-            gbase[i] = acc
-            st0 = int(poff[i])
-            acc += int(np.count_nonzero(pcol_arr[st0:st0 + int(run_len[i])]))
-        max_gslots = max(max_gslots, acc)
+    for bi, (n0, n1) in enumerate(blocks_nodes):
+        c = np.cumsum(n_train[n0:n1])
+        gbase[n0:n1] = np.concatenate([[0], c[:-1]])
+        blocks[bi][10] = int(c[-1]) if len(c) else 0  # gradient slots of the block
+        max_gslots = max(max_gslots, blocks[bi][10])
 
     # ---- parent / children in internal order (for the delta form of the step) ----
     par_int = np.full(n, -1, dtype=np.int64)
     ps = np.asarray(parent_solve, dtype=np.int64)[order]
     has_par = ps >= 0
     par_int[has_par] = solve2int[ps[has_par]]
-    kid_lists: List[List[int]] = [[] for _ in range(n)]
-    for i in range(n):
-        if par_int[i] >= 0:
-            kid_lists[int(par_int[i])].append(i)
+    child = np.nonzero(has_par)[0]
+    kid = child[np.argsort(par_int[child], kind="stable")].astype(np.int32)
     kid_ptr = np.zeros(n + 1, dtype=np.int32)
-    for i in range(n):
-        kid_ptr[i + 1] = kid_ptr[i] + len(kid_lists[i])
-    kid = np.asarray([c for lst in kid_lists for c in lst], dtype=np.int32)
+    kid_ptr[1:] = np.cumsum(np.bincount(par_int[child], minlength=n))
 
     return Lowered(
         n_nodes=n,
@@ -495,7 +708,7 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
         pcol=i32(pcol),
         pscale=np.ascontiguousarray(pscale),
         col_info=col_info,
-        col_members=[sorted(m) for m in col_members],
+        col_members=col_members,
         chain_top=i32(chain_top),
         chain_len=i32(chain_len),
         chain_ptop=i32(chain_ptop),
@@ -517,7 +730,7 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
         rec_col=rec_col,
         n_rec=len(p.recordings),
         state0=state0,
-        slot_names=slot_names,
+        slot_names=_SlotNames(grp_names, grp_int),
         dt=float(p.dt),
         n_steps=int(p.n_steps),
         max_levels=max_levels,

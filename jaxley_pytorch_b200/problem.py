@@ -70,6 +70,10 @@ class Problem:
     synapses: List[SynapseType] = field(default_factory=list)
     batch: int = 1
     current_names: List[str] = field(default_factory=list)
+    # Trainable parameter groups `(parameter name, reference nodes)`: the nodes of a
+    # group share one scale column and so one gradient, like one `make_trainable`
+    # call on a view in the reference (`modules/base.py:1625`).
+    trainable: List[Tuple[str, np.ndarray]] = field(default_factory=list)
 
     def solve_order_system(self):
         """Per solve position `j`: parent, `g_low[j]` (coupling of row `j` to its
@@ -315,7 +319,10 @@ def save_problem(problem: Problem, path: str, **extra) -> None:
         "recordings": [[n, int(i)] for n, i in problem.recordings],
         "params": list(problem.params), "states": list(problem.states),
         "channels": [], "synapses": [],
+        "trainable": [name for name, _ in problem.trainable],
     }
+    for q, (_, nodes) in enumerate(problem.trainable):
+        arrays[f"trainable/{q}"] = np.asarray(nodes, dtype=np.int64)
     for k, v in problem.params.items():
         arrays[f"param/{k}"] = v
     for k, v in problem.states.items():
@@ -377,6 +384,7 @@ def load_problem(path: str):
         stim=z["stim"] if "stim" in z else None,
         recordings=[(n, i) for n, i in meta["recordings"]], synapses=synapses,
         batch=meta["batch"], current_names=meta["current_names"],
+        trainable=[(n, z[f"trainable/{q}"]) for q, n in enumerate(meta.get("trainable", []))],
     )
     extra = {k[len("extra/"):]: z[k] for k in z.files if k.startswith("extra/")}
     return prob, extra

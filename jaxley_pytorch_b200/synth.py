@@ -18,10 +18,13 @@ Configurations (sizes from the benchmark description):
   dendrites: NaTs2T, SKv3_1, M, H; Leak everywhere) with every conductance scaled by
   U[0.5, 1.5] per parameter set; batch 256, dt 0.025 ms, 4000 steps.
 * `config_uneven`: 4096 cells of log-uniform(4, 3000) compartments and depth 1-60,
-  HH or L5PC, each with its own step current.
+  HH or L5PC, each with its own step current (1 ms, delay U[1, 5] ms, amplitude
+  U[0.05, 0.5] nA) and its own trainable conductances (one column per cell and
+  conductance), 2000 steps.
 """
 from __future__ import annotations
 
+import bisect
 from typing import Dict, List, Optional, Sequence, Tuple
 
 import numpy as np
@@ -32,73 +35,79 @@ from .problem import Problem, SynapseType
 PI = np.pi
 
 
+class CompIndex:
+    """Node of compartment `(branch, comp)` of a cell: `index[(b, k)]`."""
+
+    def __init__(self, start: np.ndarray, ncomp: np.ndarray):
+        self.start, self.ncomp = start, ncomp
+
+    def __getitem__(self, bk):
+        b, k = int(bk[0]), int(bk[1])
+        if not 0 <= k < int(self.ncomp[b]):
+            raise KeyError(bk)
+        return int(self.start[b]) + k
+
+
 def morphology(branch_parents: Sequence[int], ncomp: Sequence[int], comp_radius: Sequence[np.ndarray],
                comp_length: Sequence[np.ndarray], r_a: float = 5000.0, cm: float = 1.0):
     """Nodes and the tree system of one cell. Returns a dict of node-order arrays
-    (node order = solve order) and the compartment index of every (branch, comp)."""
+    (node order = solve order) and the compartment index of every (branch, comp).
+
+    Branches are numbered breadth first; a branch contributes its compartments and,
+    when it has children, one branchpoint node after them."""
     nb = len(branch_parents)
+    bpar = np.asarray(branch_parents, dtype=np.int64)
+    nc = np.asarray(ncomp, dtype=np.int64)
     children: List[List[int]] = [[] for _ in range(nb)]
     for b in range(1, nb):
-        children[int(branch_parents[b])].append(b)
-    # Breadth-first numbering over (branch, compartment) and branchpoint nodes.
-    order: List[Tuple[str, int, int]] = []  # ("c", branch, comp) or ("bp", branch, -1)
-    parent: List[int] = []
-    queue = [(0, -1)]
+        children[int(bpar[b])].append(b)
+    bfs = [0]
     qi = 0
-    comp_node: Dict[Tuple[int, int], int] = {}
-    bp_node: Dict[int, int] = {}
-    while qi < len(queue):
-        b, pnode = queue[qi]
+    while qi < len(bfs):
+        bfs.extend(children[bfs[qi]])
         qi += 1
-        prev = pnode
-        for k in range(int(ncomp[b])):
-            comp_node[(b, k)] = len(order)
-            order.append(("c", b, k))
-            parent.append(prev)
-            prev = comp_node[(b, k)]
-        if children[b]:
-            bp_node[b] = len(order)
-            order.append(("bp", b, -1))
-            parent.append(prev)
-            for c in children[b]:
-                queue.append((c, bp_node[b]))
-    n = len(order)
-    is_comp = np.array([o[0] == "c" for o in order])
+    bfs = np.asarray(bfs, dtype=np.int64)
+    has_kids = np.bincount(bpar[1:], minlength=nb) > 0 if nb > 1 else np.zeros(nb, dtype=bool)
+    size = nc + has_kids
+    start = np.zeros(nb, dtype=np.int64)
+    start[bfs] = np.concatenate([[0], np.cumsum(size[bfs])[:-1]])
+    n = int(size.sum())
+    bp_of = start + nc  # branchpoint node of a branch with children
+    is_comp = np.ones(n, dtype=bool)
+    is_comp[bp_of[has_kids]] = False
+    parent = np.arange(-1, n - 1, dtype=np.int64)  # within a branch: the previous node
+    first = start[bfs]
+    parent[first] = np.where(bpar[bfs] >= 0, bp_of[np.maximum(bpar[bfs], 0)], -1)
     radius = np.ones(n)
     length = np.ones(n)
-    for j, (kind, b, k) in enumerate(order):
-        if kind == "c":
-            radius[j] = comp_radius[b][k]
-            length[j] = comp_length[b][k]
+    cidx = np.repeat(start, nc) + (np.arange(int(nc.sum())) - np.repeat(np.cumsum(nc) - nc, nc))
+    radius[cidx] = np.concatenate([np.asarray(comp_radius[b], dtype=np.float64)[:nc[b]] for b in range(nb)])
+    length[cidx] = np.concatenate([np.asarray(comp_length[b], dtype=np.float64)[:nc[b]] for b in range(nb)])
     area = 2 * PI * radius * length
     rl = (length / 2) / (radius**2 * PI)  # resistive load of half a compartment
     ra = np.full(n, float(r_a))
     cmv = np.full(n, float(cm))
-    parent = np.asarray(parent, dtype=np.int64)
     # Axial conductances per directed edge (sink row), utils/morph_attributes.py:380-433.
     g_low = np.zeros(n)  # sink = node j, source = parent
     g_up = np.zeros(n)  # sink = parent, source = node j
-    for j in range(1, n):
-        p = parent[j]
-        if is_comp[j] and is_comp[p]:  # compartment to compartment
-            r = rl[p] * ra[p] + rl[j] * ra[j]
-            g_low[j] = 1 / r / area[j] / cmv[j] * 1e7
-            g_up[j] = 1 / r / area[p] / cmv[p] * 1e7
-        elif not is_comp[j]:  # j is a branchpoint, parent compartment
-            r = rl[p] * ra[p]
-            g_low[j] = 1 / r  # c2bp: not divided by area
-            g_up[j] = 1 / r / area[p] / cmv[p] * 1e7  # bp2c
-        else:  # compartment whose parent is a branchpoint
-            r = rl[j] * ra[j]
-            g_low[j] = 1 / r / area[j] / cmv[j] * 1e7  # bp2c
-            g_up[j] = 1 / r  # c2bp
+    j = np.arange(1, n)
+    p = parent[j]
+    cc = is_comp[j] & is_comp[p]  # compartment to compartment
+    c2bp = ~is_comp[j]  # j is a branchpoint, its parent a compartment
+    r_cc = rl[p] * ra[p] + rl[j] * ra[j]
+    r_pc = rl[p] * ra[p]
+    r_jc = rl[j] * ra[j]  # compartment whose parent is a branchpoint
+    g_low[j] = np.where(cc, 1 / r_cc / area[j] / cmv[j] * 1e7,
+                        np.where(c2bp, 1 / r_pc, 1 / r_jc / area[j] / cmv[j] * 1e7))
+    g_up[j] = np.where(cc, 1 / r_cc / area[p] / cmv[p] * 1e7,
+                       np.where(c2bp, 1 / r_pc / area[p] / cmv[p] * 1e7, 1 / r_jc))
     depth_of_branch = np.zeros(nb, dtype=np.int64)
-    for b in range(1, nb):
-        depth_of_branch[b] = depth_of_branch[branch_parents[b]] + 1
+    for b in bfs[1:]:
+        depth_of_branch[b] = depth_of_branch[bpar[b]] + 1
     return {
         "n": n, "parent": parent, "is_comp": is_comp, "area": area, "cm": cmv,
         "radius": radius, "length": length, "g_low": g_low, "g_up": g_up,
-        "comp_node": comp_node, "order": order, "branch_depth": depth_of_branch,
+        "comp_node": CompIndex(start, nc), "branch_depth": depth_of_branch,
     }
 
 
@@ -347,6 +356,7 @@ def config_uneven(n_cells: int = 4096, seed: int = 0, n_steps: int = 2000, min_c
     """Cells of log-uniform compartment counts and bounded depth, HH or L5PC."""
     rng = np.random.default_rng(seed)
     cells, chans, stims, recs = [], [], [], []
+    train_local = []  # per cell: [(param name, local node indices)]
     t_max = n_steps * 0.025
     for c in range(n_cells):
         ncomp_total = int(round(np.exp(rng.uniform(np.log(min_comp), np.log(max_comp)))))
@@ -355,27 +365,36 @@ def config_uneven(n_cells: int = 4096, seed: int = 0, n_steps: int = 2000, min_c
         depth_cap = int(rng.integers(1, max_depth + 1))
         parents = [-1]
         bdepth = [0]
+        elig = [0] if depth_cap > 0 else []  # branches that may take children, increasing
         for b in range(1, nb):
-            cand = [q for q in range(max(0, b - 64), b) if bdepth[q] < depth_cap]
-            p = int(rng.choice(cand)) if cand else 0
+            lo = bisect.bisect_left(elig, b - 64)  # a parent among the 64 previous branches
+            p = elig[lo + int(rng.integers(0, len(elig) - lo))] if lo < len(elig) else 0
             parents.append(p)
             bdepth.append(bdepth[p] + 1)
+            if bdepth[b] < depth_cap:
+                elig.append(b)
         lengths = rng.lognormal(np.log(30.0), 0.5, size=nb)
         radius = np.clip(2.0 - 0.05 * np.asarray(bdepth), 0.3, 2.0)
         cell = morphology(parents, [ncomp] * nb, [np.full(ncomp, r) for r in radius],
                           [np.full(ncomp, L / ncomp) for L in lengths], r_a=100.0)
         cells.append(cell)
         if rng.random() < l5pc_fraction and nb > 1:
-            chans.append(l5pc_channels(cell, None, ncomp_soma=ncomp))
+            cl = l5pc_channels(cell, None, ncomp_soma=ncomp)
+            chans.append(cl)
+            train_local.append([(k, nodes) for _, nodes, _, vals in cl for k in vals if k in L5PC_SCALED])
         else:
             comps = np.nonzero(cell["is_comp"])[0]
             chans.append([("HH", comps, "HH", {})])
+            train_local.append([(k, comps) for k in ("HH_gNa", "HH_gK", "HH_gLeak")])
         delay = float(rng.uniform(1, 5))
         amp = float(rng.uniform(0.05, 0.5))
         stims.append((c, (0, 0), step_current(delay, 1.0, amp, 0.025, t_max)))
         recs.append(("v", c, (0, 0)))
     prob = assemble(cells, chans, batch=1, dt=0.025, n_steps=n_steps, v0=-65.0, stim=stims,
                     recordings=recs)
+    offs = np.cumsum([0] + [c["n"] for c in cells])
+    prob.trainable = [(k, np.asarray(nodes) + offs[c]) for c in range(n_cells)
+                      for k, nodes in train_local[c]]
     if "CaCon_i" in prob.states:
         prob.states["CaCon_i"] = np.where(prob.states["CaCon_i"] == 0, 5e-05, prob.states["CaCon_i"])
     if "CaCon_e" in prob.states:
