@@ -104,7 +104,7 @@ typedef struct {
   int32_t chain0, n_chains;   /* chains of the block, sorted by level */
   int32_t level0, n_levels;   /* level_ptr[level0 .. level0 + n_levels] */
   int32_t pslot0, n_pslots;   /* parameter-slot range */
-  int32_t pad0, pad1;
+  int32_t n_gslots, pad1;     /* gradient slots of the block (adjoint sizing) */
 } JxbBlock;
 
 typedef struct {
@@ -181,6 +181,13 @@ typedef struct {
   const void* rec_grad;       /* (T + 1, batch, n_rec) gradient of the recordings */
   double* pgrad;              /* (batch, n_cols) float64, accumulated: d loss / d pscale */
   int32_t mode, pad2;         /* 0 = step, 1 = initial currents only */
+  /* Optional work areas in global memory instead of shared memory, for blocks whose
+   * working set exceeds the shared memory of a CTA: item i uses the bytes
+   * [gscratch + i * gscratch_stride, + gscratch_stride). gscratch is 256-byte aligned
+   * and gscratch_stride a multiple of 256 of at least jxb_sim_smem_bytes(args, kind).
+   * Null: the work areas live in shared memory. */
+  void* gscratch;
+  int64_t gscratch_stride;
 } JxbSimArgs;
 
 int jxb_sim_forward(const JxbSimArgs* args, void* stream);

@@ -70,6 +70,7 @@ class JxbSimArgs(C.Structure):
         ("traj", _p), ("traj_piv", _p),
         ("adj", _p), ("rec_grad", _p), ("pgrad", _p),
         ("mode", C.c_int32), ("pad2", C.c_int32),
+        ("gscratch", _p), ("gscratch_stride", C.c_int64),
     ]
 
 

@@ -21,6 +21,8 @@
 #include <stdio.h>
 #include <string.h>
 
+#include <mutex>
+
 #include "jxb.h"
 #include "jxb_node.cuh"
 #include "jxb_prog.cuh"
@@ -413,11 +415,19 @@ __device__ void run_steps(const JxbSimArgs& a, const JxbBlock& blk, int row0, in
   __syncthreads();
 }
 
-template <typename T, int NT>
+// Work areas of the CTA: dynamic shared memory, or (GM) the item's range of the
+// caller's global scratch for blocks too large for shared memory.
+template <bool GM>
+__device__ __forceinline__ char* work_base(const JxbSimArgs& a, char* smem_raw) {
+  if constexpr (GM) return (char*)a.gscratch + (size_t)blockIdx.x * (size_t)a.gscratch_stride;
+  return smem_raw;
+}
+
+template <typename T, int NT, bool GM>
 __global__ void __launch_bounds__(NT) sim_forward_kernel(JxbSimArgs a) {
   extern __shared__ __align__(16) char smem_raw[];
   SimSmem<T> sm;
-  sim_smem_layout<T>(a, false, &sm, smem_raw);
+  sim_smem_layout<T>(a, false, &sm, work_base<GM>(a, smem_raw));
   const JxbItem item = a.items[blockIdx.x];
   const JxbBlock blk = a.blocks[item.block];
   const int rows = item.n_rows, row0 = item.row0;
@@ -538,11 +548,11 @@ __device__ void block_solve_pivots(const JxbBlock& blk, const SimSmem<T>& sm, in
   }
 }
 
-template <typename T, int NT>
+template <typename T, int NT, bool GM>
 __global__ void __launch_bounds__(NT) sim_backward_kernel(JxbSimArgs a) {
   extern __shared__ __align__(16) char smem_raw[];
   SimSmem<T> sm;
-  sim_smem_layout<T>(a, true, &sm, smem_raw);
+  sim_smem_layout<T>(a, true, &sm, work_base<GM>(a, smem_raw));
   const JxbItem item = a.items[blockIdx.x];
   const JxbBlock blk = a.blocks[item.block];
   const int rows = item.n_rows, row0 = item.row0;
@@ -632,13 +642,58 @@ __global__ void __launch_bounds__(NT) sim_backward_kernel(JxbSimArgs a) {
   }
 }
 
+template <typename T, int NT>
+void (*pick_kernel(bool backward, bool gm))(JxbSimArgs) {
+  if (gm) return backward ? sim_backward_kernel<T, NT, true> : sim_forward_kernel<T, NT, true>;
+  return backward ? sim_backward_kernel<T, NT, false> : sim_forward_kernel<T, NT, false>;
+}
+
+// Largest dynamic shared memory already granted to a kernel on a device:
+// cudaFuncSetAttribute is called only when a launch needs more, so steady-state
+// launches make no extra runtime call.
+struct SmemGrant {
+  const void* fn;
+  int device;
+  size_t bytes;
+};
+static SmemGrant g_grants[256];
+static int g_n_grants = 0;
+static std::mutex g_grants_mu;
+
+static cudaError_t grant_smem(const void* fn, size_t smem) {
+  int dev = 0;
+  cudaError_t e = cudaGetDevice(&dev);
+  if (e != cudaSuccess) return e;
+  std::lock_guard<std::mutex> lock(g_grants_mu);
+  for (int i = 0; i < g_n_grants; ++i)
+    if (g_grants[i].fn == fn && g_grants[i].device == dev) {
+      if (g_grants[i].bytes >= smem) return cudaSuccess;
+      e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      if (e == cudaSuccess) g_grants[i].bytes = smem;
+      return e;
+    }
+  e = cudaFuncSetAttribute(fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e == cudaSuccess && g_n_grants < 256) g_grants[g_n_grants++] = {fn, dev, smem};
+  return e;
+}
+
 template <typename T>
 int launch_sim(const JxbSimArgs& a, bool backward, cudaStream_t stream) {
-  const size_t smem = sim_smem_layout<T>(a, backward, nullptr, nullptr);
-  if (smem > 227 * 1024) {
-    snprintf(g_err, sizeof(g_err), "work item needs %zu bytes of shared memory", smem);
+  const size_t need = sim_smem_layout<T>(a, backward, nullptr, nullptr);
+  const bool gm = a.gscratch != nullptr;
+  if (gm) {
+    if (((uintptr_t)a.gscratch & 255) != 0 || a.gscratch_stride <= 0 || (a.gscratch_stride & 255) != 0 ||
+        (size_t)a.gscratch_stride < need) {
+      snprintf(g_err, sizeof(g_err),
+               "gscratch must be 256-byte aligned with a stride (multiple of 256) of at least %zu bytes",
+               need);
+      return JXB_ERR_ARG;
+    }
+  } else if (need > 227 * 1024) {
+    snprintf(g_err, sizeof(g_err), "work item needs %zu bytes of shared memory", need);
     return JXB_ERR_SMEM;
   }
+  const size_t smem = gm ? 0 : need;
   const int threads = a.threads > 0 ? a.threads : 256;
   if (threads % 32 != 0 || threads > 1024) {
     snprintf(g_err, sizeof(g_err), "threads must be a multiple of 32 up to 1024");
@@ -647,12 +702,12 @@ int launch_sim(const JxbSimArgs& a, bool backward, cudaStream_t stream) {
   // Register budget by launch size: up to 256 threads, 512, 1024.
   void (*kern)(JxbSimArgs);
   if (threads <= 256)
-    kern = backward ? sim_backward_kernel<T, 256> : sim_forward_kernel<T, 256>;
+    kern = pick_kernel<T, 256>(backward, gm);
   else if (threads <= 512)
-    kern = backward ? sim_backward_kernel<T, 512> : sim_forward_kernel<T, 512>;
+    kern = pick_kernel<T, 512>(backward, gm);
   else
-    kern = backward ? sim_backward_kernel<T, 1024> : sim_forward_kernel<T, 1024>;
-  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    kern = pick_kernel<T, 1024>(backward, gm);
+  cudaError_t e = grant_smem((const void*)kern, smem);
   if (e != cudaSuccess) {
     set_err("cudaFuncSetAttribute", e);
     return JXB_ERR_LAUNCH;

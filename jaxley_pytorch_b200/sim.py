@@ -36,7 +36,8 @@ class DeviceModel:
     """A lowered model resident on one GPU."""
 
     def __init__(self, low: Lowered, dtype: torch.dtype = torch.float32, device="cuda",
-                 rows_per_item: int = 1, threads: int = 256, programs: bool = True):
+                 rows_per_item: int = 1, threads: int = 256, programs: bool = True,
+                 smem_limit: Optional[int] = None):
         self.low = low
         self.dtype = dtype
         self.device = torch.device(device)
@@ -71,40 +72,97 @@ class DeviceModel:
             self.t["cls_prog"] = torch.zeros_like(self.t["cls_prog"])
         self.pscale = f(low.pscale)
         self.stim = f(low.stim) if low.stim is not None else None
-        blocks = low.blocks
-        self.max_nodes = int(blocks[:, 1].max())
-        self.max_slots = int(blocks[:, 3].max())
-        self.max_chains = int(blocks[:, 5].max())
-        self.max_levels = int(blocks[:, 7].max())
-        self.max_pslots = max(1, int(blocks[:, 9].max()))
-        cp = low.chain_cptr
-        self.max_child = int(max(cp[b[4] + b[5]] - cp[b[4]] for b in blocks))
         self.threads = threads
-        self.launches = 0  # launches issued through this model (both kernels)
+        self.launches = 0  # kernel launches issued through this model
         self.timed_kind: Optional[str] = None  # "forward"/"backward": record events
         self.events: List = []
+        self._sides: List[torch.cuda.Stream] = []
+        self._scratch: Dict[str, torch.Tensor] = {}
+        self.smem_limit = smem_limit if smem_limit is not None else self._device_smem_limit()
         self.set_rows_per_item(rows_per_item)
 
+    def _device_smem_limit(self) -> int:
+        if self.device.type == "cuda" and torch.cuda.is_available():
+            props = torch.cuda.get_device_properties(self.device)
+            v = getattr(props, "shared_memory_per_block_optin", 0)
+            if v:
+                return int(v)
+        return 227 * 1024
+
+    def _block_maxima(self, bidx: np.ndarray) -> Dict[str, int]:
+        blocks = self.low.blocks[bidx]
+        cp = self.low.chain_cptr
+        return {
+            "max_nodes": int(blocks[:, 1].max()), "max_slots": int(blocks[:, 3].max()),
+            "max_chains": int(blocks[:, 5].max()), "max_levels": int(blocks[:, 7].max()),
+            "max_pslots": max(1, int(blocks[:, 9].max())), "max_gslots": max(1, int(blocks[:, 10].max())),
+            "max_child": int(max(cp[b[4] + b[5]] - cp[b[4]] for b in blocks)),
+        }
+
+    def _layout_bytes(self, maxima: Dict[str, int], backward: bool) -> int:
+        a = _lib.JxbSimArgs()
+        a.dtype = self.code
+        a.max_rows = self.rows_per_item
+        for k, v in maxima.items():
+            setattr(a, k, v)
+        a.n_entries = int(self.low.entries.shape[0])
+        a.n_classes = len(self.low.cls_comp)
+        return int(_lib.load().jxb_sim_smem_bytes(C.byref(a), int(backward)))
+
     def set_rows_per_item(self, rows: int) -> None:
+        """Work items = (block, rows), grouped per launch kind by the shared memory
+        their block needs: one launch per size class (up to a quarter, a half, all of
+        a CTA's shared memory, so that small blocks keep several CTAs per SM) and one
+        for blocks over the limit, whose work areas live in global scratch. The
+        groups run concurrently on forked streams."""
         low = self.low
         B = low.batch
         rows = max(1, min(int(rows), B))
-        items = []
-        for b in range(len(low.blocks)):
-            for r0 in range(0, B, rows):
-                items.append([b, r0, min(rows, B - r0), 0])
-        # Largest blocks first: CTAs are scheduled roughly in index order.
-        sizes = np.asarray([low.blocks[it[0]][1] for it in items])
-        order = np.argsort(-sizes, kind="stable")
-        items = [items[k] for k in order]
         self.rows_per_item = rows
-        self.items = torch.as_tensor(np.asarray(items, dtype=np.int32), device=self.device).contiguous()
-        self.n_items = len(items)
+        nb = len(low.blocks)
+        limits = [self.smem_limit // 4, self.smem_limit // 2, self.smem_limit]
+        self.groups: Dict[str, list] = {}
+        for kind in ("forward", "backward"):
+            bwd = kind == "backward"
+            own = [self._block_maxima(np.asarray([b])) for b in range(nb)]
+            need = np.asarray([self._layout_bytes(mx, bwd) for mx in own])
+            # A class's layout is sized by the maxima over its blocks (nodes of one,
+            # slots of another...): admit blocks smallest first while it still fits.
+            cls = np.full(nb, -1, dtype=np.int64)  # -1: global scratch
+            run: List[Optional[Dict[str, int]]] = [None] * len(limits)
+            for b in np.argsort(need, kind="stable"):
+                for c, lim in enumerate(limits):
+                    if need[b] > lim:
+                        continue
+                    cand = own[b] if run[c] is None else {k: max(v, own[b][k]) for k, v in run[c].items()}
+                    if self._layout_bytes(cand, bwd) <= lim:
+                        cls[b] = c
+                        run[c] = cand
+                        break
+            groups = []
+            for c in [-1] + list(range(len(limits) - 1, -1, -1)):  # longest items first
+                sel = np.nonzero(cls == c)[0]
+                if len(sel) == 0:
+                    continue
+                items = [[int(b), r0, min(rows, B - r0), 0] for b in sel for r0 in range(0, B, rows)]
+                # Largest blocks first: CTAs are scheduled roughly in index order.
+                sizes = np.asarray([low.blocks[it[0]][1] for it in items])
+                items = [items[k] for k in np.argsort(-sizes, kind="stable")]
+                maxima = self._block_maxima(sel)
+                stride = (self._layout_bytes(maxima, bwd) + 255) // 256 * 256
+                groups.append({
+                    "gm": c < 0, "maxima": maxima, "n_items": len(items), "stride": stride,
+                    "items": torch.as_tensor(np.asarray(items, dtype=np.int32), device=self.device).contiguous(),
+                })
+            self.groups[kind] = groups
+        self.n_items = sum(g["n_items"] for g in self.groups["forward"])
 
     def args(self, state: torch.Tensor, n_steps: int, t0: int, rec_out: Optional[torch.Tensor],
              mode: int = 0, ckpt=None, ckpt_every: int = 0, ckpt_base: int = 0, traj=None,
              pscale: Optional[torch.Tensor] = None, syn_lin=None, syn_const=None,
-             adj=None, rec_grad=None, pgrad=None, items=None) -> _lib.JxbSimArgs:
+             adj=None, rec_grad=None, pgrad=None) -> _lib.JxbSimArgs:
+        """Arguments of a launch; the per-group fields (items, block maxima, global
+        scratch) are filled in by `launch_forward` / `launch_backward`."""
         low, t = self.low, self.t
         a = _lib.JxbSimArgs()
         a.dtype = self.code
@@ -113,18 +171,10 @@ class DeviceModel:
         a.n_slots = low.n_slots
         a.n_pslots = low.n_pslots
         a.n_cols = low.n_cols
-        a.n_items = self.n_items
         a.n_steps = n_steps
         a.t0 = t0
         a.max_rows = self.rows_per_item
-        a.max_nodes = self.max_nodes
-        a.max_slots = self.max_slots
-        a.max_chains = self.max_chains
-        a.max_child = self.max_child
-        a.max_levels = self.max_levels
-        a.max_pslots = self.max_pslots
         a.threads = self.threads
-        a.max_gslots = max(1, low.max_gslots)
         a.dt = low.dt
         for k in ["node_class", "soff", "poff", "a_low", "a_up", "gsum", "cm", "cls_ptr",
                   "cls_comp", "cls_prog", "entries", "pbase", "pcol", "blocks", "chain_top", "chain_len",
@@ -132,9 +182,6 @@ class DeviceModel:
                   "area", "rec_ptr", "rec_slot", "rec_col", "parent", "kid_ptr", "kid",
                   "gk", "gbase"]:
             setattr(a, k, t[k].data_ptr())
-        a.items = (items if items is not None else self.items).data_ptr()
-        if items is not None:
-            a.n_items = int(items.shape[0])
         a.n_classes = len(low.cls_comp)
         a.n_entries = int(low.entries.shape[0])
         a.pscale = (pscale if pscale is not None else self.pscale).data_ptr()
@@ -158,15 +205,50 @@ class DeviceModel:
         a.mode = mode
         return a
 
+    def scratch(self, kind: str, group) -> torch.Tensor:
+        """Global work areas of a group of oversized blocks (allocated once)."""
+        need = group["n_items"] * group["stride"] + 256
+        buf = self._scratch.get(kind)
+        if buf is None or buf.numel() < need:
+            buf = torch.empty(need, dtype=torch.uint8, device=self.device)
+            self._scratch[kind] = buf
+        return buf
+
+    def group_args(self, args: _lib.JxbSimArgs, kind: str, group) -> _lib.JxbSimArgs:
+        """A copy of `args` completed for one item group of a launch kind."""
+        a = _lib.JxbSimArgs.from_buffer_copy(args)
+        for k, v in group["maxima"].items():
+            setattr(a, k, v)
+        a.items = group["items"].data_ptr()
+        a.n_items = group["n_items"]
+        if group["gm"]:
+            buf = self.scratch(kind, group)
+            a.gscratch = (buf.data_ptr() + 255) // 256 * 256
+            a.gscratch_stride = group["stride"]
+        return a
+
     def _launch(self, kind: str, fn, args, stream) -> None:
         st = torch.cuda.current_stream(self.device)
-        s = stream if stream is not None else st.cuda_stream
+        main = stream if stream is not None else st.cuda_stream
+        groups = self.groups[kind]
         timed = self.timed_kind == kind and stream is None
         if timed:
             e0 = torch.cuda.Event(enable_timing=True)
             e0.record(st)
-        _lib.check(fn(C.byref(args), C.c_void_p(s)), f"jxb_sim_{kind}")
-        self.launches += 1
+        fork = len(groups) > 1 and stream is None
+        if fork:  # every group but the last on its own side stream, joined below
+            while len(self._sides) < len(groups) - 1:
+                self._sides.append(torch.cuda.Stream(self.device))
+            for side in self._sides[:len(groups) - 1]:
+                side.wait_stream(st)
+        for gi, g in enumerate(groups):
+            a = self.group_args(args, kind, g)
+            s = self._sides[gi].cuda_stream if (fork and gi < len(groups) - 1) else main
+            _lib.check(fn(C.byref(a), C.c_void_p(s)), f"jxb_sim_{kind}")
+            self.launches += 1
+        if fork:
+            for side in self._sides[:len(groups) - 1]:
+                st.wait_stream(side)
         if timed:
             e1 = torch.cuda.Event(enable_timing=True)
             e1.record(st)

@@ -6,7 +6,9 @@ re-entered from inside a step): its trajectory scratch is a fixed array inside t
 library. This test calls it through the C ABI and checks it against
 jxb_sim_backward on the same inputs, twice in a row (the array keeps the previous
 call's contents, which must not leak into the next result). Tolerance: identical
-results (the same kernel on the same data), float64 and float32.
+state adjoints (the same kernel on the same data); parameter gradients to 1e-12
+relative, because the float64 column sums are accumulated with atomics whose order
+varies between launches. Float64 and float32.
 """
 import ctypes as C
 
@@ -35,6 +37,8 @@ def _adjoint(sim, ckpt, rec_grad, T, noalloc):
         t0 = seg * K
         a = m.args(ckpt[seg], min(K, T - t0), t0, None, traj=traj, adj=adj,
                    rec_grad=rec_grad, pgrad=pgrad)
+        (group,) = m.groups["backward"]  # every block of the fixture fits shared memory
+        a = m.group_args(a, "backward", group)
         a.ckpt = ckpt[seg].data_ptr()
         a.traj_piv = piv.data_ptr() if piv is not None else None
         _lib.check(fn(C.byref(a), C.c_void_p(stream)), fn.__name__)
@@ -58,7 +62,7 @@ def test_noalloc_adjoint_matches_scratch_adjoint(cuda_device, dtype):
     for _ in range(2):
         adj, pg = _adjoint(sim, ckpt, rec_grad, T, noalloc=True)
         assert torch.equal(adj, ref_adj)
-        assert torch.equal(pg, ref_pg)
+        assert (pg - ref_pg).abs().max().item() <= 1e-12 * ref_pg.abs().max().item()
     assert ref_pg.abs().max() > 0
 
 
@@ -70,7 +74,8 @@ def test_noalloc_rejects_oversized_segments(cuda_device):
     state = m.initial_state()
     adj = torch.zeros_like(state)
     pgrad = torch.zeros((low.batch, low.n_cols), dtype=torch.float64, device=cuda_device)
-    a = m.args(state, 10**6, 0, None, adj=adj, pgrad=pgrad)
+    a = m.group_args(m.args(state, 10**6, 0, None, adj=adj, pgrad=pgrad), "backward",
+                     m.groups["backward"][0])
     a.ckpt = state.data_ptr()
     rc = _lib.load().jxb_sim_backward_noalloc(C.byref(a), C.c_void_p(torch.cuda.current_stream().cuda_stream))
     assert rc == 5  # JXB_ERR_TOO_LARGE
