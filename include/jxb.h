@@ -188,6 +188,14 @@ typedef struct {
    * Null: the work areas live in shared memory. */
   void* gscratch;
   int64_t gscratch_stride;
+  /* Optional node schedule of the per-node phases (channels, adjoint): for block b,
+   * sched[sched_ptr[b] .. sched_ptr[b+1]) holds sched_warps x k x 32 block-relative
+   * node indices (-1 = idle lane): warp w, iteration q, lane l processes
+   * sched[sched_ptr[b] + (w * k + q) * 32 + l]. Used when sched_warps equals the
+   * launch's warps per CTA; otherwise (or null) nodes are strided over the threads. */
+  const int32_t* sched_ptr;
+  const int16_t* sched;
+  int32_t sched_warps, pad5;
 } JxbSimArgs;
 
 int jxb_sim_forward(const JxbSimArgs* args, void* stream);

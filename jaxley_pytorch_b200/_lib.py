@@ -71,6 +71,7 @@ class JxbSimArgs(C.Structure):
         ("adj", _p), ("rec_grad", _p), ("pgrad", _p),
         ("mode", C.c_int32), ("pad2", C.c_int32),
         ("gscratch", _p), ("gscratch_stride", C.c_int64),
+        ("sched_ptr", _p), ("sched", _p), ("sched_warps", C.c_int32), ("pad5", C.c_int32),
     ]
 
 

@@ -38,6 +38,8 @@ void set_err(const char* what, cudaError_t e) {
 constexpr int kMaxWrites = 24;  // undo-log entries of one node's channel updates
 constexpr int FLAG_COMP = 1, FLAG_STIM = 2, FLAG_REC = 4;
 
+constexpr int kManyKids = 1 << 30;  // chain descriptor flag: more than two child chains
+
 template <typename T>
 struct SimSmem {
   // per block
@@ -45,6 +47,7 @@ struct SimSmem {
   int* soff;                 // n_nodes, relative to the block's first slot
   short *cls, *poff;         // n_nodes (poff relative to the block's first parameter slot)
   unsigned char* flags;      // n_nodes
+  int4* cdesc;               // n_chains: {top, bot | many-children flag, two child tops, parent top}
   short *ctop, *clen, *cptop;  // n_chains (node indices relative to the block)
   int* ccp;                  // n_chains + 1 (relative)
   short* cchild;             // n_child
@@ -97,6 +100,7 @@ __host__ __device__ inline size_t sim_smem_layout(const JxbSimArgs& a, bool back
   s.pc = (int*)take(sizeof(int) * np);
   s.gk = (int*)take(sizeof(int) * np);
   s.gbase = (int*)take(sizeof(int) * nn);
+  s.cdesc = (int4*)take(sizeof(int4) * nc);
   s.ccp = (int*)take(sizeof(int) * (nc + 1));
   s.lp = (int*)take(sizeof(int) * (nl + 1));
   s.ents = (ChanEntry*)take(sizeof(ChanEntry) * ne);
@@ -119,7 +123,7 @@ __host__ __device__ inline size_t sim_smem_layout(const JxbSimArgs& a, bool back
 // Stages the block's topology, the channel programs, the parameter values of the
 // item's rows and the rows' states (and adjoints) in shared memory.
 template <typename T>
-__device__ void stage_item(const JxbSimArgs& a, const JxbBlock& blk, int row0, int rows,
+__device__ __forceinline__ void stage_item(const JxbSimArgs& a, const JxbBlock& blk, int row0, int rows,
                            const SimSmem<T>& sm, T dt, const T* state_src, const T* adj_src) {
   const int tid = threadIdx.x, NT = blockDim.x;
   const int nn = blk.n_nodes, ns = blk.n_slots, node0 = blk.node0;
@@ -155,11 +159,20 @@ __device__ void stage_item(const JxbSimArgs& a, const JxbBlock& blk, int row0, i
   const int nc = blk.n_chains, c0 = blk.chain0;
   const int k0 = a.chain_cptr[c0];
   for (int c = tid; c < nc; c += NT) {
-    sm.ctop[c] = (short)(a.chain_top[c0 + c] - node0);
-    sm.clen[c] = (short)a.chain_len[c0 + c];
-    int pt = a.chain_ptop[c0 + c];
+    const int top = a.chain_top[c0 + c] - node0;
+    const int len = a.chain_len[c0 + c];
+    const int pt = a.chain_ptop[c0 + c];
+    const int kb = a.chain_cptr[c0 + c], ke = a.chain_cptr[c0 + c + 1];
+    sm.ctop[c] = (short)top;
+    sm.clen[c] = (short)len;
     sm.cptop[c] = (short)(pt >= 0 ? pt - node0 : -1);
-    sm.ccp[c] = a.chain_cptr[c0 + c] - k0;
+    sm.ccp[c] = kb - k0;
+    // One 16-byte record per chain: what a solve level reads before its arithmetic.
+    unsigned kids = 0xFFFFFFFFu;
+    if (ke - kb >= 1) kids = (kids & 0xFFFF0000u) | (unsigned)(a.chain_child[kb] - node0);
+    if (ke - kb >= 2) kids = (kids & 0x0000FFFFu) | ((unsigned)(a.chain_child[kb + 1] - node0) << 16);
+    sm.cdesc[c] = make_int4(top, (top + len - 1) | (ke - kb > 2 ? kManyKids : 0), (int)kids,
+                            pt >= 0 ? pt - node0 : -1);
   }
   if (tid == 0) sm.ccp[nc] = a.chain_cptr[c0 + nc] - k0;
   const int nk = a.chain_cptr[c0 + nc] - k0;
@@ -201,7 +214,7 @@ __device__ void stage_item(const JxbSimArgs& a, const JxbBlock& blk, int row0, i
 
 // Voltages of the staged states (after a barrier that follows `stage_item`).
 template <typename T>
-__device__ void init_voltages(const JxbBlock& blk, const SimSmem<T>& sm, int rows) {
+__device__ __forceinline__ void init_voltages(const JxbBlock& blk, const SimSmem<T>& sm, int rows) {
   const int nn = blk.n_nodes, ns = blk.n_slots;
   for (int w = threadIdx.x; w < nn * rows; w += blockDim.x) {
     const int r = w / nn, j = w - r * nn;
@@ -209,12 +222,123 @@ __device__ void init_voltages(const JxbBlock& blk, const SimSmem<T>& sm, int row
   }
 }
 
-// Chain elimination (leaves first) and back-substitution of every tree of the block
-// for all rows. `al`/`au` are A[i, parent] / A[parent, i]; the adjoint passes them
-// swapped to solve with the transposed matrix. On return `S` holds the solution.
+// Chain recurrences with the coefficients of up to kSeg consecutive nodes loaded
+// into registers before the dependent arithmetic (a chain is processed in segments
+// of kSeg nodes): the recurrence then waits on arithmetic only, not on a shared
+// memory load after every step. The operations and their order are those of the
+// node-by-node form.
+constexpr int kSeg = 4;
+
+// Elimination of chain c, bottom to top, after its child chains: D receives the
+// reciprocal of every pivot, S the eliminated right-hand side.
 template <typename T>
-__device__ void block_solve(const JxbBlock& blk, const SimSmem<T>& sm, int rows, const T* al,
-                            const T* au, T* V = nullptr) {
+__device__ __forceinline__ void chain_eliminate(const SimSmem<T>& sm, int c, T* __restrict__ Dr,
+                                                T* __restrict__ Sr, const T* __restrict__ al,
+                                                const T* __restrict__ au) {
+  const int4 dsc = sm.cdesc[c];
+  const int top = dsc.x;
+  const int bot = dsc.y & ~kManyKids;
+  T d = Dr[bot], s = Sr[bot];
+  if (!(dsc.y & kManyKids)) {
+    // up to two child chains: their values are loaded together
+    const int k0 = dsc.z & 0xFFFF, k1 = (unsigned)dsc.z >> 16;
+    T u0 = T(0), q0 = T(0), l0 = T(0), s0 = T(0), u1 = T(0), q1 = T(0), l1 = T(0), s1 = T(0);
+    if (k0 != 0xFFFF) { u0 = au[k0]; q0 = Dr[k0]; l0 = al[k0]; s0 = Sr[k0]; }
+    if (k1 != 0xFFFF) { u1 = au[k1]; q1 = Dr[k1]; l1 = al[k1]; s1 = Sr[k1]; }
+    if (k0 != 0xFFFF) {
+      const T f = u0 * q0;
+      d -= l0 * f;
+      s -= s0 * f;
+    }
+    if (k1 != 0xFFFF) {
+      const T f = u1 * q1;
+      d -= l1 * f;
+      s -= s1 * f;
+    }
+  } else {
+    for (int k = sm.ccp[c]; k < sm.ccp[c + 1]; ++k) {
+      const int ct = sm.cchild[k];
+      const T f = au[ct] * Dr[ct];
+      d -= al[ct] * f;
+      s -= Sr[ct] * f;
+    }
+  }
+  T id = rcp(d);
+  Dr[bot] = id;
+  Sr[bot] = s;
+  for (int hi = bot - 1; hi >= top; hi -= kSeg) {
+    const int n = min(kSeg, hi - top + 1);
+    T dd[kSeg], ss[kSeg], lo[kSeg], up[kSeg];
+#pragma unroll
+    for (int q = 0; q < kSeg; ++q)
+      if (q < n) {
+        dd[q] = Dr[hi - q];
+        ss[q] = Sr[hi - q];
+        lo[q] = al[hi - q + 1];
+        up[q] = au[hi - q + 1];
+      }
+#pragma unroll
+    for (int q = 0; q < kSeg; ++q)
+      if (q < n) {
+        const T f = up[q] * id;
+        d = dd[q] - lo[q] * f;
+        s = ss[q] - s * f;
+        id = rcp(d);
+        dd[q] = id;
+        ss[q] = s;
+      }
+#pragma unroll
+    for (int q = 0; q < kSeg; ++q)
+      if (q < n) {
+        Dr[hi - q] = dd[q];
+        Sr[hi - q] = ss[q];
+      }
+  }
+}
+
+// Back-substitution of chain c, top to bottom, from its parent's solution; adds the
+// solution to `Vr` when given.
+template <typename T>
+__device__ __forceinline__ void chain_backsub(const SimSmem<T>& sm, int c, const T* __restrict__ Dr,
+                                              T* __restrict__ Sr, const T* __restrict__ al,
+                                              T* __restrict__ Vr) {
+  const int4 dsc = sm.cdesc[c];
+  const int top = dsc.x;
+  const int bot = dsc.y & ~kManyKids;
+  const int pt = dsc.w;
+  T xp = pt >= 0 ? Sr[pt] : T(0);
+  for (int l0 = top; l0 <= bot; l0 += kSeg) {
+    const int n = min(kSeg, bot - l0 + 1);
+    T dd[kSeg], ss[kSeg], ll[kSeg];
+#pragma unroll
+    for (int q = 0; q < kSeg; ++q)
+      if (q < n) {
+        dd[q] = Dr[l0 + q];
+        ss[q] = Sr[l0 + q];
+        ll[q] = al[l0 + q];
+      }
+#pragma unroll
+    for (int q = 0; q < kSeg; ++q)
+      if (q < n) {
+        const T x = (ss[q] - ll[q] * xp) * dd[q];
+        ss[q] = x;
+        xp = x;
+      }
+#pragma unroll
+    for (int q = 0; q < kSeg; ++q)
+      if (q < n) {
+        Sr[l0 + q] = ss[q];
+        if (Vr) Vr[l0 + q] += ss[q];
+      }
+  }
+}
+
+// Chain elimination (leaves first) and back-substitution of every tree of the block
+// for all rows. `al`/`au` are A[i, parent] / A[parent, i]. On return `S` holds the
+// solution (and `V`, when given, has it added).
+template <typename T>
+__device__ __forceinline__ void block_solve(const JxbBlock& blk, const SimSmem<T>& sm, int rows,
+                                            const T* al, const T* au, T* V = nullptr) {
   const int tid = threadIdx.x, NT = blockDim.x;
   const int nn = blk.n_nodes;
   const int nlev = blk.n_levels;
@@ -222,31 +346,8 @@ __device__ void block_solve(const JxbBlock& blk, const SimSmem<T>& sm, int rows,
   for (int h = 0; h < nlev; ++h) {
     const int c0 = sm.lp[h], nch = sm.lp[h + 1] - c0;
     for (int w = tid; w < nch * rows; w += NT) {
-      const int c = c0 + w % nch;
-      const int r = w / nch;
-      T* Dr = sm.D + (size_t)r * nn;
-      T* Sr = sm.S + (size_t)r * nn;
-      const int top = sm.ctop[c];
-      const int bot = top + sm.clen[c] - 1;
-      // D receives the reciprocal of every eliminated pivot.
-      T d = Dr[bot], s = Sr[bot];
-      for (int k = sm.ccp[c]; k < sm.ccp[c + 1]; ++k) {
-        const int ct = sm.cchild[k];
-        const T f = au[ct] * Dr[ct];
-        d -= al[ct] * f;
-        s -= Sr[ct] * f;
-      }
-      T id = rcp(d);
-      Dr[bot] = id;
-      Sr[bot] = s;
-      for (int j = bot - 1; j >= top; --j) {
-        const T f = au[j + 1] * id;
-        d = Dr[j] - al[j + 1] * f;
-        s = Sr[j] - s * f;
-        id = rcp(d);
-        Dr[j] = id;
-        Sr[j] = s;
-      }
+      const int r = rows == 1 ? 0 : w / nch;  // no division for one row
+      chain_eliminate<T>(sm, c0 + (w - r * nch), sm.D + (size_t)r * nn, sm.S + (size_t)r * nn, al, au);
     }
     __syncthreads();
   }
@@ -254,21 +355,9 @@ __device__ void block_solve(const JxbBlock& blk, const SimSmem<T>& sm, int rows,
   for (int h = nlev - 1; h >= 0; --h) {
     const int c0 = sm.lp[h], nch = sm.lp[h + 1] - c0;
     for (int w = tid; w < nch * rows; w += NT) {
-      const int c = c0 + w % nch;
-      const int r = w / nch;
-      const T* Dr = sm.D + (size_t)r * nn;
-      T* Sr = sm.S + (size_t)r * nn;
-      const int top = sm.ctop[c];
-      const int bot = top + sm.clen[c] - 1;
-      const int pt = sm.cptop[c];
-      T xp = pt >= 0 ? Sr[pt] : T(0);
-      T* Vr = V ? V + (size_t)r * nn : nullptr;
-      for (int j = top; j <= bot; ++j) {
-        const T x = (Sr[j] - al[j] * xp) * Dr[j];
-        Sr[j] = x;
-        xp = x;
-        if (Vr) Vr[j] += x;
-      }
+      const int r = rows == 1 ? 0 : w / nch;
+      chain_backsub<T>(sm, c0 + (w - r * nch), sm.D + (size_t)r * nn, sm.S + (size_t)r * nn, al,
+                       V ? V + (size_t)r * nn : nullptr);
     }
     __syncthreads();
   }
@@ -341,21 +430,62 @@ __device__ __forceinline__ void record_node(const JxbSimArgs& a, int i, const T*
 }
 
 
+// The (row, node) pairs one thread visits in a per-node phase. With a node schedule
+// for this launch's warp count, warp w visits its listed nodes (each chunk of 32
+// lanes holds nodes of one class; the chunks are balanced over the warps by cost),
+// every row of a node in turn; otherwise the pairs are strided over the threads.
+struct NodeWalk {
+  const short* sc;  // schedule of this thread (stride 32), or null
+  int n;            // visits
+  int rows, nn, w0, stride;
+
+  __device__ __forceinline__ NodeWalk(const JxbSimArgs& a, const JxbBlock& blk, int rows_, int item_block) {
+    const int tid = threadIdx.x, NT = blockDim.x;
+    rows = rows_;
+    nn = blk.n_nodes;
+    if (a.sched && a.sched_warps * 32 == NT) {
+      const int s0 = a.sched_ptr[item_block], s1 = a.sched_ptr[item_block + 1];
+      const int per_warp = (s1 - s0) / a.sched_warps;  // iterations x 32
+      sc = a.sched + s0 + (tid >> 5) * per_warp + (tid & 31);
+      n = per_warp / 32 * rows;
+      w0 = stride = 0;
+    } else {
+      sc = nullptr;
+      w0 = tid;
+      stride = NT;
+      n = tid < nn * rows ? (nn * rows - tid + NT - 1) / NT : 0;
+    }
+  }
+  // (r, j) of visit q; false for an idle lane.
+  __device__ __forceinline__ bool get(int q, int& r, int& j) const {
+    if (sc) {
+      const int k = rows == 1 ? q : q / rows;
+      r = q - k * rows;
+      j = __ldg(sc + k * 32);
+      return j >= 0;
+    }
+    const int w = w0 + q * stride;
+    r = rows == 1 ? 0 : w / nn;
+    j = w - r * nn;
+    return true;
+  }
+};
+
 // Runs `n_steps` forward steps of one item from the staged state. Used by the
 // forward kernel (ckpt/rec outputs) and by the adjoint (trajectory store).
 // On return sm.st holds the state after the last step; `X1` (if not null) receives
 // the final voltages.
 template <typename T>
-__device__ void run_steps(const JxbSimArgs& a, const JxbBlock& blk, int row0, int rows,
-                          const SimSmem<T>& sm, T dt, int t0, int nsteps, int mode, bool record,
-                          bool ckpt, T* traj, T* X1, T* piv = nullptr) {
-  const int tid = threadIdx.x, NT = blockDim.x;
+__device__ __forceinline__ void run_steps(const JxbSimArgs& a, const JxbBlock& blk, int item_block, int row0,
+                                          int rows, const SimSmem<T>& sm, T dt, int t0, int nsteps, int mode,
+                                          bool record, bool ckpt, T* traj, T* X1, T* piv = nullptr) {
   const int nn = blk.n_nodes, ns = blk.n_slots, np = blk.n_pslots;
-  const int total = nn * rows;
   for (int step = 0; step <= nsteps; ++step) {
     const int t = t0 + step;
-    for (int w = tid; w < total; w += NT) {
-      const int r = w / nn, j = w - r * nn;
+    const NodeWalk walk(a, blk, rows, item_block);
+    for (int q = 0; q < walk.n; ++q) {
+      int r, j;
+      if (!walk.get(q, r, j)) continue;
       const int i = blk.node0 + j;
       const int b = row0 + r;
       T* x = sm.st + (size_t)r * ns + sm.soff[j];
@@ -423,8 +553,9 @@ __device__ __forceinline__ char* work_base(const JxbSimArgs& a, char* smem_raw) 
   return smem_raw;
 }
 
+// float: at most 64 registers, so that two 512-thread CTAs (four of 256) fit an SM.
 template <typename T, int NT, bool GM>
-__global__ void __launch_bounds__(NT) sim_forward_kernel(JxbSimArgs a) {
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 1024 / NT : 1) sim_forward_kernel(JxbSimArgs a) {
   extern __shared__ __align__(16) char smem_raw[];
   SimSmem<T> sm;
   sim_smem_layout<T>(a, false, &sm, work_base<GM>(a, smem_raw));
@@ -437,7 +568,7 @@ __global__ void __launch_bounds__(NT) sim_forward_kernel(JxbSimArgs a) {
   init_voltages<T>(blk, sm, rows);
   __syncthreads();
   const int nsteps = a.mode == 0 ? a.n_steps : 0;
-  run_steps<T>(a, blk, row0, rows, sm, dt, a.t0, nsteps, a.mode, a.n_rec > 0, a.ckpt != nullptr,
+  run_steps<T>(a, blk, item.block, row0, rows, sm, dt, a.t0, nsteps, a.mode, a.n_rec > 0, a.ckpt != nullptr,
                (T*)a.traj, nullptr);
   // Write the resident states back.
   const int ns = blk.n_slots;
@@ -497,52 +628,74 @@ __device__ __forceinline__ void node_adjoint(const SimSmem<T>& sm, int j, T* x, 
   }
 }
 
-// Transposed solve with the reciprocal pivots of the forward elimination (the
-// pivots of A and A^T coincide): only the right-hand side is eliminated.
+// Elimination of chain c for the transposed system with the stored reciprocal
+// pivots: only the right-hand side is eliminated.
 template <typename T>
-__device__ void block_solve_pivots(const JxbBlock& blk, const SimSmem<T>& sm, int rows,
-                                   const T* al, const T* au) {
+__device__ __forceinline__ void chain_eliminate_rhs(const SimSmem<T>& sm, int c, const T* __restrict__ Dr,
+                                                    T* __restrict__ Sr, const T* __restrict__ au) {
+  const int4 dsc = sm.cdesc[c];
+  const int top = dsc.x;
+  const int bot = dsc.y & ~kManyKids;
+  T s = Sr[bot];
+  if (!(dsc.y & kManyKids)) {
+    const int k0 = dsc.z & 0xFFFF, k1 = (unsigned)dsc.z >> 16;
+    T s0 = T(0), u0 = T(0), q0 = T(0), s1 = T(0), u1 = T(0), q1 = T(0);
+    if (k0 != 0xFFFF) { s0 = Sr[k0]; u0 = au[k0]; q0 = Dr[k0]; }
+    if (k1 != 0xFFFF) { s1 = Sr[k1]; u1 = au[k1]; q1 = Dr[k1]; }
+    if (k0 != 0xFFFF) s -= s0 * (u0 * q0);
+    if (k1 != 0xFFFF) s -= s1 * (u1 * q1);
+  } else {
+    for (int k = sm.ccp[c]; k < sm.ccp[c + 1]; ++k) {
+      const int ct = sm.cchild[k];
+      s -= Sr[ct] * (au[ct] * Dr[ct]);
+    }
+  }
+  Sr[bot] = s;
+  for (int hi = bot - 1; hi >= top; hi -= kSeg) {
+    const int n = min(kSeg, hi - top + 1);
+    T ss[kSeg], up[kSeg], dn[kSeg];
+#pragma unroll
+    for (int q = 0; q < kSeg; ++q)
+      if (q < n) {
+        ss[q] = Sr[hi - q];
+        up[q] = au[hi - q + 1];
+        dn[q] = Dr[hi - q + 1];
+      }
+#pragma unroll
+    for (int q = 0; q < kSeg; ++q)
+      if (q < n) {
+        s = ss[q] - s * (up[q] * dn[q]);
+        ss[q] = s;
+      }
+#pragma unroll
+    for (int q = 0; q < kSeg; ++q)
+      if (q < n) Sr[hi - q] = ss[q];
+  }
+}
+
+// Transposed solve with the reciprocal pivots of the forward elimination (the
+// pivots of A and A^T coincide): only the right-hand side is eliminated. Levels as in
+// `block_solve`.
+template <typename T>
+__device__ __forceinline__ void block_solve_pivots(const JxbBlock& blk, const SimSmem<T>& sm, int rows,
+                                                   const T* al, const T* au) {
   const int tid = threadIdx.x, NT = blockDim.x;
   const int nn = blk.n_nodes;
   const int nlev = blk.n_levels;
   for (int h = 0; h < nlev; ++h) {
     const int c0 = sm.lp[h], nch = sm.lp[h + 1] - c0;
     for (int w = tid; w < nch * rows; w += NT) {
-      const int c = c0 + w % nch;
-      const int r = w / nch;
-      const T* Dr = sm.D + (size_t)r * nn;
-      T* Sr = sm.S + (size_t)r * nn;
-      const int top = sm.ctop[c];
-      const int bot = top + sm.clen[c] - 1;
-      T s = Sr[bot];
-      for (int k = sm.ccp[c]; k < sm.ccp[c + 1]; ++k) {
-        const int ct = sm.cchild[k];
-        s -= Sr[ct] * (au[ct] * Dr[ct]);
-      }
-      Sr[bot] = s;
-      for (int j = bot - 1; j >= top; --j) {
-        s = Sr[j] - s * (au[j + 1] * Dr[j + 1]);
-        Sr[j] = s;
-      }
+      const int r = rows == 1 ? 0 : w / nch;  // no division for one row
+      chain_eliminate_rhs<T>(sm, c0 + (w - r * nch), sm.D + (size_t)r * nn, sm.S + (size_t)r * nn, au);
     }
     __syncthreads();
   }
   for (int h = nlev - 1; h >= 0; --h) {
     const int c0 = sm.lp[h], nch = sm.lp[h + 1] - c0;
     for (int w = tid; w < nch * rows; w += NT) {
-      const int c = c0 + w % nch;
-      const int r = w / nch;
-      const T* Dr = sm.D + (size_t)r * nn;
-      T* Sr = sm.S + (size_t)r * nn;
-      const int top = sm.ctop[c];
-      const int bot = top + sm.clen[c] - 1;
-      const int pt = sm.cptop[c];
-      T xp = pt >= 0 ? Sr[pt] : T(0);
-      for (int j = top; j <= bot; ++j) {
-        const T x = (Sr[j] - al[j] * xp) * Dr[j];
-        Sr[j] = x;
-        xp = x;
-      }
+      const int r = rows == 1 ? 0 : w / nch;
+      chain_backsub<T>(sm, c0 + (w - r * nch), sm.D + (size_t)r * nn, sm.S + (size_t)r * nn, al,
+                       (T*)nullptr);
     }
     __syncthreads();
   }
@@ -567,7 +720,7 @@ __global__ void __launch_bounds__(NT) sim_backward_kernel(JxbSimArgs a) {
   init_voltages<T>(blk, sm, rows);
   __syncthreads();
   T* piv = (T*)a.traj_piv;
-  run_steps<T>(a, blk, row0, rows, sm, dt, a.t0, K, 0, false, false, traj, sm.X1, piv);
+  run_steps<T>(a, blk, item.block, row0, rows, sm, dt, a.t0, K, 0, false, false, traj, sm.X1, piv);
 
   const T* rec_grad = (const T*)a.rec_grad;
   const int total = nn * rows;
@@ -595,8 +748,10 @@ __global__ void __launch_bounds__(NT) sim_backward_kernel(JxbSimArgs a) {
     // the forward elimination.
     block_solve_pivots<T>(blk, sm, rows, sm.au, sm.al);
     // Phase 4: vector-Jacobian products of the step.
-    for (int w = tid; w < total; w += nthr) {
-      const int r = w / nn, j = w - r * nn;
+    const NodeWalk walk(a, blk, rows, item.block);
+    for (int q = 0; q < walk.n; ++q) {
+      int r, j;
+      if (!walk.get(q, r, j)) continue;
       const int b = row0 + r;
       T* x = sm.st + (size_t)r * ns + sm.soff[j];
       T* lam = sm.adj + (size_t)r * ns + sm.soff[j];

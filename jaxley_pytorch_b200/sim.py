@@ -32,12 +32,64 @@ def _ptr(t: Optional[torch.Tensor]) -> Optional[int]:
     return None if t is None else t.data_ptr()
 
 
+def class_costs(low: Lowered) -> np.ndarray:
+    """Relative cost of one node of every class in the per-node phases: a channel
+    costs its overhead plus its gates, the interpreter (classes without a
+    compile-time program) about 1.7 times a program, a branchpoint (no channels)
+    only its assembly."""
+    out = np.zeros(len(low.cls_comp))
+    for c in range(len(out)):
+        if not low.cls_comp[c]:
+            out[c] = 0.15
+            continue
+        ents = low.entries[low.cls_ptr[c]:low.cls_ptr[c + 1]]
+        cost = 0.3 + sum(0.5 + 1.5 * int(e[1]) for e in ents)
+        out[c] = cost * (1.0 if low.cls_prog[c] else 1.7)
+    return out
+
+
+def node_schedule(low: Lowered, n_warps: int):
+    """Per block, the nodes every warp visits in the per-node phases: the block's nodes
+    are cut into chunks of up to 32 nodes of one class (in node order), and the
+    chunks go, most expensive first, to the warp with the least work so far. Returns
+    `(sched_ptr (n_blocks + 1,) int32, sched int16)` in the layout of
+    `JxbSimArgs.sched`."""
+    import heapq
+
+    cost = class_costs(low)
+    parts, ptr = [], [0]
+    for b in low.blocks:
+        n0, nn = int(b[0]), int(b[1])
+        cls = low.node_class[n0:n0 + nn]
+        chunks = []  # (cost, node indices)
+        for c in np.unique(cls):
+            nodes = np.nonzero(cls == c)[0]
+            for k in range(0, len(nodes), 32):
+                chunks.append((float(cost[c]), nodes[k:k + 32]))
+        order = sorted(range(len(chunks)), key=lambda q: -chunks[q][0])
+        heap = [(0.0, w) for w in range(n_warps)]
+        lists: List[List[int]] = [[] for _ in range(n_warps)]
+        for q in order:
+            load, w = heapq.heappop(heap)
+            lists[w].append(q)
+            heapq.heappush(heap, (load + chunks[q][0], w))
+        kmax = max(1, max(len(x) for x in lists))
+        arr = np.full((n_warps, kmax, 32), -1, dtype=np.int16)
+        for w in range(n_warps):
+            for k, q in enumerate(lists[w]):
+                nodes = chunks[q][1]
+                arr[w, k, :len(nodes)] = nodes
+        parts.append(arr.reshape(-1))
+        ptr.append(ptr[-1] + arr.size)
+    return np.asarray(ptr, dtype=np.int32), np.concatenate(parts)
+
+
 class DeviceModel:
     """A lowered model resident on one GPU."""
 
     def __init__(self, low: Lowered, dtype: torch.dtype = torch.float32, device="cuda",
                  rows_per_item: int = 1, threads: int = 256, programs: bool = True,
-                 smem_limit: Optional[int] = None):
+                 smem_limit: Optional[int] = None, schedule: bool = True):
         self.low = low
         self.dtype = dtype
         self.device = torch.device(device)
@@ -79,6 +131,12 @@ class DeviceModel:
         self._sides: List[torch.cuda.Stream] = []
         self._scratch: Dict[str, torch.Tensor] = {}
         self.smem_limit = smem_limit if smem_limit is not None else self._device_smem_limit()
+        self.sched_warps = 0
+        if schedule and threads % 32 == 0:
+            sp, sc = node_schedule(low, threads // 32)
+            self.t["sched_ptr"] = i(sp)
+            self.t["sched"] = torch.as_tensor(sc, device=dev).contiguous()
+            self.sched_warps = threads // 32
         self.set_rows_per_item(rows_per_item)
 
     def _device_smem_limit(self) -> int:
@@ -203,6 +261,10 @@ class DeviceModel:
         a.rec_grad = _ptr(rec_grad)
         a.pgrad = _ptr(pgrad)
         a.mode = mode
+        if self.sched_warps:
+            a.sched_ptr = t["sched_ptr"].data_ptr()
+            a.sched = t["sched"].data_ptr()
+            a.sched_warps = self.sched_warps
         return a
 
     def scratch(self, kind: str, group) -> torch.Tensor:
@@ -281,12 +343,12 @@ class Simulation:
                  max_block_nodes: int = 4096, rows_per_item: int = 1,
                  segment: Optional[int] = None, init_steady: bool = False,
                  low: Optional[Lowered] = None, checkpoint: int = 100, threads: int = 256,
-                 keep_currents: bool = True, programs: bool = True):
+                 keep_currents: bool = True, programs: bool = True, schedule: bool = True):
         self.problem = problem
         self.low = low if low is not None else lower(problem, max_block_nodes=max_block_nodes,
                                                      keep_currents=keep_currents)
         self.model = DeviceModel(self.low, dtype, device, rows_per_item, threads=threads,
-                                 programs=programs)
+                                 programs=programs, schedule=schedule)
         self.segment = segment
         self.init_steady = init_steady
         self.checkpoint = int(checkpoint)

@@ -46,3 +46,20 @@ def test_global_scratch_matches_shared_memory(cuda_device, dtype, mode):
     scale = g0.abs().max().item()
     assert scale > 0
     assert (g0 - g1).abs().max().item() <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+@pytest.mark.parametrize("threads", [64, 256])
+def test_node_schedule_does_not_change_results(cuda_device, dtype, threads):
+    """The per-warp node schedule only reorders which thread handles which node."""
+    prob = synth.config_uneven(n_cells=16, n_steps=60, max_comp=400, seed=9)
+    low = lower(prob, max_block_nodes=512, keep_currents=False)
+    kw = dict(low=low, dtype=dtype, device=cuda_device, checkpoint=25, threads=threads)
+    a = Simulation(prob, schedule=False, **kw)
+    b = Simulation(prob, schedule=True, **kw)
+    assert b.model.sched_warps == threads // 32 and a.model.sched_warps == 0
+    r0, g0 = _grad_run(a, 60)
+    r1, g1 = _grad_run(b, 60)
+    torch.cuda.synchronize()
+    assert torch.equal(r0, r1)
+    assert (g0 - g1).abs().max().item() <= 1e-12 * g0.abs().max().item()

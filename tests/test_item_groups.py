@@ -70,3 +70,29 @@ def test_layout_grows_with_the_block():
     both = m._layout_bytes(m._block_maxima(np.arange(len(low.blocks))), True)
     assert both >= max(sizes)
     assert _lib.JxbSimArgs.gscratch.offset > _lib.JxbSimArgs.mode.offset
+
+
+@pytest.mark.parametrize("warps", [1, 4, 16])
+def test_node_schedule_covers_every_node_once(warps):
+    from jaxley_pytorch_b200.sim import class_costs, node_schedule
+
+    low, _ = _model(1 << 30)
+    ptr, sched = node_schedule(low, warps)
+    cost = class_costs(low)
+    assert len(ptr) == len(low.blocks) + 1 and ptr[-1] == len(sched)
+    for b, blk in enumerate(low.blocks):
+        part = sched[ptr[b]:ptr[b + 1]].reshape(warps, -1, 32)
+        nodes = part[part >= 0]
+        assert sorted(nodes.tolist()) == list(range(blk[1]))
+        cls = low.node_class[blk[0]:blk[0] + blk[1]]
+        loads = []
+        for w in range(warps):
+            load = 0.0
+            for k in range(part.shape[1]):
+                chunk = part[w, k][part[w, k] >= 0]
+                if len(chunk):
+                    assert len(set(cls[chunk].tolist())) == 1  # one class per chunk
+                    load += cost[cls[chunk[0]]]
+            loads.append(load)
+        # greedy balance: no warp exceeds the mean by more than the dearest chunk
+        assert max(loads) <= np.mean(loads) + cost.max() + 1e-9
