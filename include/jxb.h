@@ -196,6 +196,12 @@ typedef struct {
   const int32_t* sched_ptr;
   const int16_t* sched;
   int32_t sched_warps, pad5;
+  /* Optional (adjoint): the per-node gradient slots of item i in global memory at
+   * [gacc + i * gacc_stride, + max_rows * max_gslots * sizeof(dtype)) instead of
+   * shared memory (frees shared memory for more CTAs per SM). 256-byte aligned,
+   * stride a multiple of 256. Null: the slots live in shared memory. */
+  void* gacc;
+  int64_t gacc_stride;
 } JxbSimArgs;
 
 int jxb_sim_forward(const JxbSimArgs* args, void* stream);

@@ -72,6 +72,7 @@ class JxbSimArgs(C.Structure):
         ("mode", C.c_int32), ("pad2", C.c_int32),
         ("gscratch", _p), ("gscratch_stride", C.c_int64),
         ("sched_ptr", _p), ("sched", _p), ("sched_warps", C.c_int32), ("pad5", C.c_int32),
+        ("gacc", _p), ("gacc_stride", C.c_int64),
     ]
 
 

@@ -48,7 +48,6 @@ struct SimSmem {
   short *cls, *poff;         // n_nodes (poff relative to the block's first parameter slot)
   unsigned char* flags;      // n_nodes
   int4* cdesc;               // n_chains: {top, bot | many-children flag, two child tops, parent top}
-  short *ctop, *clen, *cptop;  // n_chains (node indices relative to the block)
   int* ccp;                  // n_chains + 1 (relative)
   short* cchild;             // n_child
   int* lp;                   // n_levels + 1
@@ -59,7 +58,7 @@ struct SimSmem {
   T* pb;                     // n_pslots (parameter bases)
   int* pc;                   // n_pslots (parameter columns)
   int* gk;                   // n_pslots (gradient rank or -1)
-  int* gbase;                // n_nodes (first gradient slot)
+  const int* gbase;          // n_nodes (first gradient slot), global
   T* gacc;                   // rows * max_gslots (adjoint only)
   // per row
   T *st, *D, *S, *pv;        // rows * (n_slots | n_nodes | n_nodes | n_pslots)
@@ -88,18 +87,19 @@ __host__ __device__ inline size_t sim_smem_layout(const JxbSimArgs& a, bool back
   s.D = (T*)take(sizeof(T) * R * nn);
   s.S = (T*)take(sizeof(T) * R * nn);
   s.V = (T*)take(sizeof(T) * R * nn);
-  s.X1 = backward ? (T*)take(sizeof(T) * R * nn) : nullptr;
+  s.X1 = backward ? s.V : nullptr;  // the reverse sweep does not use V
   s.pv = (T*)take(sizeof(T) * R * np);
-  s.gacc = backward ? (T*)take(sizeof(T) * R * (size_t)a.max_gslots) : nullptr;
+  s.gacc = (backward && !a.gacc) ? (T*)take(sizeof(T) * R * (size_t)a.max_gslots) : nullptr;
   s.al = (T*)take(sizeof(T) * nn);
   s.au = (T*)take(sizeof(T) * nn);
-  s.dg = (T*)take(sizeof(T) * nn);
-  s.cm = (T*)take(sizeof(T) * nn);
+  // The adjoint reads cm from global memory and forms the diagonal constant on the
+  // fly (shared memory goes to more CTAs per SM instead).
+  s.dg = backward ? nullptr : (T*)take(sizeof(T) * nn);
+  s.cm = backward ? nullptr : (T*)take(sizeof(T) * nn);
   s.pb = (T*)take(sizeof(T) * np);
   s.soff = (int*)take(sizeof(int) * nn);
   s.pc = (int*)take(sizeof(int) * np);
   s.gk = (int*)take(sizeof(int) * np);
-  s.gbase = (int*)take(sizeof(int) * nn);
   s.cdesc = (int4*)take(sizeof(int4) * nc);
   s.ccp = (int*)take(sizeof(int) * (nc + 1));
   s.lp = (int*)take(sizeof(int) * (nl + 1));
@@ -108,9 +108,6 @@ __host__ __device__ inline size_t sim_smem_layout(const JxbSimArgs& a, bool back
   s.cprog = (int*)take(sizeof(int) * a.n_classes);
   s.cls = (short*)take(sizeof(short) * nn);
   s.poff = (short*)take(sizeof(short) * nn);
-  s.ctop = (short*)take(sizeof(short) * nc);
-  s.clen = (short*)take(sizeof(short) * nc);
-  s.cptop = (short*)take(sizeof(short) * nc);
   s.cchild = (short*)take(sizeof(short) * (nk + 1));
   s.par = (short*)take(sizeof(short) * nn);
   s.kptr = (short*)take(sizeof(short) * (nn + 1));
@@ -137,12 +134,11 @@ __device__ __forceinline__ void stage_item(const JxbSimArgs& a, const JxbBlock& 
     const bool comp = a.cls_comp[cls] != 0;
     sm.al[j] = -(dt * gl[i]);
     sm.au[j] = -(dt * gu[i]);
-    sm.dg[j] = (comp ? T(1) : T(0)) + dt * gs[i];
-    sm.cm[j] = cmv[i];
+    if (sm.dg) sm.dg[j] = (comp ? T(1) : T(0)) + dt * gs[i];
+    if (sm.cm) sm.cm[j] = cmv[i];
     sm.soff[j] = a.soff[i] - blk.slot0;
     sm.cls[j] = (short)cls;
     sm.poff[j] = (short)(a.poff[i] - blk.pslot0);
-    sm.gbase[j] = a.gbase[i];
     unsigned char f = comp ? FLAG_COMP : 0;
     if (a.stim_ptr[i + 1] > a.stim_ptr[i]) f |= FLAG_STIM;
     if (a.n_rec > 0 && a.rec_ptr[i + 1] > a.rec_ptr[i]) f |= FLAG_REC;
@@ -163,9 +159,6 @@ __device__ __forceinline__ void stage_item(const JxbSimArgs& a, const JxbBlock& 
     const int len = a.chain_len[c0 + c];
     const int pt = a.chain_ptop[c0 + c];
     const int kb = a.chain_cptr[c0 + c], ke = a.chain_cptr[c0 + c + 1];
-    sm.ctop[c] = (short)top;
-    sm.clen[c] = (short)len;
-    sm.cptop[c] = (short)(pt >= 0 ? pt - node0 : -1);
     sm.ccp[c] = kb - k0;
     // One 16-byte record per chain: what a solve level reads before its arithmetic.
     unsigned kids = 0xFFFFFFFFu;
@@ -535,7 +528,8 @@ __device__ __forceinline__ void run_steps(const JxbSimArgs& a, const JxbBlock& b
         const int c = sm.kids[k];
         axv += sm.au[c] * (Vr[c] - v);
       }
-      sm.D[(size_t)r * nn + j] = sm.dg[j] + lin_t;
+      const T dgj = sm.dg ? sm.dg[j] : ((f & FLAG_COMP) ? T(1) : T(0)) + dt * ((const T*)a.gsum)[i];
+      sm.D[(size_t)r * nn + j] = dgj + lin_t;
       sm.S[(size_t)r * nn + j] = ((f & FLAG_COMP) ? dt * (cst / cmv) - lin_t * v : T(0)) - axv;
     }
     if (step == nsteps) break;
@@ -702,12 +696,14 @@ __device__ __forceinline__ void block_solve_pivots(const JxbBlock& blk, const Si
 }
 
 template <typename T, int NT, bool GM>
-__global__ void __launch_bounds__(NT) sim_backward_kernel(JxbSimArgs a) {
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 1024 / NT : 1) sim_backward_kernel(JxbSimArgs a) {
   extern __shared__ __align__(16) char smem_raw[];
   SimSmem<T> sm;
   sim_smem_layout<T>(a, true, &sm, work_base<GM>(a, smem_raw));
   const JxbItem item = a.items[blockIdx.x];
   const JxbBlock blk = a.blocks[item.block];
+  sm.gbase = a.gbase + blk.node0;
+  if (a.gacc) sm.gacc = (T*)((char*)a.gacc + (size_t)blockIdx.x * (size_t)a.gacc_stride);
   const int rows = item.n_rows, row0 = item.row0;
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int nn = blk.n_nodes, ns = blk.n_slots, np = blk.n_pslots;
@@ -719,6 +715,7 @@ __global__ void __launch_bounds__(NT) sim_backward_kernel(JxbSimArgs a) {
   __syncthreads();
   init_voltages<T>(blk, sm, rows);
   __syncthreads();
+  sm.cm = (T*)a.cm + blk.node0;  // read only
   T* piv = (T*)a.traj_piv;
   run_steps<T>(a, blk, item.block, row0, rows, sm, dt, a.t0, K, 0, false, false, traj, sm.X1, piv);
 
@@ -847,6 +844,15 @@ int launch_sim(const JxbSimArgs& a, bool backward, cudaStream_t stream) {
   } else if (need > 227 * 1024) {
     snprintf(g_err, sizeof(g_err), "work item needs %zu bytes of shared memory", need);
     return JXB_ERR_SMEM;
+  }
+  if (backward && a.gacc) {
+    const size_t gneed = sizeof(T) * (size_t)a.max_rows * (size_t)a.max_gslots;
+    if (((uintptr_t)a.gacc & 255) != 0 || a.gacc_stride <= 0 || (a.gacc_stride & 255) != 0 ||
+        (size_t)a.gacc_stride < gneed) {
+      snprintf(g_err, sizeof(g_err),
+               "gacc must be 256-byte aligned with a stride (multiple of 256) of at least %zu bytes", gneed);
+      return JXB_ERR_ARG;
+    }
   }
   const size_t smem = gm ? 0 : need;
   const int threads = a.threads > 0 ? a.threads : 256;

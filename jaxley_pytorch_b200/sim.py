@@ -94,6 +94,7 @@ class DeviceModel:
         self.dtype = dtype
         self.device = torch.device(device)
         self.code = _dtype_code(dtype)
+        self.itemsize = torch.empty((), dtype=dtype).element_size()
         dev = self.device
 
         def f(x):
@@ -161,6 +162,8 @@ class DeviceModel:
         a = _lib.JxbSimArgs()
         a.dtype = self.code
         a.max_rows = self.rows_per_item
+        if backward:
+            a.gacc = 256  # gradient slots in global memory (placeholder address for sizing)
         for k, v in maxima.items():
             setattr(a, k, v)
         a.n_entries = int(self.low.entries.shape[0])
@@ -208,8 +211,10 @@ class DeviceModel:
                 items = [items[k] for k in np.argsort(-sizes, kind="stable")]
                 maxima = self._block_maxima(sel)
                 stride = (self._layout_bytes(maxima, bwd) + 255) // 256 * 256
+                gstride = (rows * maxima["max_gslots"] * self.itemsize + 255) // 256 * 256
                 groups.append({
                     "gm": c < 0, "maxima": maxima, "n_items": len(items), "stride": stride,
+                    "gacc_stride": gstride if bwd else 0, "key": (kind, c),
                     "items": torch.as_tensor(np.asarray(items, dtype=np.int32), device=self.device).contiguous(),
                 })
             self.groups[kind] = groups
@@ -269,12 +274,7 @@ class DeviceModel:
 
     def scratch(self, kind: str, group) -> torch.Tensor:
         """Global work areas of a group of oversized blocks (allocated once)."""
-        need = group["n_items"] * group["stride"] + 256
-        buf = self._scratch.get(kind)
-        if buf is None or buf.numel() < need:
-            buf = torch.empty(need, dtype=torch.uint8, device=self.device)
-            self._scratch[kind] = buf
-        return buf
+        return self._buffer(("work", kind), group["n_items"] * group["stride"] + 256)
 
     def group_args(self, args: _lib.JxbSimArgs, kind: str, group) -> _lib.JxbSimArgs:
         """A copy of `args` completed for one item group of a launch kind."""
@@ -287,7 +287,18 @@ class DeviceModel:
             buf = self.scratch(kind, group)
             a.gscratch = (buf.data_ptr() + 255) // 256 * 256
             a.gscratch_stride = group["stride"]
+        if group["gacc_stride"]:
+            buf = self._buffer(("gacc",) + group["key"], group["n_items"] * group["gacc_stride"] + 256)
+            a.gacc = (buf.data_ptr() + 255) // 256 * 256
+            a.gacc_stride = group["gacc_stride"]
         return a
+
+    def _buffer(self, key, nbytes: int) -> torch.Tensor:
+        buf = self._scratch.get(key)
+        if buf is None or buf.numel() < nbytes:
+            buf = torch.empty(nbytes, dtype=torch.uint8, device=self.device)
+            self._scratch[key] = buf
+        return buf
 
     def _launch(self, kind: str, fn, args, stream) -> None:
         st = torch.cuda.current_stream(self.device)
