@@ -9,6 +9,11 @@ gradient with respect to the 256 x 10 conductance scales through the adjoint
 (checkpoint every 100 steps). Compartment-steps count compartments x rows x steps
 (branchpoints excluded, every simulated step once).
 
+The same JSON line carries `uneven`: the uneven batch of 4096 seeded cells
+(log-uniform 4-3000 compartments, depth 1-60, HH or L5PC, 2000 steps, forward +
+adjoint), persistent (autotuned launches, whole iteration in one CUDA graph) against
+the plain per-step form (one launch per step and adjoint step), in compartment-steps/s.
+
 `--impl reference` times the CPU restatement of the reference's torch path (eager
 autograd) on the host cores, on a bounded sample of the same workload.
 
@@ -49,6 +54,11 @@ def parse():
     ap.add_argument("--cpu-batch", type=int, default=16)
     ap.add_argument("--cpu-tsteps", type=int, default=200)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-uneven", action="store_true",
+                    help="skip the uneven-batch persistent vs per-step measurement")
+    ap.add_argument("--uneven-cells", type=int, default=4096)
+    ap.add_argument("--uneven-tsteps", type=int, default=2000)
+    ap.add_argument("--uneven-plain-tsteps", type=int, default=100)
     return ap.parse_args()
 
 
@@ -278,6 +288,79 @@ def run_ours(args, rank, world, device):
     return out
 
 
+def run_uneven(args, device):
+    """Uneven batch: 4096 seeded cells (log-uniform 4-3000 compartments, depth 1-60,
+    HH or L5PC, own step current and trainable conductances), float32, 2000 steps,
+    forward + adjoint of an MSE loss. The persistent form (autotuned block size,
+    threads and checkpoint interval; the whole iteration replayed as one CUDA graph)
+    against the plain per-step form (one launch per step and per adjoint step,
+    checkpoint every step) on the same cells, the latter on a 100-step horizon."""
+    import torch
+
+    from jaxley_pytorch_b200 import synth
+    from jaxley_pytorch_b200.graphs import GraphedIteration
+    from jaxley_pytorch_b200.sim import Simulation
+    from jaxley_pytorch_b200.tune import autotune
+
+    T = args.uneven_tsteps
+    prob = synth.config_uneven(n_cells=args.uneven_cells, n_steps=T)
+    n_comp = int(len(prob.comp_inds))
+    choice, low, table = autotune(prob, dtype=torch.float32, device=device, probe_steps=40,
+                                  block_nodes=(1024, 2048), threads=(256, 512), rows=(1,),
+                                  checkpoints=(50, 100, 200), horizon=T, reps=1)
+
+    def timed(fn, reps):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        for _ in range(reps):
+            fn()
+        e1.record()
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    def loss_of(target):
+        return lambda rec: ((rec - target) ** 2).mean()
+
+    sim = Simulation(prob, low=low, dtype=torch.float32, device=device, threads=choice.threads,
+                     rows_per_item=choice.rows_per_item, checkpoint=choice.checkpoint)
+    ps0 = sim.model.pscale.clone()
+    with torch.no_grad():
+        target = sim.run(pscale=ps0 * 1.05).detach()
+    it = GraphedIteration(sim, loss_of(target), ps0.clone().requires_grad_(True), warmup=1)
+    ms = timed(it.replay, 2)
+    loss = float(it.loss)
+    launches = it.launches_per_replay
+    del it
+    # the plain per-step form: one launch per step, checkpoint every step
+    Tp = args.uneven_plain_tsteps
+    plain = Simulation(prob, low=low, dtype=torch.float32, device=device, threads=choice.threads,
+                       rows_per_item=choice.rows_per_item, checkpoint=1, segment=1)
+    with torch.no_grad():
+        tp = plain.run(n_steps=Tp, pscale=ps0 * 1.05).detach()
+
+    def plain_step():
+        ps = ps0.clone().requires_grad_(True)
+        rec = plain.run(n_steps=Tp, pscale=ps)
+        torch.autograd.grad(((rec - tp) ** 2).mean(), ps)
+
+    ms_plain = timed(plain_step, 2)
+    rate = n_comp * T / (ms / 1e3)
+    rate_plain = n_comp * Tp / (ms_plain / 1e3)
+    return {
+        "workload": f"uneven_{args.uneven_cells}cells_t{T}_fwd_adjoint", "cells": args.uneven_cells,
+        "compartments": n_comp, "nodes": prob.n_nodes, "time_steps": T,
+        "persistent": {"value": rate, "unit": UNIT, "ms_per_iteration": ms, "graph_launches": launches,
+                       "max_block_nodes": choice.max_block_nodes, "threads_per_cta": choice.threads,
+                       "checkpoint": choice.checkpoint, "loss": loss},
+        "per_step": {"value": rate_plain, "unit": UNIT, "ms_per_iteration": ms_plain, "time_steps": Tp,
+                     "checkpoint": 1},
+        "persistent_over_per_step": rate / rate_plain,
+        "tuning": table,
+    }
+
+
 def cpu_sample(batch: int, tsteps: int, reps: int = 1):
     """Times the torch CPU restatement of the reference path (forward + autograd
     backward) on `batch` rows x `tsteps` steps of the workload."""
@@ -341,6 +424,8 @@ def main():
                                              device_id=torch.device("cuda", local))
     device = torch.device("cuda", local)
     out = run_ours(args, rank, world, device)
+    if world == 1 and not args.no_uneven:
+        out["uneven"] = run_uneven(args, device)
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             v, cores, t = cpu_sample(args.cpu_batch, args.cpu_tsteps, reps=0)
