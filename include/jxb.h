@@ -113,7 +113,7 @@ typedef struct {
   int32_t pad;
 } JxbItem;
 
-typedef struct {
+typedef struct JxbSimArgs_ {
   int32_t dtype;
   int32_t batch;              /* rows of state / pscale / rec buffers */
   int32_t n_nodes, n_slots, n_pslots, n_cols;
@@ -202,6 +202,10 @@ typedef struct {
    * stride a multiple of 256. Null: the slots live in shared memory. */
   void* gacc;
   int64_t gacc_stride;
+  /* Set by jxb_sim_forward_multi / jxb_sim_backward_multi (leave null): the device
+   * copies of the requests' arguments and the (request, item) pair of every CTA. */
+  const struct JxbSimArgs_* multi;
+  const int32_t* multi_items;
 } JxbSimArgs;
 
 int jxb_sim_forward(const JxbSimArgs* args, void* stream);
@@ -220,6 +224,26 @@ int jxb_sim_backward(const JxbSimArgs* args, void* stream);
  * in the same launch. It calls no cudaMalloc, cudaFree or allocating library routine. */
 int jxb_sim_backward_noalloc(const JxbSimArgs* args, void* stream);
 int64_t jxb_sim_smem_bytes(const JxbSimArgs* args, int backward);
+
+/* Continuous batching of requests (no counterpart in the reference, whose
+ * `jx.integrate` simulates one module per call, integrate.py:396-666): one launch
+ * runs the work items of several independent problems. `launch` gives the
+ * work-area sizing (max_* fields at least each request's, n_entries and n_classes
+ * at least each request's, max_gslots for the adjoint), threads, and optional
+ * gscratch / gacc buffers indexed by the launch's CTA; `reqs` (host, n_reqs) are the
+ * requests' arguments as for jxb_sim_forward / jxb_sim_backward, each with its own
+ * state, time window (t0, n_steps), buffers and items; `pairs` (host, n_pairs x 2)
+ * the (request, item) pair of every CTA. The library validates every request and
+ * pair, copies them into `dev_scratch` (device, 256-byte aligned, at least
+ * jxb_sim_multi_scratch_bytes bytes) on `stream` and launches. The scratch must
+ * stay untouched until the launch has run. */
+int jxb_sim_forward_multi(const JxbSimArgs* launch, const JxbSimArgs* reqs, int n_reqs,
+                          const int32_t* pairs, int n_pairs, void* dev_scratch, int64_t scratch_bytes,
+                          void* stream);
+int jxb_sim_backward_multi(const JxbSimArgs* launch, const JxbSimArgs* reqs, int n_reqs,
+                           const int32_t* pairs, int n_pairs, void* dev_scratch, int64_t scratch_bytes,
+                           void* stream);
+int64_t jxb_sim_multi_scratch_bytes(int n_reqs, int n_pairs);
 
 /* ---------------------------------------------------------------------------------
  * Synapses in the regular layout (E = T * k synapses ordered by target).

@@ -73,6 +73,7 @@ class JxbSimArgs(C.Structure):
         ("gscratch", _p), ("gscratch_stride", C.c_int64),
         ("sched_ptr", _p), ("sched", _p), ("sched_warps", C.c_int32), ("pad5", C.c_int32),
         ("gacc", _p), ("gacc_stride", C.c_int64),
+        ("multi", _p), ("multi_items", _p),
     ]
 
 
@@ -98,6 +99,9 @@ EXPORTED = [
     "jxb_sim_backward",
     "jxb_sim_backward_noalloc",
     "jxb_sim_smem_bytes",
+    "jxb_sim_forward_multi",
+    "jxb_sim_backward_multi",
+    "jxb_sim_multi_scratch_bytes",
     "jxb_synapse_forward",
     "jxb_synapse_backward",
     "jxb_last_error",
@@ -125,6 +129,13 @@ def load(path: str = LIB_PATH) -> C.CDLL:
         fn = getattr(lib, name)
         fn.restype = C.c_int
         fn.argtypes = [C.POINTER(JxbSimArgs), C.c_void_p]
+    for name in ["jxb_sim_forward_multi", "jxb_sim_backward_multi"]:
+        fn = getattr(lib, name)
+        fn.restype = C.c_int
+        fn.argtypes = [C.POINTER(JxbSimArgs), C.POINTER(JxbSimArgs), C.c_int, _p, C.c_int, _p,
+                       C.c_int64, C.c_void_p]
+    lib.jxb_sim_multi_scratch_bytes.restype = C.c_int64
+    lib.jxb_sim_multi_scratch_bytes.argtypes = [C.c_int, C.c_int]
     for name in ["jxb_synapse_forward", "jxb_synapse_backward"]:
         fn = getattr(lib, name)
         fn.restype = C.c_int

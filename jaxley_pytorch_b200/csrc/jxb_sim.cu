@@ -121,7 +121,8 @@ __host__ __device__ inline size_t sim_smem_layout(const JxbSimArgs& a, bool back
 // item's rows and the rows' states (and adjoints) in shared memory.
 template <typename T>
 __device__ __forceinline__ void stage_item(const JxbSimArgs& a, const JxbBlock& blk, int row0, int rows,
-                           const SimSmem<T>& sm, T dt, const T* state_src, const T* adj_src) {
+                                           const SimSmem<T>& sm, T dt, const T* state_src, const T* adj_src,
+                                           int gslots = 0) {
   const int tid = threadIdx.x, NT = blockDim.x;
   const int nn = blk.n_nodes, ns = blk.n_slots, node0 = blk.node0;
   const T* gl = (const T*)a.a_low;
@@ -201,7 +202,7 @@ __device__ __forceinline__ void stage_item(const JxbSimArgs& a, const JxbBlock& 
     }
   }
   if (sm.gacc) {
-    for (int q = tid; q < rows * a.max_gslots; q += NT) sm.gacc[q] = T(0);
+    for (int q = tid; q < rows * gslots; q += NT) sm.gacc[q] = T(0);
   }
 }
 
@@ -547,13 +548,14 @@ __device__ __forceinline__ char* work_base(const JxbSimArgs& a, char* smem_raw) 
   return smem_raw;
 }
 
-// float: at most 64 registers, so that two 512-thread CTAs (four of 256) fit an SM.
-template <typename T, int NT, bool GM>
-__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 1024 / NT : 1) sim_forward_kernel(JxbSimArgs a) {
-  extern __shared__ __align__(16) char smem_raw[];
+// Forward launch of one work item: `a` describes the problem (a request), `L` the
+// launch (work-area sizing, global scratch).
+template <typename T, bool GM>
+__device__ __forceinline__ void sim_forward_body(const JxbSimArgs& a, const JxbSimArgs& L, int item_idx,
+                                                 char* smem_raw) {
   SimSmem<T> sm;
-  sim_smem_layout<T>(a, false, &sm, work_base<GM>(a, smem_raw));
-  const JxbItem item = a.items[blockIdx.x];
+  sim_smem_layout<T>(L, false, &sm, work_base<GM>(L, smem_raw));
+  const JxbItem item = a.items[item_idx];
   const JxbBlock blk = a.blocks[item.block];
   const int rows = item.n_rows, row0 = item.row0;
   const T dt = T(a.dt);
@@ -695,15 +697,17 @@ __device__ __forceinline__ void block_solve_pivots(const JxbBlock& blk, const Si
   }
 }
 
-template <typename T, int NT, bool GM>
-__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 1024 / NT : 1) sim_backward_kernel(JxbSimArgs a) {
-  extern __shared__ __align__(16) char smem_raw[];
+// Adjoint launch of one work item (`a`: the problem, `L`: the launch).
+template <typename T, bool GM>
+__device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const JxbSimArgs& L, int item_idx,
+                                                  char* smem_raw) {
   SimSmem<T> sm;
-  sim_smem_layout<T>(a, true, &sm, work_base<GM>(a, smem_raw));
-  const JxbItem item = a.items[blockIdx.x];
+  sim_smem_layout<T>(L, true, &sm, work_base<GM>(L, smem_raw));
+  const JxbItem item = a.items[item_idx];
   const JxbBlock blk = a.blocks[item.block];
   sm.gbase = a.gbase + blk.node0;
-  if (a.gacc) sm.gacc = (T*)((char*)a.gacc + (size_t)blockIdx.x * (size_t)a.gacc_stride);
+  if (L.gacc) sm.gacc = (T*)((char*)L.gacc + (size_t)blockIdx.x * (size_t)L.gacc_stride);
+  const int gslots = L.max_gslots;
   const int rows = item.n_rows, row0 = item.row0;
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int nn = blk.n_nodes, ns = blk.n_slots, np = blk.n_pslots;
@@ -711,7 +715,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 1024 / NT : 1) sim_backwa
   const int K = a.n_steps;
   T* traj = (T*)a.traj;
   // Recompute the segment from its checkpoint, storing the state before every step.
-  stage_item<T>(a, blk, row0, rows, sm, dt, (const T*)a.ckpt, (const T*)a.adj);
+  stage_item<T>(a, blk, row0, rows, sm, dt, (const T*)a.ckpt, (const T*)a.adj, gslots);
   __syncthreads();
   init_voltages<T>(blk, sm, rows);
   __syncthreads();
@@ -764,7 +768,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 1024 / NT : 1) sim_backwa
       T lv = comp ? lr : T(0);
       lam[0] = T(0);
       node_adjoint<T>(sm, j, x, lam, sm.pv + (size_t)r * np,
-                      sm.gacc + (size_t)r * a.max_gslots, dt, lrs, xnew, lv);
+                      sm.gacc + (size_t)r * gslots, dt, lrs, xnew, lv);
       lam[0] = lv;
       sm.X1[(size_t)r * nn + j] = x[0];
     }
@@ -779,7 +783,7 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 1024 / NT : 1) sim_backwa
     int npar = 0;
     for (int q = sm.cptr[cls]; q < sm.cptr[cls + 1]; ++q) npar += sm.ents[q].np;
     const int po = sm.poff[j];
-    const T* ga = sm.gacc + (size_t)r * a.max_gslots + sm.gbase[j];
+    const T* ga = sm.gacc + (size_t)r * gslots + sm.gbase[j];
     double* pg = a.pgrad + (size_t)(row0 + r) * a.n_cols;
     for (int k = 0; k < npar; ++k) {
       const int q = sm.gk[po + k];
@@ -794,10 +798,58 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 1024 / NT : 1) sim_backwa
   }
 }
 
+// Arguments of a request in a multi-request launch, copied into shared memory.
+template <typename T>
+__device__ JxbSimArgs& request_args_slot() {
+  __shared__ JxbSimArgs s;
+  return s;
+}
+
+// A launch runs the items of one problem (`L.items`), or, with `L.multi`, the
+// (request, item) pairs `L.multi_items` of several problems whose arguments are in
+// `L.multi` (continuous batching of requests); the work-area sizing and global
+// scratch are the launch's.
+template <typename T, bool MULTI>
+__device__ __forceinline__ const JxbSimArgs& item_args(const JxbSimArgs& L, int& item_idx) {
+  item_idx = blockIdx.x;
+  if constexpr (MULTI) {
+    JxbSimArgs& s = request_args_slot<T>();
+    const int2 mi = reinterpret_cast<const int2*>(L.multi_items)[blockIdx.x];
+    const unsigned long long* src = reinterpret_cast<const unsigned long long*>(L.multi + mi.x);
+    unsigned long long* dst = reinterpret_cast<unsigned long long*>(&s);
+    for (int q = threadIdx.x; q < (int)(sizeof(JxbSimArgs) / 8); q += blockDim.x) dst[q] = src[q];
+    __syncthreads();
+    item_idx = mi.y;
+    return s;
+  }
+  return L;
+}
+
+// float: at most 64 registers, so that two 512-thread CTAs (four of 256) fit an SM.
+template <typename T, int NT, bool GM, bool MULTI>
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 1024 / NT : 1) sim_forward_kernel(JxbSimArgs L) {
+  extern __shared__ __align__(16) char smem_raw[];
+  int item_idx;
+  const JxbSimArgs& a = item_args<T, MULTI>(L, item_idx);
+  sim_forward_body<T, GM>(a, L, item_idx, smem_raw);
+}
+
+template <typename T, int NT, bool GM, bool MULTI>
+__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 1024 / NT : 1) sim_backward_kernel(JxbSimArgs L) {
+  extern __shared__ __align__(16) char smem_raw[];
+  int item_idx;
+  const JxbSimArgs& a = item_args<T, MULTI>(L, item_idx);
+  sim_backward_body<T, GM>(a, L, item_idx, smem_raw);
+}
+
 template <typename T, int NT>
-void (*pick_kernel(bool backward, bool gm))(JxbSimArgs) {
-  if (gm) return backward ? sim_backward_kernel<T, NT, true> : sim_forward_kernel<T, NT, true>;
-  return backward ? sim_backward_kernel<T, NT, false> : sim_forward_kernel<T, NT, false>;
+void (*pick_kernel(bool backward, bool gm, bool multi))(JxbSimArgs) {
+  if (multi) {
+    if (gm) return backward ? sim_backward_kernel<T, NT, true, true> : sim_forward_kernel<T, NT, true, true>;
+    return backward ? sim_backward_kernel<T, NT, false, true> : sim_forward_kernel<T, NT, false, true>;
+  }
+  if (gm) return backward ? sim_backward_kernel<T, NT, true, false> : sim_forward_kernel<T, NT, true, false>;
+  return backward ? sim_backward_kernel<T, NT, false, false> : sim_forward_kernel<T, NT, false, false>;
 }
 
 // Largest dynamic shared memory already granted to a kernel on a device:
@@ -863,11 +915,11 @@ int launch_sim(const JxbSimArgs& a, bool backward, cudaStream_t stream) {
   // Register budget by launch size: up to 256 threads, 512, 1024.
   void (*kern)(JxbSimArgs);
   if (threads <= 256)
-    kern = pick_kernel<T, 256>(backward, gm);
+    kern = pick_kernel<T, 256>(backward, gm, a.multi != nullptr);
   else if (threads <= 512)
-    kern = pick_kernel<T, 512>(backward, gm);
+    kern = pick_kernel<T, 512>(backward, gm, a.multi != nullptr);
   else
-    kern = pick_kernel<T, 1024>(backward, gm);
+    kern = pick_kernel<T, 1024>(backward, gm, a.multi != nullptr);
   cudaError_t e = grant_smem((const void*)kern, smem);
   if (e != cudaSuccess) {
     set_err("cudaFuncSetAttribute", e);
@@ -945,6 +997,83 @@ extern "C" int jxb_sim_backward(const JxbSimArgs* a, void* stream) {
   if (rc != JXB_OK || a->n_items <= 0) return rc;
   if (a->dtype == JXB_F32) return launch_sim<float>(*a, true, (cudaStream_t)stream);
   return launch_sim<double>(*a, true, (cudaStream_t)stream);
+}
+
+// ---------------------------------------------------------------------------------
+// Continuous batching: one launch over the work items of several problems.
+// ---------------------------------------------------------------------------------
+static size_t multi_pairs_offset(int n_reqs) { return (sizeof(JxbSimArgs) * (size_t)n_reqs + 255) / 256 * 256; }
+
+extern "C" int64_t jxb_sim_multi_scratch_bytes(int n_reqs, int n_pairs) {
+  if (n_reqs < 0 || n_pairs < 0) return -1;
+  return (int64_t)(multi_pairs_offset(n_reqs) + sizeof(int32_t) * 2 * (size_t)n_pairs);
+}
+
+static int launch_multi(const JxbSimArgs* launch, const JxbSimArgs* reqs, int n_reqs, const int32_t* pairs,
+                        int n_pairs, void* dev_scratch, int64_t scratch_bytes, void* stream, bool backward) {
+  if (!launch || (n_reqs > 0 && !reqs) || (n_pairs > 0 && !pairs) || n_reqs < 0 || n_pairs < 0)
+    return JXB_ERR_ARG;
+  if (launch->dtype != JXB_F32 && launch->dtype != JXB_F64) return JXB_ERR_DTYPE;
+  if (n_pairs == 0) return JXB_OK;
+  if (!dev_scratch || ((uintptr_t)dev_scratch & 255) != 0 ||
+      scratch_bytes < jxb_sim_multi_scratch_bytes(n_reqs, n_pairs)) {
+    snprintf(g_err, sizeof(g_err), "multi launch: device scratch of %lld bytes (256-byte aligned) needed",
+             (long long)jxb_sim_multi_scratch_bytes(n_reqs, n_pairs));
+    return JXB_ERR_ARG;
+  }
+  const JxbSimArgs& L = *launch;
+  if (L.max_rows <= 0 || L.max_nodes <= 0 || L.max_nodes > 32767 || L.max_slots <= 0) {
+    snprintf(g_err, sizeof(g_err), "multi launch: bad block sizes");
+    return JXB_ERR_ARG;
+  }
+  for (int r = 0; r < n_reqs; ++r) {
+    const JxbSimArgs& q = reqs[r];
+    if (q.dtype != L.dtype) return JXB_ERR_DTYPE;
+    int rc = check_sim_args(&q, backward);
+    if (rc != JXB_OK) return rc;
+    if (q.max_rows > L.max_rows || q.max_nodes > L.max_nodes || q.max_slots > L.max_slots ||
+        q.max_chains > L.max_chains || q.max_child > L.max_child || q.max_levels > L.max_levels ||
+        q.max_pslots > L.max_pslots || q.n_entries > L.n_entries || q.n_classes > L.n_classes ||
+        (backward && q.max_gslots > L.max_gslots)) {
+      snprintf(g_err, sizeof(g_err), "multi launch: request %d exceeds the launch's block sizes", r);
+      return JXB_ERR_ARG;
+    }
+  }
+  for (int k = 0; k < n_pairs; ++k) {
+    const int r = pairs[2 * k], it = pairs[2 * k + 1];
+    if (r < 0 || r >= n_reqs || it < 0 || it >= reqs[r].n_items) {
+      snprintf(g_err, sizeof(g_err), "multi launch: pair %d (request %d, item %d) out of range", k, r, it);
+      return JXB_ERR_ARG;
+    }
+  }
+  cudaStream_t st = (cudaStream_t)stream;
+  char* dev = (char*)dev_scratch;
+  cudaError_t e = cudaMemcpyAsync(dev, reqs, sizeof(JxbSimArgs) * (size_t)n_reqs, cudaMemcpyHostToDevice, st);
+  if (e == cudaSuccess)
+    e = cudaMemcpyAsync(dev + multi_pairs_offset(n_reqs), pairs, sizeof(int32_t) * 2 * (size_t)n_pairs,
+                        cudaMemcpyHostToDevice, st);
+  if (e != cudaSuccess) {
+    set_err("cudaMemcpyAsync", e);
+    return JXB_ERR_LAUNCH;
+  }
+  JxbSimArgs M = L;
+  M.multi = (const JxbSimArgs*)dev;
+  M.multi_items = (const int32_t*)(dev + multi_pairs_offset(n_reqs));
+  M.n_items = n_pairs;
+  if (M.dtype == JXB_F32) return launch_sim<float>(M, backward, st);
+  return launch_sim<double>(M, backward, st);
+}
+
+extern "C" int jxb_sim_forward_multi(const JxbSimArgs* launch, const JxbSimArgs* reqs, int n_reqs,
+                                     const int32_t* pairs, int n_pairs, void* dev_scratch,
+                                     int64_t scratch_bytes, void* stream) {
+  return launch_multi(launch, reqs, n_reqs, pairs, n_pairs, dev_scratch, scratch_bytes, stream, false);
+}
+
+extern "C" int jxb_sim_backward_multi(const JxbSimArgs* launch, const JxbSimArgs* reqs, int n_reqs,
+                                      const int32_t* pairs, int n_pairs, void* dev_scratch,
+                                      int64_t scratch_bytes, void* stream) {
+  return launch_multi(launch, reqs, n_reqs, pairs, n_pairs, dev_scratch, scratch_bytes, stream, true);
 }
 
 extern "C" int64_t jxb_sim_smem_bytes(const JxbSimArgs* a, int backward) {
