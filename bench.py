@@ -14,6 +14,11 @@ The same JSON line carries `uneven`: the uneven batch of 4096 seeded cells
 adjoint), persistent (autotuned launches, whole iteration in one CUDA graph) against
 the plain per-step form (one launch per step and adjoint step), in compartment-steps/s.
 
+and `serving`: a Poisson stream of single-cell simulation and gradient requests
+(8-3000 compartments, 5-200 ms, 30 % gradients) at 80 % of the server's measured
+capacity, served with continuous batching: p50/p99 latency and throughput, beside the
+plain one-request-at-a-time path on the same arrivals.
+
 `--impl reference` times the CPU restatement of the reference's torch path (eager
 autograd) on the host cores, on a bounded sample of the same workload.
 
@@ -59,6 +64,9 @@ def parse():
     ap.add_argument("--uneven-cells", type=int, default=4096)
     ap.add_argument("--uneven-tsteps", type=int, default=2000)
     ap.add_argument("--uneven-plain-tsteps", type=int, default=100)
+    ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream measurement")
+    ap.add_argument("--serve-requests", type=int, default=240)
+    ap.add_argument("--serve-capacity-requests", type=int, default=160)
     return ap.parse_args()
 
 
@@ -361,6 +369,48 @@ def run_uneven(args, device):
     }
 
 
+def run_serving(args, device):
+    """Serving stream: seeded single-cell requests from the uneven-batch generator
+    (8-3000 compartments), horizons U[5, 200] ms, 30 % with gradients, float32.
+    For each scheduling policy (equal progress: every request advances by 1/16 of
+    its work per tick; fixed: 200 steps per tick) the capacity is measured on a
+    closed batch (all requests waiting), then Poisson arrivals at 80 % of that
+    capacity give p50/p99 latency and compartment-steps/s. The plain per-request
+    path (one request at a time) runs on the same arrivals, bounded to the same wall
+    time."""
+    from jaxley_pytorch_b200.serve import Request, Server, make_stream, serve_plain
+
+    def copy(reqs, zero=False):
+        return [Request(problem=r.problem, n_steps=r.n_steps, grad=r.grad, arrival=0.0 if zero else r.arrival,
+                        rid=r.rid) for r in reqs]
+
+    policies = {"equal_progress_16": dict(progress_ticks=16, chunk=200, checkpoint=200),
+                "fixed_chunk_200": dict(progress_ticks=0, chunk=200, checkpoint=200)}
+    Server(device=device, threads=256, **policies["fixed_chunk_200"]).run(make_stream(8, seed=99, rate=1e6))
+    closed = make_stream(args.serve_capacity_requests, seed=7, rate=1e9)
+    out = {"workload": "serving_stream_8_3000comp_5_200ms_30pct_grad", "unit": UNIT, "policies": {}}
+    stream = None
+    for name, pol in policies.items():
+        cap = Server(device=device, threads=256, **pol).run(copy(closed, zero=True))
+        capacity = cap["requests"] / cap["makespan_s"]
+        stream = make_stream(args.serve_requests, seed=8, rate=0.8 * capacity)
+        st = Server(device=device, threads=256, **pol).run(stream)
+        out["policies"][name] = {
+            "capacity_rps": capacity, "closed_batch_throughput": cap["throughput"],
+            "arrival_rate_rps": 0.8 * capacity, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "p99_over_p50": st["p99_over_p50"], "throughput": st["throughput"], "requests": st["requests"],
+            "ticks": st["ticks"], "launches": st["launches"], "makespan_s": st["makespan_s"]}
+    first = out["policies"]["equal_progress_16"]
+    out.update({k: first[k] for k in ("p50_ms", "p99_ms", "p99_over_p50", "throughput", "capacity_rps",
+                                      "arrival_rate_rps")})
+    stream = make_stream(args.serve_requests, seed=8, rate=first["arrival_rate_rps"])
+    pl = serve_plain(copy(stream), device=device, threads=256, checkpoint=200, time_limit=first["makespan_s"])
+    out["plain_per_request"] = {"p50_ms": pl["p50_ms"], "p99_ms": pl["p99_ms"], "throughput": pl["throughput"],
+                                "requests_done": pl["requests"], "of": len(stream), "wall_s": pl["makespan_s"]}
+    out["throughput_over_plain"] = first["throughput"] / pl["throughput"] if pl["throughput"] else None
+    return out
+
+
 def cpu_sample(batch: int, tsteps: int, reps: int = 1):
     """Times the torch CPU restatement of the reference path (forward + autograd
     backward) on `batch` rows x `tsteps` steps of the workload."""
@@ -426,6 +476,8 @@ def main():
     out = run_ours(args, rank, world, device)
     if world == 1 and not args.no_uneven:
         out["uneven"] = run_uneven(args, device)
+    if world == 1 and not args.no_serving:
+        out["serving"] = run_serving(args, device)
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             v, cores, t = cpu_sample(args.cpu_batch, args.cpu_tsteps, reps=0)

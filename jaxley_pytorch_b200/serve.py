@@ -74,14 +74,27 @@ class _Active:
         self.req = req
         dev, dtype = server.device, server.dtype
         self.low = lower(req.problem, max_block_nodes=server.max_block_nodes, keep_currents=False)
-        self.model = DeviceModel(self.low, dtype, dev, 1, threads=server.threads, smem_limit=1 << 30)
-        (self.group_f,) = self.model.groups["forward"]
-        (self.group_b,) = self.model.groups["backward"]
-        items = self.group_f["items"].cpu().numpy()
-        self.item_nodes = self.low.blocks[items[:, 0], 1].astype(np.int64)  # nodes of every item
+        self.model = DeviceModel(self.low, dtype, dev, 1, threads=server.threads,
+                                 smem_limit=server.smem_limit)
+        # all items of the request in one set for the multi-request launches
+        low = self.low
+        items = np.asarray([[b, r, 1, 0] for b in range(len(low.blocks)) for r in range(low.batch)],
+                           dtype=np.int32)
+        items = items[np.argsort(-low.blocks[items[:, 0], 1], kind="stable")]
+        self.item_nodes = low.blocks[items[:, 0], 1].astype(np.int64)  # nodes of every item
+        group = {"maxima": self.model._block_maxima(np.arange(len(low.blocks))),
+                 "items": torch.as_tensor(items, device=dev).contiguous(), "n_items": len(items)}
+        self.group_f = self.group_b = group
         m, low = self.model, self.low
         self.T = int(req.n_steps)
-        self.K = min(server.checkpoint, self.T)
+        if server.progress_ticks:
+            # equal progress: every request needs about `progress_ticks` ticks (a gradient
+            # request half of them forward, half adjoint), whatever its horizon
+            n = max(1, server.progress_ticks // (2 if req.grad else 1))
+            self.chunk = max(server.min_chunk, -(-self.T // n))
+        else:
+            self.chunk = server.chunk
+        self.K = min(self.chunk if server.progress_ticks else server.checkpoint, self.T)
         self.nseg = (self.T + self.K - 1) // self.K
         self.state = m.initial_state()
         self.rec = torch.zeros((self.T + 1, low.batch, low.n_rec), dtype=dtype, device=dev)
@@ -103,24 +116,34 @@ class _Active:
         # initial currents (and the first recording)
         a = m.args(self.state, 0, 0, self.rec, mode=1, pscale=self.pscale)
         m.launch_forward(a)
+        # argument templates: a tick only sets the time window (and the checkpoint)
+        self.base_f = self._items(m.args(self.state, 1, 0, self.rec, pscale=self.pscale,
+                                         ckpt=self.ckpt if req.grad else None,
+                                         ckpt_every=self.K if req.grad else 0), self.group_f)
+        if req.grad:
+            b = m.args(self.ckpt[0], 1, 0, None, pscale=self.pscale, traj=self.traj, adj=self.adj,
+                       rec_grad=self.rec_grad, pgrad=self.pgrad)
+            b.traj_piv = self.piv.data_ptr()
+            self.base_b = self._items(b, self.group_b)
+            self.ckpt_ptr0 = self.ckpt.data_ptr()
+            self.ckpt_stride = self.ckpt[0].numel() * self.ckpt.element_size()
+        self.sizes = {k: np.asarray([int(getattr(self.base_f, f)) for f in _SIZE_FIELDS], dtype=np.int64)
+                      for k in ("forward", "backward")}
 
-    def forward_args(self, chunk: int) -> Tuple[_lib.JxbSimArgs, int]:
-        k = min(chunk, self.T - self.t)
-        m = self.model
-        a = m.args(self.state, k, self.t, self.rec, pscale=self.pscale,
-                   ckpt=self.ckpt if self.req.grad else None,
-                   ckpt_every=self.K if self.req.grad else 0)
-        return self._items(a, self.group_f), k
+    def forward_args(self) -> Tuple[_lib.JxbSimArgs, int]:
+        k = min(self.chunk, self.T - self.t)
+        a = _lib.JxbSimArgs.from_buffer_copy(self.base_f)
+        a.n_steps = k
+        a.t0 = self.t
+        return a, k
 
     def backward_args(self) -> _lib.JxbSimArgs:
-        m = self.model
         t0 = self.seg * self.K
-        k = min(self.K, self.T - t0)
-        a = m.args(self.ckpt[self.seg], k, t0, None, pscale=self.pscale, traj=self.traj, adj=self.adj,
-                   rec_grad=self.rec_grad, pgrad=self.pgrad)
-        a.ckpt = self.ckpt[self.seg].data_ptr()
-        a.traj_piv = self.piv.data_ptr()
-        return self._items(a, self.group_b)
+        a = _lib.JxbSimArgs.from_buffer_copy(self.base_b)
+        a.n_steps = min(self.K, self.T - t0)
+        a.t0 = t0
+        a.ckpt = self.ckpt_ptr0 + self.seg * self.ckpt_stride
+        return a
 
     @staticmethod
     def _items(a: _lib.JxbSimArgs, group) -> _lib.JxbSimArgs:
@@ -147,6 +170,11 @@ def launch_sizes(args: Sequence[_lib.JxbSimArgs]) -> Dict[str, int]:
     return {f: max([int(getattr(a, f)) for a in args] + [1]) for f in _SIZE_FIELDS}
 
 
+def _stacked_sizes(sizes: Sequence[np.ndarray]) -> Dict[str, int]:
+    mx = np.max(np.stack(sizes), axis=0) if len(sizes) else np.ones(len(_SIZE_FIELDS), np.int64)
+    return {f: max(1, int(v)) for f, v in zip(_SIZE_FIELDS, mx)}
+
+
 def pair_list(item_nodes: Sequence[np.ndarray]) -> np.ndarray:
     """(request, item) of every CTA of a multi-request launch, items of more nodes
     first (CTAs are scheduled roughly in index order). `item_nodes[r]` holds the node
@@ -163,7 +191,8 @@ class Server:
 
     def __init__(self, device="cuda", dtype=torch.float32, hbm_budget: Optional[int] = None,
                  chunk: int = 200, threads: int = 256, checkpoint: int = 100,
-                 max_block_nodes: int = 4096, max_active: int = 4096):
+                 max_block_nodes: int = 4096, max_active: int = 4096, progress_ticks: int = 0,
+                 min_chunk: int = 20):
         self.device = torch.device(device)
         self.dtype = dtype
         self.code = _lib.F32 if dtype == torch.float32 else _lib.F64
@@ -172,6 +201,8 @@ class Server:
             hbm_budget = int(free * 0.5)
         self.hbm_budget = int(hbm_budget)
         self.chunk = int(chunk)
+        self.progress_ticks = int(progress_ticks)  # 0: fixed chunk of `chunk` steps per tick
+        self.min_chunk = int(min_chunk)
         self.threads = int(threads)
         self.checkpoint = int(checkpoint)
         self.max_block_nodes = int(max_block_nodes)
@@ -224,7 +255,7 @@ class Server:
         L = _lib.JxbSimArgs()
         L.dtype = self.code
         L.threads = self.threads
-        for f, v in launch_sizes(args).items():
+        for f, v in _stacked_sizes([act.sizes[kind] for act in acts]).items():
             setattr(L, f, v)
         pairs = pair_list([act.item_nodes for act in acts])
         n = len(pairs)
@@ -261,7 +292,7 @@ class Server:
         steps: Dict[int, int] = {}
         for act in self.active:
             if act.phase == "fwd":
-                a, k = act.forward_args(self.chunk)
+                a, k = act.forward_args()
                 steps[id(act)] = k
                 key = ("forward", act.gm["forward"])
             else:
