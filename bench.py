@@ -14,7 +14,9 @@ The same JSON line carries `uneven`: the uneven batch of 4096 seeded cells
 adjoint), persistent (autotuned launches, whole iteration in one CUDA graph) against
 the plain per-step form (one launch per step and adjoint step), in compartment-steps/s.
 
-and `serving`: a Poisson stream of single-cell simulation and gradient requests
+`network`: a training step (simulation, MSE, adjoint, capturable Adam on the synaptic
+weights, one CUDA graph) of 2048 4-compartment HH cells with in-degree 64 of two
+synapse types, 32 rows of Poisson input, 2000 steps; and `serving`: a Poisson stream of single-cell simulation and gradient requests
 (8-3000 compartments, 5-200 ms, 30 % gradients) at 80 % of the server's measured
 capacity, served with continuous batching: p50/p99 latency and throughput, beside the
 plain one-request-at-a-time path on the same arrivals.
@@ -65,6 +67,8 @@ def parse():
     ap.add_argument("--uneven-tsteps", type=int, default=2000)
     ap.add_argument("--uneven-plain-tsteps", type=int, default=100)
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream measurement")
+    ap.add_argument("--no-network", action="store_true", help="skip the network training-step measurement")
+    ap.add_argument("--net-tsteps", type=int, default=2000)
     ap.add_argument("--serve-requests", type=int, default=240)
     ap.add_argument("--serve-capacity-requests", type=int, default=160)
     return ap.parse_args()
@@ -411,6 +415,56 @@ def run_serving(args, device):
     return out
 
 
+def run_network(args, device):
+    """Fixed in-degree network: 2048 HH cells of 1 branch x 4 compartments, 64
+    KineticSynapse and 64 SigmoidRateSynapse inputs on compartment 0 of every cell
+    (131,072 synapses per type, gS ~ U[0, 1e-3] uS), 32 rows of Poisson input (20 Hz,
+    0.2 nA one-step pulses), float32, 2000 steps. One training step = the simulation,
+    the MSE of all somatic voltages to a target, the adjoint, and Adam
+    (capturable) on the synaptic weights of both types, replayed as one CUDA graph."""
+    import torch
+
+    from jaxley_pytorch_b200.graphs import GraphedIteration
+    from jaxley_pytorch_b200.network import NetworkSimulation, config_network
+
+    T = args.net_tsteps
+    prob = config_network(n_cells=2048, ncomp=4, k=64, batch=32, n_steps=T, seed=0)
+    net = NetworkSimulation(prob, dtype=torch.float32, device=device, checkpoint=50, threads=256,
+                            max_block_nodes=256)
+    sizes = [ty.E for ty in net.types]
+    with torch.no_grad():
+        tgt_params = [[ty.params[0] * 1.2] + ty.params[1:] for ty in net.types]
+        target = net.run(net.model.pscale, tgt_params).detach()
+
+    def run(w):
+        parts = torch.split(w, sizes)
+        return net.run(net.model.pscale, [[parts[t]] + ty.params[1:] for t, ty in enumerate(net.types)])
+
+    def loss_fn(rec):
+        return ((rec - target) ** 2).mean()
+
+    w = torch.cat([ty.params[0] for ty in net.types]).clone().requires_grad_(True)
+    it = GraphedIteration(net, loss_fn, w, optimizer=torch.optim.Adam([w], lr=1e-6, capturable=True),
+                          warmup=1, run=run)
+    it.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 2
+    e0.record()
+    for _ in range(reps):
+        it.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    n_comp = len(prob.comp_inds)
+    return {"workload": f"network_2048x4_k64x2_b32_t{T}_train_step", "compartments": n_comp,
+            "synapses": int(sum(sizes)), "batch": 32, "time_steps": T,
+            "value": n_comp * 32 * T / (ms / 1e3), "unit": UNIT,
+            "synapse_steps_per_s": sum(sizes) * 32 * T / (ms / 1e3),
+            "ms_per_training_step": ms, "graph_launches": it.launches_per_replay,
+            "loss": float(it.loss)}
+
+
 def cpu_sample(batch: int, tsteps: int, reps: int = 1):
     """Times the torch CPU restatement of the reference path (forward + autograd
     backward) on `batch` rows x `tsteps` steps of the workload."""
@@ -478,6 +532,8 @@ def main():
         out["uneven"] = run_uneven(args, device)
     if world == 1 and not args.no_serving:
         out["serving"] = run_serving(args, device)
+    if world == 1 and not args.no_network:
+        out["network"] = run_network(args, device)
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             v, cores, t = cpu_sample(args.cpu_batch, args.cpu_tsteps, reps=0)

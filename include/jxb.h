@@ -206,6 +206,19 @@ typedef struct JxbSimArgs_ {
    * copies of the requests' arguments and the (request, item) pair of every CTA. */
   const struct JxbSimArgs_* multi;
   const int32_t* multi_items;
+  /* Synapse outputs by target (optional; needs syn_lin/syn_const): with syn_ptr set,
+   * syn_lin/syn_const hold the synapse step's per-target slope and offset of every
+   * synapse type (the `lin`, `const` outputs of jxb_synapse_forward, concatenated),
+   * and node i (internal order) adds, for q in [syn_ptr[i], syn_ptr[i+1]) and row b,
+   * lin += syn_lin[syn_off[q] + b * syn_rs[q]] and const -= syn_const[...], as the
+   * reference's index_add of (lin, -const) (modules/network.py:402-407). The adjoint
+   * then writes d loss / d syn_lin and d loss / d syn_const of its step to
+   * g_syn_lin / g_syn_const at the same positions. */
+  const int32_t* syn_ptr;
+  const int32_t* syn_off;
+  const int32_t* syn_rs;
+  void* g_syn_lin;
+  void* g_syn_const;
 } JxbSimArgs;
 
 int jxb_sim_forward(const JxbSimArgs* args, void* stream);

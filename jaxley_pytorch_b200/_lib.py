@@ -74,6 +74,7 @@ class JxbSimArgs(C.Structure):
         ("sched_ptr", _p), ("sched", _p), ("sched_warps", C.c_int32), ("pad5", C.c_int32),
         ("gacc", _p), ("gacc_stride", C.c_int64),
         ("multi", _p), ("multi_items", _p),
+        ("syn_ptr", _p), ("syn_off", _p), ("syn_rs", _p), ("g_syn_lin", _p), ("g_syn_const", _p),
     ]
 
 

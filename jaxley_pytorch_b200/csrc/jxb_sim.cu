@@ -514,8 +514,16 @@ __device__ __forceinline__ void run_steps(const JxbSimArgs& a, const JxbBlock& b
       node_channels<T>(sm, j, x, sm.pv + (size_t)r * np, dt, 0, lin, cst);
       if (f & FLAG_STIM) cst += stim_current<T>(a, i, b, t);
       if (a.syn_lin) {
-        lin += ((const T*)a.syn_lin)[(size_t)b * a.n_nodes + i];
-        cst += ((const T*)a.syn_const)[(size_t)b * a.n_nodes + i];
+        if (a.syn_ptr) {  // per-target synapse outputs (modules/network.py:402-407)
+          for (int q = a.syn_ptr[i]; q < a.syn_ptr[i + 1]; ++q) {
+            const size_t o = (size_t)a.syn_off[q] + (size_t)b * a.syn_rs[q];
+            lin += ((const T*)a.syn_lin)[o];
+            cst -= ((const T*)a.syn_const)[o];
+          }
+        } else {
+          lin += ((const T*)a.syn_lin)[(size_t)b * a.n_nodes + i];
+          cst += ((const T*)a.syn_const)[(size_t)b * a.n_nodes + i];
+        }
       }
       const T cmv = sm.cm[j];
       // Delta form of the implicit step: A (v' - v) = rhs - A v, with
@@ -766,6 +774,20 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
       // branchpoints have no channels).
       const T lrs = T(1000.0) * dt * lr / sm.cm[j];
       T lv = comp ? lr : T(0);
+      if (a.g_syn_lin && a.syn_ptr) {
+        // d loss / d (synaptic slope, offset) of node j: the slope enters the
+        // diagonal (and, on compartments, the right-hand side as -lin * v), the
+        // offset the right-hand side with a minus sign.
+        const int i = blk.node0 + j;
+        const T f = lr * dt / sm.cm[j];
+        const T gl = comp ? -f * xnew : -f * (xnew - x[0]);
+        const T gc = comp ? -f : T(0);
+        for (int q = a.syn_ptr[i]; q < a.syn_ptr[i + 1]; ++q) {
+          const size_t o = (size_t)a.syn_off[q] + (size_t)b * a.syn_rs[q];
+          ((T*)a.g_syn_lin)[o] = gl;
+          ((T*)a.g_syn_const)[o] = gc;
+        }
+      }
       lam[0] = T(0);
       node_adjoint<T>(sm, j, x, lam, sm.pv + (size_t)r * np,
                       sm.gacc + (size_t)r * gslots, dt, lrs, xnew, lv);

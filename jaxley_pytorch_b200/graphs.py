@@ -18,7 +18,8 @@ from .sim import Simulation
 
 
 class GraphedIteration:
-    """`loss_fn(recordings) -> scalar` on `sim.run(pscale=params)`, its gradient with
+    """`loss_fn(recordings) -> scalar` on `sim.run(pscale=params)` (or on `run(params)`
+    when given, e.g. a network's simulation with `params` as its synapse weights), its gradient with
     respect to `params` (a leaf tensor on the device) and an optional optimizer step
     over `[params]` (it must be capturable, e.g. `torch.optim.Adam(..., capturable=True)`).
 
@@ -29,11 +30,13 @@ class GraphedIteration:
 
     def __init__(self, sim: Simulation, loss_fn: Callable[[torch.Tensor], torch.Tensor],
                  params: torch.Tensor, n_steps: Optional[int] = None,
-                 optimizer: Optional[torch.optim.Optimizer] = None, warmup: int = 2):
+                 optimizer: Optional[torch.optim.Optimizer] = None, warmup: int = 2,
+                 run: Optional[Callable[[torch.Tensor], torch.Tensor]] = None):
         if not params.is_leaf or not params.requires_grad:
             raise ValueError("params must be a leaf tensor that requires grad")
         self.sim, self.loss_fn, self.params = sim, loss_fn, params
         self.n_steps, self.optimizer = n_steps, optimizer
+        self.run_fn = run
         dev = sim.model.device
         side = torch.cuda.Stream(dev)
         side.wait_stream(torch.cuda.current_stream(dev))
@@ -49,7 +52,10 @@ class GraphedIteration:
         self.launches_per_replay = sim.model.launches - n0
 
     def _body(self):
-        rec = self.sim.run(n_steps=self.n_steps, pscale=self.params)
+        if self.run_fn is not None:
+            rec = self.run_fn(self.params)
+        else:
+            rec = self.sim.run(n_steps=self.n_steps, pscale=self.params)
         loss = self.loss_fn(rec)
         (g,) = torch.autograd.grad(loss, self.params)
         if self.optimizer is not None:

@@ -1,0 +1,340 @@
+"""Networks: the synapse step fused into the simulation loop, with its adjoint.
+
+Every step of `jx.integrate` on a network (`modules/network.py:350-478`) runs the
+synapse pass of every synapse type on the voltages before the step (kinetic states
+advance), adds each target's summed slope and offset to its linear and constant
+terms, and then takes the cell step. Here a step is one `jxb_synapse_forward` launch
+per synapse type, reading the voltages straight from the simulation's state vector
+(the presynaptic and postsynaptic indices are state-slot offsets), and one
+one-step `jxb_sim_forward` launch that adds the synaptic terms by target
+(`JxbSimArgs.syn_ptr`). The whole loop is graph-capturable.
+
+The adjoint runs segments of `checkpoint` steps in reverse. The forward stores the
+cell state before every step and the kinetic states every `checkpoint` steps; a
+segment first recomputes its kinetic states and synaptic terms, then, step by step
+in reverse: the one-step cell adjoint (`jxb_sim_backward`, which also returns the
+gradient of the step's synaptic slopes and offsets), the synapse adjoint of every
+type (`jxb_synapse_backward`: voltage gradient in the state layout, kinetic-state
+gradient, parameter gradients summed over the batch), and the voltage gradient added
+to the state adjoint.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from typing import Dict, List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _lib
+from .kernels.synapse_step import KINETIC, _transposed_index
+from .problem import Problem, SynapseType
+from .sim import Simulation
+
+DIFF = 1e-3  # finite-difference step of the synaptic current slope (modules/network.py:434-478)
+
+
+class _SynType:
+    """Device plan of one synapse type in the regular layout."""
+
+    def __init__(self, syn: SynapseType, low, area: np.ndarray, B: int, dtype, device, dt: float):
+        self.model = int(syn.model)
+        self.k = int(syn.k)
+        self.E = len(syn.pre)
+        self.T = self.E // self.k
+        soff = np.asarray(low.soff, dtype=np.int64)
+        n2i = np.asarray(low.node2int, dtype=np.int64)
+        pre_slot = soff[n2i[np.asarray(syn.pre, dtype=np.int64)]].astype(np.int32)
+        tgt_slot = soff[n2i[np.asarray(syn.targets, dtype=np.int64)]].astype(np.int32)
+        nodes, inv = _transposed_index(pre_slot)
+        i32 = lambda x: torch.as_tensor(np.ascontiguousarray(x), dtype=torch.int32, device=device)  # noqa: E731
+        self.pre = i32(pre_slot)
+        self.targets = i32(tgt_slot)
+        self.pre_nodes = i32(nodes)
+        self.inv = i32(inv)
+        self.target_int = n2i[np.asarray(syn.targets, dtype=np.int64)]  # internal node of every target
+        self.params = [torch.as_tensor(np.asarray(p, dtype=np.float64), dtype=dtype, device=device).contiguous()
+                       for p in syn.params]
+        self.param_names = list(syn.param_names)
+        self.area = torch.as_tensor(np.asarray(area, dtype=np.float64)[np.asarray(syn.post)], dtype=dtype,
+                                    device=device).contiguous()
+        self.scalars = torch.tensor([dt, DIFF], dtype=dtype, device=device)
+        self.kinetic = self.model == KINETIC
+        if self.kinetic:
+            s0 = np.array(np.broadcast_to(np.asarray(syn.state, dtype=np.float64), (B, self.E)))
+            self.s0 = torch.as_tensor(s0, dtype=dtype, device=device)
+        self.dtype = dtype
+
+    def args(self, state: torch.Tensor, n_slots: int, B: int, params: Sequence[torch.Tensor]):
+        a = _lib.JxbSynArgs()
+        a.dtype = _lib.F32 if self.dtype == torch.float32 else _lib.F64
+        a.model = self.model
+        a.batch, a.n_nodes = B, n_slots
+        a.n_syn = self.E
+        a.k = self.k
+        a.targets_are_nodes = 0
+        a.v = state.data_ptr()
+        a.pre = self.pre.data_ptr()
+        a.targets = self.targets.data_ptr()
+        for q, p in enumerate(params):
+            a.p[q] = p.data_ptr()
+        a.area = self.area.data_ptr()
+        a.scalars = self.scalars.data_ptr()
+        a.inv_width = self.inv.shape[1]
+        a.n_pre_nodes = self.pre_nodes.shape[0]
+        a.inv = self.inv.data_ptr()
+        a.pre_nodes = self.pre_nodes.data_ptr()
+        return a
+
+
+def _stream():
+    return C.c_void_p(torch.cuda.current_stream().cuda_stream)
+
+
+class NetworkSimulation:
+    """`jx.integrate` for a `Problem` with synapses (regular layout) on the CUDA
+    kernels. `run(pscale, syn_params)` returns the recordings `(B, n_rec, T + 1)`,
+    differentiable with respect to the cell parameter scales and the synapse
+    parameters (lists of `(E,)` tensors per synapse type, in the reference order)."""
+
+    def __init__(self, problem: Problem, dtype=torch.float32, device="cuda", checkpoint: int = 50,
+                 threads: int = 256, max_block_nodes: int = 256, rows_per_item: int = 1):
+        if not problem.synapses:
+            raise ValueError("the problem has no synapses (use Simulation)")
+        self.problem = problem
+        self.sim = Simulation(problem, dtype=dtype, device=device, threads=threads, segment=1,
+                              checkpoint=1, keep_currents=False, max_block_nodes=max_block_nodes,
+                              rows_per_item=rows_per_item)
+        self.low = low = self.sim.low
+        self.model = self.sim.model
+        self.dtype, self.device = dtype, torch.device(device)
+        self.B = low.batch
+        self.checkpoint = int(checkpoint)
+        area = np.asarray(problem.params["area"], dtype=np.float64)
+        if area.ndim == 2:
+            area = area[0]
+        self.types = [_SynType(s, low, area, self.B, dtype, device, low.dt) for s in problem.synapses]
+        # per-target CSR over internal nodes into the concatenated per-type outputs
+        offs, entries = 0, []
+        self.region = []
+        for ty in self.types:
+            self.region.append((offs, self.B * ty.T))
+            for t in range(ty.T):
+                entries.append((int(ty.target_int[t]), offs + t, ty.T))
+            offs += self.B * ty.T
+        self.syn_size = offs
+        entries.sort(key=lambda e: e[0])
+        n = low.n_nodes
+        ptr = np.zeros(n + 1, dtype=np.int32)
+        ptr[1:] = np.cumsum(np.bincount([e[0] for e in entries], minlength=n))
+        i32 = lambda x: torch.as_tensor(np.asarray(x, dtype=np.int32), device=device).contiguous()  # noqa: E731
+        self.syn_ptr = i32(ptr)
+        self.syn_off = i32([e[1] for e in entries] or [0])
+        self.syn_rs = i32([e[2] for e in entries] or [1])
+
+    def _zeros(self, *shape, dtype=None):
+        return torch.zeros(shape, dtype=dtype or self.dtype, device=self.device)
+
+    def _set_syn(self, a, lin, cst):
+        a.syn_lin = lin.data_ptr()
+        a.syn_const = cst.data_ptr()
+        a.syn_ptr = self.syn_ptr.data_ptr()
+        a.syn_off = self.syn_off.data_ptr()
+        a.syn_rs = self.syn_rs.data_ptr()
+
+    def _syn_forward(self, ty: _SynType, k: int, state, s, s_new, lin, cst, params):
+        a = ty.args(state, self.low.n_slots, self.B, params)
+        a.s = s.data_ptr() if ty.kinetic else None
+        a.s_new = s_new.data_ptr() if ty.kinetic else None
+        a.store_current = 0
+        off, size = self.region[k]
+        a.lin = lin.data_ptr() + off * lin.element_size()
+        a.cst = cst.data_ptr() + off * cst.element_size()
+        _lib.check(_lib.load().jxb_synapse_forward(C.byref(a), _stream()), "jxb_synapse_forward")
+
+    def forward_raw(self, pscale: torch.Tensor, syn_params: List[List[torch.Tensor]], T: int,
+                    keep: bool = False):
+        """Runs T steps; with `keep` also stores what the adjoint needs. Returns
+        `(rec (T + 1, B, n_rec), saved)`."""
+        m, low, B = self.model, self.low, self.B
+        state = m.initial_state()
+        rec = self._zeros(T + 1, B, low.n_rec)
+        m.launch_forward(m.args(state, 0, 0, rec, mode=1, pscale=pscale))
+        lin = self._zeros(self.syn_size)
+        cst = self._zeros(self.syn_size)
+        K = self.checkpoint
+        s_cur = [ty.s0.clone() if ty.kinetic else None for ty in self.types]
+        s_nxt = [torch.empty_like(s) if s is not None else None for s in s_cur]
+        saved = None
+        if keep:
+            saved = {"states": self._zeros(T, B, low.n_slots),
+                     "s_ckpt": [self._zeros((T + K - 1) // K, B, ty.E) if ty.kinetic else None
+                                for ty in self.types]}
+        for t in range(T):
+            if keep and t % K == 0:
+                for q, ty in enumerate(self.types):
+                    if ty.kinetic:
+                        saved["s_ckpt"][q][t // K].copy_(s_cur[q])
+            for q, ty in enumerate(self.types):
+                self._syn_forward(ty, q, state, s_cur[q], s_nxt[q], lin, cst, syn_params[q])
+            a = m.args(state, 1, t, rec, pscale=pscale, ckpt=saved["states"] if keep else None,
+                       ckpt_every=1 if keep else 0)
+            self._set_syn(a, lin, cst)
+            m.launch_forward(a)
+            s_cur, s_nxt = s_nxt, s_cur
+        return rec, saved
+
+    def backward_raw(self, pscale, syn_params, T: int, saved, rec_grad: torch.Tensor):
+        """Returns `(d loss / d pscale (B, n_cols) float64, [per type: (n_params, E)])`."""
+        m, low, B = self.model, self.low, self.B
+        K = self.checkpoint
+        adj = self._zeros(B, low.n_slots)
+        pgrad = self._zeros(B, low.n_cols, dtype=torch.float64)
+        traj = self._zeros(1, B, low.n_slots)
+        piv = self._zeros(1, B, low.n_nodes)
+        LC_lin = self._zeros(K, self.syn_size)
+        LC_cst = self._zeros(K, self.syn_size)
+        g_lin = self._zeros(self.syn_size)
+        g_cst = self._zeros(self.syn_size)
+        s_seg = [self._zeros(K + 1, B, ty.E) if ty.kinetic else None for ty in self.types]
+        g_s = [self._zeros(B, ty.E) if ty.kinetic else None for ty in self.types]
+        g_s2 = [self._zeros(B, ty.E) if ty.kinetic else None for ty in self.types]
+        g_v = self._zeros(B, low.n_slots)
+        g_pre = [self._zeros(ty.E, B) for ty in self.types]
+        g_post = [self._zeros(B, ty.T) for ty in self.types]
+        n_par = [len(p) for p in syn_params]
+        g_par = [self._zeros(n_par[q], ty.E) for q, ty in enumerate(self.types)]
+        g_par_acc = [self._zeros(n_par[q], ty.E) for q, ty in enumerate(self.types)]
+        states = saved["states"]
+        rec_grad = rec_grad.contiguous()
+        for seg in range((T + K - 1) // K - 1, -1, -1):
+            t0 = seg * K
+            k = min(K, T - t0)
+            # recompute the segment's kinetic states and synaptic terms
+            for q, ty in enumerate(self.types):
+                if ty.kinetic:
+                    s_seg[q][0].copy_(saved["s_ckpt"][q][seg])
+            for i in range(k):
+                for q, ty in enumerate(self.types):
+                    self._syn_forward(ty, q, states[t0 + i], s_seg[q][i] if ty.kinetic else None,
+                                      s_seg[q][i + 1] if ty.kinetic else None, LC_lin[i], LC_cst[i],
+                                      syn_params[q])
+            for i in range(k - 1, -1, -1):
+                t = t0 + i
+                a = m.args(states[t], 1, t, None, pscale=pscale, traj=traj, adj=adj, rec_grad=rec_grad,
+                           pgrad=pgrad)
+                a.ckpt = states[t].data_ptr()
+                a.traj_piv = piv.data_ptr()
+                self._set_syn(a, LC_lin[i], LC_cst[i])
+                a.g_syn_lin = g_lin.data_ptr()
+                a.g_syn_const = g_cst.data_ptr()
+                m.launch_backward(a)
+                for q, ty in enumerate(self.types):
+                    b = ty.args(states[t], low.n_slots, B, syn_params[q])
+                    b.s = s_seg[q][i].data_ptr() if ty.kinetic else None
+                    b.g_s_new = g_s[q].data_ptr() if ty.kinetic else None
+                    b.g_current = None
+                    off, size = self.region[q]
+                    b.g_lin = g_lin.data_ptr() + off * g_lin.element_size()
+                    b.g_const = g_cst.data_ptr() + off * g_cst.element_size()
+                    b.g_s = g_s2[q].data_ptr() if ty.kinetic else None
+                    b.g_v = g_v.data_ptr()
+                    b.need = (1 << n_par[q]) - 1
+                    b.g_params = g_par[q].data_ptr()
+                    b.g_pre = g_pre[q].data_ptr()
+                    b.g_post = g_post[q].data_ptr()
+                    _lib.check(_lib.load().jxb_synapse_backward(C.byref(b), _stream()), "jxb_synapse_backward")
+                    adj.add_(g_v)
+                    g_par_acc[q].add_(g_par[q])
+                    if ty.kinetic:
+                        g_s[q], g_s2[q] = g_s2[q], g_s[q]
+        return pgrad, g_par_acc
+
+    def run(self, pscale: Optional[torch.Tensor] = None, syn_params: Optional[List[List[torch.Tensor]]] = None,
+            n_steps: Optional[int] = None):
+        """Recordings `(B, n_rec, T + 1)`; differentiable with respect to `pscale` and
+        the synapse parameter tensors."""
+        T = int(self.low.n_steps if n_steps is None else n_steps)
+        if pscale is None:
+            pscale = self.model.pscale
+        if syn_params is None:
+            syn_params = [ty.params for ty in self.types]
+        flat = [p for ps in syn_params for p in ps]
+        if torch.is_grad_enabled() and (pscale.requires_grad or any(p.requires_grad for p in flat)):
+            return _NetFn.apply(self, T, [len(ps) for ps in syn_params], pscale, *flat)
+        rec, _ = self.forward_raw(pscale.detach().contiguous(), [[p.detach() for p in ps] for ps in syn_params], T)
+        return rec.permute(1, 2, 0)
+
+
+class _NetFn(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, net: NetworkSimulation, T: int, counts, pscale, *flat):
+        ps = pscale.detach().to(net.dtype).contiguous()
+        params, q = [], 0
+        for c in counts:
+            params.append([p.detach().to(net.dtype).contiguous() for p in flat[q:q + c]])
+            q += c
+        rec, saved = net.forward_raw(ps, params, T, keep=True)
+        ctx.net, ctx.T, ctx.counts, ctx.saved_data = net, T, counts, saved
+        ctx.params = params
+        ctx.save_for_backward(ps)
+        ctx.dtypes = (pscale.dtype, [p.dtype for p in flat])
+        return rec.permute(1, 2, 0)
+
+    @staticmethod
+    def backward(ctx, grad_out):
+        (ps,) = ctx.saved_tensors
+        net = ctx.net
+        rec_grad = grad_out.to(net.dtype).permute(2, 0, 1).contiguous()
+        pgrad, g_par = net.backward_raw(ps, ctx.params, ctx.T, ctx.saved_data, rec_grad)
+        out = [None, None, None, pgrad.to(ctx.dtypes[0])]
+        dts = ctx.dtypes[1]
+        q = 0
+        for t, c in enumerate(ctx.counts):
+            for i in range(c):
+                out.append(g_par[t][i].to(dts[q]))
+                q += 1
+        return tuple(out)
+
+
+def config_network(n_cells: int = 2048, ncomp: int = 4, k: int = 64, batch: int = 32, n_steps: int = 2000,
+                   seed: int = 0, rate_hz: float = 20.0, amp: float = 0.2, dt: float = 0.025) -> Problem:
+    """Fixed in-degree network: `n_cells` cells of one branch x `ncomp` compartments
+    with HH, `k` KineticSynapse and `k` SigmoidRateSynapse inputs on compartment 0 of
+    every cell (presynaptic cells uniform without replacement, excluding the cell,
+    ordered by postsynaptic cell; gS ~ U[0, 1e-3] uS), `batch` rows of Poisson input
+    (rate_hz per cell, one-step pulses of `amp` nA on compartment 0)."""
+    from . import synth
+
+    rng = np.random.default_rng(seed)
+    cells = [synth.morphology([-1], [ncomp], [np.full(ncomp, 1.0)], [np.full(ncomp, 10.0)]) for _ in range(n_cells)]
+    chans = [[("HH", np.arange(ncomp), "HH", {})] for _ in range(n_cells)]
+    t_max = n_steps * dt
+    L = int(t_max // dt) + 2
+    prob = synth.assemble(cells, chans, batch=1, dt=dt, n_steps=n_steps, v0=-65.0,
+                          recordings=[("v", c, (0, 0)) for c in range(n_cells)])
+    offs = np.cumsum([0] + [c["n"] for c in cells])
+    soma = offs[:-1]
+    # Poisson input: (batch, n_cells, L) one-step pulses
+    spikes = rng.random((batch, n_cells, L)) < rate_hz * dt * 1e-3
+    prob.stim_inds = soma.astype(np.int64)
+    prob.stim = (spikes * amp).astype(np.float64)
+    prob.batch = batch
+    syns = []
+    for model, name, pnames, pdef in [
+        # defaults of synapses/kinetic.py:27-35 and synapses/sigmoid_rate.py:26-31
+        (0, "KineticSynapse", ["gS", "e_syn", "alpha", "beta", "v_th", "delta"], [None, 0.0, 1.0, 0.2, -20.0, 2.0]),
+        (1, "SigmoidRateSynapse", ["gS", "x_offset", "slope"], [None, -60.0, 0.25]),
+    ]:
+        pre = np.empty(n_cells * k, dtype=np.int64)
+        for c in range(n_cells):
+            choice = rng.choice(n_cells - 1, size=k, replace=False)
+            choice[choice >= c] += 1
+            pre[c * k:(c + 1) * k] = soma[np.sort(choice)]
+        post = np.repeat(soma, k)
+        params = [rng.uniform(0.0, 1e-3, size=n_cells * k)] + [np.full(n_cells * k, float(v)) for v in pdef[1:]]
+        syns.append(SynapseType(model=model, name=name, pre=pre, post=post, k=k, targets=soma.copy(),
+                                params=params, param_names=[f"{name}_{p}" for p in pnames],
+                                state=np.zeros((1, n_cells * k)) if model == 0 else None))
+    prob.synapses = syns
+    return prob
