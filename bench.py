@@ -147,6 +147,17 @@ def traffic_from_profiles(kernel: str):
     return None
 
 
+def max_over_ranks(x: float, world: int, device) -> float:
+    """The largest of every rank's `x` (the timing of a multi-GPU run is its slowest rank)."""
+    if world == 1:
+        return x
+    import torch
+
+    t = torch.tensor([x], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
 def workload(rank: int, batch: int, tsteps: int):
     from jaxley_pytorch_b200 import synth
 
@@ -203,13 +214,6 @@ def run_ours(args, rank, world, device):
         if world > 1:
             torch.distributed.barrier()
 
-    def max_over_ranks(x: float) -> float:
-        if world == 1:
-            return x
-        t = torch.tensor([x], device=device, dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        return float(t.item())
-
     ps = ps0.clone().requires_grad_(True)
     for _ in range(args.warmup):
         train_step(ps)
@@ -230,7 +234,7 @@ def run_ours(args, rank, world, device):
         torch.cuda.synchronize()
     barrier()
     launches = sim.model.launches - launches0
-    ms = max_over_ranks(e0.elapsed_time(e1))
+    ms = max_over_ranks(e0.elapsed_time(e1), world, device)
     bwd = [(a.elapsed_time(b), k) for a, b, k in sim.model.events]
     sim.model.timed_kind = None
     # Forward launch durations (one extra measured pass, outside the timed region).
@@ -260,7 +264,7 @@ def run_ours(args, rank, world, device):
         g_host.copy_(g, non_blocking=True)
     f1.record()
     torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(f0.elapsed_time(f1))
+    e2e_ms = max_over_ranks(f0.elapsed_time(f1), world, device)
     e2e = {"value": comp_steps / (e2e_ms / 1e3), "unit": UNIT,
            "h2d_bytes_per_step": int(ps_host.numel() * ps_host.element_size()),
            "d2h_bytes_per_step": int(loss_host.element_size() + g_host.numel() * g_host.element_size())}
@@ -444,6 +448,7 @@ def run_network(args, device):
         return ((rec - target) ** 2).mean()
 
     w = torch.cat([ty.params[0] for ty in net.types]).clone().requires_grad_(True)
+    syn0 = net.syn_launches
     it = GraphedIteration(net, loss_fn, w, optimizer=torch.optim.Adam([w], lr=1e-6, capturable=True),
                           warmup=1, run=run)
     it.replay()
@@ -461,7 +466,8 @@ def run_network(args, device):
             "synapses": int(sum(sizes)), "batch": 32, "time_steps": T,
             "value": n_comp * 32 * T / (ms / 1e3), "unit": UNIT,
             "synapse_steps_per_s": sum(sizes) * 32 * T / (ms / 1e3),
-            "ms_per_training_step": ms, "graph_launches": it.launches_per_replay,
+            "ms_per_training_step": ms, "graph_sim_launches": it.launches_per_replay,
+            "graph_synapse_launches": (net.syn_launches - syn0) // 2,  # warm-up + capture
             "loss": float(it.loss)}
 
 

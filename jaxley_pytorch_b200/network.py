@@ -131,6 +131,7 @@ class NetworkSimulation:
         self.syn_ptr = i32(ptr)
         self.syn_off = i32([e[1] for e in entries] or [0])
         self.syn_rs = i32([e[2] for e in entries] or [1])
+        self.syn_launches = 0  # synapse kernel launches issued (forward and adjoint)
 
     def _zeros(self, *shape, dtype=None):
         return torch.zeros(shape, dtype=dtype or self.dtype, device=self.device)
@@ -151,6 +152,7 @@ class NetworkSimulation:
         a.lin = lin.data_ptr() + off * lin.element_size()
         a.cst = cst.data_ptr() + off * cst.element_size()
         _lib.check(_lib.load().jxb_synapse_forward(C.byref(a), _stream()), "jxb_synapse_forward")
+        self.syn_launches += 1
 
     def forward_raw(self, pscale: torch.Tensor, syn_params: List[List[torch.Tensor]], T: int,
                     keep: bool = False):
@@ -244,6 +246,7 @@ class NetworkSimulation:
                     b.g_pre = g_pre[q].data_ptr()
                     b.g_post = g_post[q].data_ptr()
                     _lib.check(_lib.load().jxb_synapse_backward(C.byref(b), _stream()), "jxb_synapse_backward")
+                    self.syn_launches += 1
                     adj.add_(g_v)
                     g_par_acc[q].add_(g_par[q])
                     if ty.kinetic:
