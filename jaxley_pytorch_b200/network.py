@@ -61,8 +61,9 @@ class _SynType:
         self.scalars = torch.tensor([dt, DIFF], dtype=dtype, device=device)
         self.kinetic = self.model == KINETIC
         if self.kinetic:
-            s0 = np.array(np.broadcast_to(np.asarray(syn.state, dtype=np.float64), (B, self.E)))
-            self.s0 = torch.as_tensor(s0, dtype=dtype, device=device)
+            # row-major (B, E): np.array of a broadcast view would keep its axis order
+            s0 = np.broadcast_to(np.asarray(syn.state, dtype=np.float64), (B, self.E)).copy(order="C")
+            self.s0 = torch.as_tensor(s0, dtype=dtype, device=device).contiguous()
         self.dtype = dtype
 
     def args(self, state: torch.Tensor, n_slots: int, B: int, params: Sequence[torch.Tensor]):
@@ -73,11 +74,11 @@ class _SynType:
         a.n_syn = self.E
         a.k = self.k
         a.targets_are_nodes = 0
-        a.v = state.data_ptr()
+        a.v = _ptr(state, self.dtype, B * n_slots, "state")
         a.pre = self.pre.data_ptr()
         a.targets = self.targets.data_ptr()
         for q, p in enumerate(params):
-            a.p[q] = p.data_ptr()
+            a.p[q] = _ptr(p, self.dtype, self.E, self.param_names[q] if q < len(self.param_names) else "param")
         a.area = self.area.data_ptr()
         a.scalars = self.scalars.data_ptr()
         a.inv_width = self.inv.shape[1]
@@ -85,6 +86,15 @@ class _SynType:
         a.inv = self.inv.data_ptr()
         a.pre_nodes = self.pre_nodes.data_ptr()
         return a
+
+
+def _ptr(t: torch.Tensor, dtype, numel: int, what: str) -> int:
+    """Device address of a row-major tensor the kernels index flat; anything else
+    (another dtype, a transposed or strided view, a wrong size) is refused."""
+    if t.dtype != dtype or not t.is_contiguous() or t.numel() != numel:
+        raise ValueError(f"{what}: expected a contiguous {dtype} tensor of {numel} elements, got "
+                         f"{t.dtype} {tuple(t.shape)} with strides {t.stride()}")
+    return t.data_ptr()
 
 
 def _stream():
@@ -145,8 +155,8 @@ class NetworkSimulation:
 
     def _syn_forward(self, ty: _SynType, k: int, state, s, s_new, lin, cst, params):
         a = ty.args(state, self.low.n_slots, self.B, params)
-        a.s = s.data_ptr() if ty.kinetic else None
-        a.s_new = s_new.data_ptr() if ty.kinetic else None
+        a.s = _ptr(s, self.dtype, self.B * ty.E, "s") if ty.kinetic else None
+        a.s_new = _ptr(s_new, self.dtype, self.B * ty.E, "s_new") if ty.kinetic else None
         a.store_current = 0
         off, size = self.region[k]
         a.lin = lin.data_ptr() + off * lin.element_size()

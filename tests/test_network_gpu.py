@@ -119,3 +119,22 @@ def test_graphed_adam_training_step_matches_eager(cuda_device):
         it.replay()
     torch.cuda.synchronize()
     assert (wg.detach() - we.detach()).abs().max().item() <= 1e-12
+
+
+@pytest.mark.parametrize("K", [1, 7])
+def test_gradients_independent_of_checkpoint_interval(cuda_device, K):
+    """The adjoint recomputes each segment's kinetic synapse states from the stored
+    ones; every checkpoint interval must give the gradients of a single segment."""
+    prob = _small(n_steps=40, batch=2)
+    w = torch.as_tensor(np.random.default_rng(3).normal(size=(2, len(prob.recordings), 41)), device=cuda_device)
+
+    def grads(k):
+        net = NetworkSimulation(prob, dtype=torch.float64, device=cuda_device, checkpoint=k, max_block_nodes=16)
+        params = [[p.clone().requires_grad_(True) for p in ty.params] for ty in net.types]
+        ps = net.model.pscale.clone().requires_grad_(True)
+        loss = (net.run(ps, params) * w).sum()
+        return [g.cpu().numpy() for g in torch.autograd.grad(loss, [ps] + [p for ty in params for p in ty])]
+
+    ref, got = grads(40), grads(K)
+    for a, b in zip(ref, got):
+        assert np.abs(a - b).max() <= 1e-10 * max(1.0, np.abs(a).max()), np.abs(a - b).max()
