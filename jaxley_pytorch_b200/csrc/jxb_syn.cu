@@ -2,14 +2,17 @@
 // layout: E = T * k synapses ordered by postsynaptic target, k per target
 // (jaxley-pytorch kernels/synapse_step.py, modules/network.py:381-478).
 //
-// forward:  one warp per (batch row, target); lanes stride over the target's k
-//           synapses (coalesced state/parameter reads, gathered presynaptic
-//           voltages), the slope and offset sums over k are warp reductions.
+// forward:  one warp per target looping over the batch rows; lanes stride over the
+//           target's k synapses (coalesced state reads, gathered presynaptic
+//           voltages, parameters reused from L1 across the rows), the slope and
+//           offset sums over k are warp reductions.
 // backward: one CTA per target, warps over batch rows, lanes over synapses. The
 //           parameter gradients (summed over the batch) are reduced across warps in
-//           shared memory in a fixed order; the presynaptic voltage gradients go to
-//           an (E, batch) buffer that a second kernel sums per presynaptic node
-//           through the transposed index. No atomics, deterministic.
+//           shared memory in a fixed order; the presynaptic voltage gradients of the
+//           CTA's synapses are staged in shared memory and written to an (E, batch)
+//           buffer row by row (coalesced), which a second kernel sums per
+//           presynaptic node through the transposed index. No atomics, deterministic.
+// float: fast reciprocal / division / exp (jxb_math.cuh); float64 stays exact.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -26,7 +29,8 @@ namespace {
 
 using namespace jxb;
 
-template <typename T> __device__ __forceinline__ T sigm(T x) { return T(1) / (T(1) + ex(-x)); }
+template <typename T> __device__ __forceinline__ T qdiv(T x, T y) { return jxb::fdiv(x, y); }
+template <typename T> __device__ __forceinline__ T sigm(T x) { return jxb::rcp(T(1) + ex(-x)); }
 
 template <typename T>
 __device__ __forceinline__ T warp_sum(T v) {
@@ -42,57 +46,58 @@ struct SynP {
 
 template <typename T>
 __global__ void syn_forward_kernel(JxbSynArgs a, SynP<T> P) {
-  const int gw = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const int tgt = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const int lane = threadIdx.x & 31;
   const int nt = a.n_syn / a.k;
-  if (gw >= nt * a.batch) return;
-  const int tgt = gw % nt;
-  const int64_t b = gw / nt;
-  const T* v = (const T*)a.v + b * a.n_nodes;
+  if (tgt >= nt) return;
   const T* sc = (const T*)a.scalars;
   const T dt = sc[0], diff = sc[1];
   const int node = a.targets_are_nodes ? tgt : a.targets[tgt];
-  const T vp = v[node];
   const T* area = (const T*)a.area;
-  T lin = T(0), cst = T(0);
-  for (int kk = lane; kk < a.k; kk += 32) {
-    const int e = tgt * a.k + kk;
-    const T vpre = v[a.pre[e]];
-    const T gs = P.p[0][e];
-    T i0, i1;
-    if (a.model == 0) {  // synapses/kinetic.py:37-63
-      const T e_syn = P.p[1][e], alpha = P.p[2][e], beta = P.p[3][e], v_th = P.p[4][e],
-              delta = P.p[5][e];
-      const T s = ((const T*)a.s)[b * a.n_syn + e];
-      const T tr = sigm((vpre - v_th) / delta);
-      const T aa = alpha * tr;
-      const T rate = aa + beta;
-      const T s_inf = aa / rate;
-      const T s_new = s_inf + (s - s_inf) * ex(-dt * rate);
-      ((T*)a.s_new)[b * a.n_syn + e] = s_new;
-      i0 = gs * s_new * (vp - e_syn);
-      i1 = gs * s_new * ((vp + diff) - e_syn);
-    } else {  // synapses/sigmoid_rate.py:43-50
-      const T x_off = P.p[1][e], slope = P.p[2][e];
-      i0 = -gs * sigm((vpre - x_off) * slope);
-      i1 = -gs * sigm(((vpre + diff) - x_off) * slope);
+  for (int64_t b = 0; b < a.batch; ++b) {
+    const T* v = (const T*)a.v + b * a.n_nodes;
+    const T vp = v[node];
+    T lin = T(0), cst = T(0);
+    for (int kk = lane; kk < a.k; kk += 32) {
+      const int e = tgt * a.k + kk;
+      const T vpre = v[a.pre[e]];
+      const T gs = P.p[0][e];
+      T i0, i1;
+      if (a.model == 0) {  // synapses/kinetic.py:37-63
+        const T e_syn = P.p[1][e], alpha = P.p[2][e], beta = P.p[3][e], v_th = P.p[4][e],
+                delta = P.p[5][e];
+        const T s = ((const T*)a.s)[b * a.n_syn + e];
+        const T tr = sigm(qdiv<T>(vpre - v_th, delta));
+        const T aa = alpha * tr;
+        const T rate = aa + beta;
+        const T s_inf = qdiv<T>(aa, rate);
+        const T s_new = s_inf + (s - s_inf) * ex(-dt * rate);
+        ((T*)a.s_new)[b * a.n_syn + e] = s_new;
+        i0 = gs * s_new * (vp - e_syn);
+        i1 = gs * s_new * ((vp + diff) - e_syn);
+      } else {  // synapses/sigmoid_rate.py:43-50
+        const T x_off = P.p[1][e], slope = P.p[2][e];
+        i0 = -gs * sigm((vpre - x_off) * slope);
+        i1 = -gs * sigm(((vpre + diff) - x_off) * slope);
+      }
+      const T d0 = qdiv<T>(i0, area[e]) * T(100000.0);
+      const T d1 = qdiv<T>(i1, area[e]) * T(100000.0);
+      const T vt = qdiv<T>(d1 - d0, diff);
+      lin += vt;
+      cst += d0 - vt * vp;
+      if (a.store_current) ((T*)a.current)[b * a.n_syn + e] = i0;
     }
-    const T d0 = i0 / area[e] * T(100000.0);
-    const T d1 = i1 / area[e] * T(100000.0);
-    const T vt = (d1 - d0) / diff;
-    lin += vt;
-    cst += d0 - vt * vp;
-    if (a.store_current) ((T*)a.current)[b * a.n_syn + e] = i0;
-  }
-  lin = warp_sum(lin);
-  cst = warp_sum(cst);
-  if (lane == 0) {
-    ((T*)a.lin)[b * nt + tgt] = lin;
-    ((T*)a.cst)[b * nt + tgt] = cst;
+    lin = warp_sum(lin);
+    cst = warp_sum(cst);
+    if (lane == 0) {
+      ((T*)a.lin)[b * nt + tgt] = lin;
+      ((T*)a.cst)[b * nt + tgt] = cst;
+    }
   }
 }
 
 constexpr int kBwdWarps = 4;
+constexpr int kStageBytes = 64 * 1024;  // largest staged (k, batch) tile of presynaptic gradients
 
 template <typename T>
 __global__ void syn_backward_kernel(JxbSynArgs a, SynP<T> P) {
@@ -110,6 +115,8 @@ __global__ void syn_backward_kernel(JxbSynArgs a, SynP<T> P) {
   const int np = a.model == 0 ? 6 : 3;
   T* g_pre = (T*)a.g_pre;
   T* myred = red + (size_t)warp * 6 * a.k;
+  // the CTA's presynaptic gradients, (k, batch), staged for coalesced stores
+  T* stile = a.batch * a.k * (int)sizeof(T) <= kStageBytes ? red + (size_t)kBwdWarps * 6 * a.k : nullptr;
   for (int q = lane; q < 6 * a.k; q += 32) myred[q] = T(0);
   __syncwarp();
   for (int64_t b = warp; b < a.batch; b += kBwdWarps) {
@@ -133,11 +140,11 @@ __global__ void syn_backward_kernel(JxbSynArgs a, SynP<T> P) {
         alpha = P.p[2][e];
         delta = P.p[5][e];
         s = ((const T*)a.s)[b * a.n_syn + e];
-        x = (vpre - v_th) / delta;
+        x = qdiv<T>(vpre - v_th, delta);
         tr = sigm(x);
         const T aa = alpha * tr;
         rate = aa + beta;
-        s_inf = aa / rate;
+        s_inf = qdiv<T>(aa, rate);
         decay = ex(-dt * rate);
         s_new = s_inf + (s - s_inf) * decay;
         w0 = vp - e_syn;
@@ -154,16 +161,16 @@ __global__ void syn_backward_kernel(JxbSynArgs a, SynP<T> P) {
         i0 = -gs * sig0;
         i1 = -gs * sig1;
       }
-      const T d0 = i0 / ar * T(100000.0);
-      const T d1 = i1 / ar * T(100000.0);
-      const T vt = (d1 - d0) / diff;
+      const T d0 = qdiv<T>(i0, ar) * T(100000.0);
+      const T d1 = qdiv<T>(i1, ar) * T(100000.0);
+      const T vt = qdiv<T>(d1 - d0, diff);
       // Backward (kernels/synapse_step.py:256-305).
       const T g_vt = glin - gconst * vp;
       T g_vp = -gconst * vt;
-      const T g_d1 = g_vt / diff;
+      const T g_d1 = qdiv<T>(g_vt, diff);
       const T g_d0 = gconst - g_d1;
-      T g_i0 = g_d0 * T(100000.0) / ar;
-      const T g_i1 = g_d1 * T(100000.0) / ar;
+      T g_i0 = qdiv<T>(g_d0 * T(100000.0), ar);
+      const T g_i1 = qdiv<T>(g_d1 * T(100000.0), ar);
       if (a.g_current) g_i0 += ((const T*)a.g_current)[b * a.n_syn + e];
       T g_vpre;
       if (a.model == 0) {
@@ -172,10 +179,10 @@ __global__ void syn_backward_kernel(JxbSynArgs a, SynP<T> P) {
         if (a.g_s_new) g_sn += ((const T*)a.g_s_new)[b * a.n_syn + e];
         g_vp += gs * s_new * (g_i0 + g_i1);
         const T g_sinf = g_sn * (T(1) - decay);
-        const T g_rate = -dt * decay * g_sn * (s - s_inf) - g_sinf * s_inf / rate;
-        const T g_a = g_sinf / rate + g_rate;
+        const T g_rate = -dt * decay * g_sn * (s - s_inf) - qdiv<T>(g_sinf * s_inf, rate);
+        const T g_a = qdiv<T>(g_sinf, rate) + g_rate;
         const T g_x = g_a * alpha * tr * (T(1) - tr);
-        g_vpre = g_x / delta;
+        g_vpre = qdiv<T>(g_x, delta);
         ((T*)a.g_s)[b * a.n_syn + e] = g_sn * decay;
         gq[0] += s_new * g_w;
         gq[a.k] += -gs * s_new * (g_i0 + g_i1);
@@ -192,7 +199,8 @@ __global__ void syn_backward_kernel(JxbSynArgs a, SynP<T> P) {
         gq[2 * a.k] += g_z0 * u0 + g_z1 * u1;
       }
       gvp_sum += g_vp;
-      g_pre[(int64_t)e * a.batch + b] = g_vpre;
+      if (stile) stile[(size_t)kk * a.batch + b] = g_vpre;
+      else g_pre[(int64_t)e * a.batch + b] = g_vpre;
     }
     gvp_sum = warp_sum(gvp_sum);
     // The postsynaptic voltage gradient of this row, added to g_v at the target by
@@ -201,6 +209,11 @@ __global__ void syn_backward_kernel(JxbSynArgs a, SynP<T> P) {
   }
   // Sum the parameter gradients over the warps (batch slices), fixed order.
   __syncthreads();
+  if (stile) {
+    const int n = a.k * a.batch;
+    T* dst = g_pre + (int64_t)tgt * a.k * a.batch;  // rows e = tgt * k + kk are consecutive
+    for (int q = threadIdx.x; q < n; q += blockDim.x) dst[q] = stile[q];
+  }
   int row = 0;
   for (int q = 0; q < np; ++q) {
     if (!(a.need & (1 << q))) continue;
@@ -246,8 +259,8 @@ int fwd(const JxbSynArgs& a, cudaStream_t st) {
   SynP<T> P;
   for (int q = 0; q < 6; ++q) P.p[q] = (const T*)a.p[q];
   const int nt = a.n_syn / a.k;
-  const int64_t warps = (int64_t)nt * a.batch;
-  const int threads = 256;
+  const int64_t warps = (int64_t)nt;  // one warp per target, looping over the rows
+  const int threads = 128;
   syn_forward_kernel<T><<<(unsigned)((warps * 32 + threads - 1) / threads), threads, 0, st>>>(a, P);
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
@@ -267,7 +280,8 @@ int bwd(const JxbSynArgs& a, cudaStream_t st) {
     set_err("cudaMemsetAsync", e);
     return JXB_ERR_LAUNCH;
   }
-  const size_t smem = sizeof(T) * (size_t)kBwdWarps * 6 * a.k;
+  const size_t stage = sizeof(T) * (size_t)a.k * a.batch;
+  const size_t smem = sizeof(T) * (size_t)kBwdWarps * 6 * a.k + (stage <= (size_t)kStageBytes ? stage : 0);
   if (smem > 227 * 1024) {
     snprintf(g_err, sizeof(g_err), "synapse backward: %d synapses per target exceed shared memory", a.k);
     return JXB_ERR_TOO_LARGE;
