@@ -269,6 +269,9 @@ def run_ours(args, rank, world, device):
            "h2d_bytes_per_step": int(ps_host.numel() * ps_host.element_size()),
            "d2h_bytes_per_step": int(loss_host.element_size() + g_host.numel() * g_host.element_size())}
 
+    stored = sim.stores_trajectory(T)
+    stored_mode = ("reverse sweep over the trajectory stored by the forward" if stored
+                   else "recompute of each segment from its checkpoint")
     S, P, fwd_b, bwd_b = algorithmic_bytes(low, 4)
     peak, peak_kind = measured_peak_hbm()
     bwd_ms = float(np.mean([t for t, _ in bwd])) if bwd else None
@@ -295,8 +298,10 @@ def run_ours(args, rank, world, device):
                    "nodes": prob.n_nodes, "tree_height": prob.meta["height"], "batch": B,
                    "time_steps": T, "checkpoint": args.checkpoint,
                    "threads_per_cta": args.threads, "rows_per_cta": args.rows,
-                   "l2": "working set larger than L2 (trajectory buffer %d MB)"
-                         % (args.checkpoint * B * low.n_slots * 4 // 2**20),
+                   "adjoint": stored_mode,
+                   "l2": "working set larger than L2 (%s %d MB)" % (
+                       ("stored trajectory", sim.trajectory_bytes(T) // 2**20) if stored
+                       else ("trajectory buffer", args.checkpoint * B * low.n_slots * 4 // 2**20)),
                    "loss": "MSE of the somatic voltage to a held-out parameter set's trace"},
         "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
         "clocks": clocks.summary(), "loss": float(loss.detach()),

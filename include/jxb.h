@@ -174,13 +174,21 @@ typedef struct JxbSimArgs_ {
   void* state;                /* (batch, n_slots), updated in place */
   void* ckpt;                 /* optional (n_ckpt, batch, n_slots): state at t0 + m*ckpt_every */
   int32_t ckpt_every, ckpt_base;  /* ckpt index of t0 is (t0 - ckpt_base) / ckpt_every */
-  void* traj;                 /* optional (n_steps, batch, n_slots): state before each step */
-  void* traj_piv;             /* adjoint: (n_steps, batch, n_nodes) reciprocal pivots */
+  /* Trajectory. Adjoint: scratch (n_steps, batch, n_slots) for the state before each
+   * recomputed step and (n_steps, batch, n_nodes) for the reciprocal pivots; with
+   * traj_stored the caller's forward has filled both and the adjoint reads them
+   * (traj then holds n_steps + 1 entries, the last being the state after the
+   * segment, and ckpt must point at entry 0). Forward (optional, mode 0): the launch
+   * stores the state before each of its steps and after its last step
+   * (n_steps + 1 entries) and, with traj_piv, the pivots of each step. */
+  void* traj;
+  void* traj_piv;
   /* adjoint */
   void* adj;                  /* (batch, n_slots) adjoint of the state, updated in place */
   const void* rec_grad;       /* (T + 1, batch, n_rec) gradient of the recordings */
   double* pgrad;              /* (batch, n_cols) float64, accumulated: d loss / d pscale */
-  int32_t mode, pad2;         /* 0 = step, 1 = initial currents only */
+  int32_t mode;               /* 0 = step, 1 = initial currents only */
+  int32_t traj_stored;        /* adjoint: traj / traj_piv hold the forward's values */
   /* Optional work areas in global memory instead of shared memory, for blocks whose
    * working set exceeds the shared memory of a CTA: item i uses the bytes
    * [gscratch + i * gscratch_stride, + gscratch_stride). gscratch is 256-byte aligned

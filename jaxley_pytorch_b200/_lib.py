@@ -69,7 +69,7 @@ class JxbSimArgs(C.Structure):
         ("ckpt_every", C.c_int32), ("ckpt_base", C.c_int32),
         ("traj", _p), ("traj_piv", _p),
         ("adj", _p), ("rec_grad", _p), ("pgrad", _p),
-        ("mode", C.c_int32), ("pad2", C.c_int32),
+        ("mode", C.c_int32), ("traj_stored", C.c_int32),
         ("gscratch", _p), ("gscratch_stride", C.c_int64),
         ("sched_ptr", _p), ("sched", _p), ("sched_warps", C.c_int32), ("pad5", C.c_int32),
         ("gacc", _p), ("gacc_stride", C.c_int64),

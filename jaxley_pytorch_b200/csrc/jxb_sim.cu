@@ -472,7 +472,8 @@ struct NodeWalk {
 template <typename T>
 __device__ __forceinline__ void run_steps(const JxbSimArgs& a, const JxbBlock& blk, int item_block, int row0,
                                           int rows, const SimSmem<T>& sm, T dt, int t0, int nsteps, int mode,
-                                          bool record, bool ckpt, T* traj, T* X1, T* piv = nullptr) {
+                                          bool record, bool ckpt, T* traj, T* X1, T* piv = nullptr,
+                                          bool traj_final = false) {
   const int nn = blk.n_nodes, ns = blk.n_slots, np = blk.n_pslots;
   for (int step = 0; step <= nsteps; ++step) {
     const int t = t0 + step;
@@ -491,6 +492,10 @@ __device__ __forceinline__ void run_steps(const JxbSimArgs& a, const JxbBlock& b
         piv[((size_t)(step - 1) * a.batch + b) * a.n_nodes + i] = sm.D[(size_t)r * nn + j];
       if (record && step > 0 && (f & FLAG_REC)) record_node<T>(a, i, x, b, t);
       if (step == nsteps) {
+        if (traj_final) {  // the state after the last step closes the trajectory
+          T* g = traj + ((size_t)nsteps * a.batch + b) * a.n_slots + blk.slot0 + sm.soff[j];
+          for (int q = 0; q < nslot; ++q) g[q] = x[q];
+        }
         if (mode != 0) {
           T lin, cst;
           if (mode == 2) node_channels<T>(sm, j, x, sm.pv + (size_t)r * np, dt, 2, lin, cst);
@@ -572,8 +577,11 @@ __device__ __forceinline__ void sim_forward_body(const JxbSimArgs& a, const JxbS
   init_voltages<T>(blk, sm, rows);
   __syncthreads();
   const int nsteps = a.mode == 0 ? a.n_steps : 0;
+  // With `traj`, the launch also stores the state before every step, the state after
+  // the last one and the reciprocal pivots of every step (`traj_piv`), for an
+  // adjoint that then skips its recompute (`traj_stored`).
   run_steps<T>(a, blk, item.block, row0, rows, sm, dt, a.t0, nsteps, a.mode, a.n_rec > 0, a.ckpt != nullptr,
-               (T*)a.traj, nullptr);
+               (T*)a.traj, nullptr, (T*)a.traj_piv, a.traj != nullptr && nsteps > 0);
   // Write the resident states back.
   const int ns = blk.n_slots;
   for (int r = 0; r < rows; ++r) {
@@ -722,14 +730,25 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
   const T dt = T(a.dt);
   const int K = a.n_steps;
   T* traj = (T*)a.traj;
-  // Recompute the segment from its checkpoint, storing the state before every step.
   stage_item<T>(a, blk, row0, rows, sm, dt, (const T*)a.ckpt, (const T*)a.adj, gslots);
   __syncthreads();
-  init_voltages<T>(blk, sm, rows);
-  __syncthreads();
-  sm.cm = (T*)a.cm + blk.node0;  // read only
   T* piv = (T*)a.traj_piv;
-  run_steps<T>(a, blk, item.block, row0, rows, sm, dt, a.t0, K, 0, false, false, traj, sm.X1, piv);
+  if (a.traj_stored) {
+    // The forward stored the segment's states (entries 0..K) and pivots: the final
+    // voltages are those of entry K.
+    for (int w = tid; w < nn * rows; w += nthr) {
+      const int r = w / nn, j = w - r * nn;
+      sm.X1[(size_t)r * nn + j] = traj[((size_t)K * a.batch + row0 + r) * a.n_slots + blk.slot0 + sm.soff[j]];
+    }
+    sm.cm = (T*)a.cm + blk.node0;  // read only
+    __syncthreads();
+  } else {
+    // Recompute the segment from its checkpoint, storing the state before every step.
+    init_voltages<T>(blk, sm, rows);
+    __syncthreads();
+    sm.cm = (T*)a.cm + blk.node0;  // read only
+    run_steps<T>(a, blk, item.block, row0, rows, sm, dt, a.t0, K, 0, false, false, traj, sm.X1, piv);
+  }
 
   const T* rec_grad = (const T*)a.rec_grad;
   const int total = nn * rows;
@@ -1167,6 +1186,7 @@ extern "C" int jxb_sim_backward_noalloc(const JxbSimArgs* a, void* stream) {
   // The caller's trajectory pointers are ignored; the rest is checked and launched
   // as by jxb_sim_backward.
   JxbSimArgs b = *a;
+  b.traj_stored = 0;  // the segment is recomputed into the library's array
   b.traj = g_noalloc_ptr[dev];
   b.traj_piv = (unsigned char*)g_noalloc_ptr[dev] + piv_off;
   const int rc = jxb::check_sim_args(&b, true);

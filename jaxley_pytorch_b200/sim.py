@@ -346,15 +346,19 @@ class Simulation:
 
     `segment` is the number of steps per launch (1 = the plain per-step drop-in;
     `None` = the whole horizon in one persistent launch). `checkpoint` is the number
-    of steps between stored states for the adjoint (each backward launch recomputes
-    one such segment).
+    of steps per adjoint launch. `store_trajectory`: the forward stores the state
+    before every step and the pivots of every step, and the adjoint reads them
+    instead of recomputing each segment from a stored state every `checkpoint` steps
+    (`"auto"`: for persistent launches, when the trajectory takes at most
+    `store_fraction` of the free device memory).
     """
 
     def __init__(self, problem: Problem, dtype=torch.float32, device="cuda",
                  max_block_nodes: int = 4096, rows_per_item: int = 1,
                  segment: Optional[int] = None, init_steady: bool = False,
                  low: Optional[Lowered] = None, checkpoint: int = 100, threads: int = 256,
-                 keep_currents: bool = True, programs: bool = True, schedule: bool = True):
+                 keep_currents: bool = True, programs: bool = True, schedule: bool = True,
+                 store_trajectory="auto", store_fraction: float = 0.5):
         self.problem = problem
         self.low = low if low is not None else lower(problem, max_block_nodes=max_block_nodes,
                                                      keep_currents=keep_currents)
@@ -363,12 +367,38 @@ class Simulation:
         self.segment = segment
         self.init_steady = init_steady
         self.checkpoint = int(checkpoint)
+        if store_trajectory not in (True, False, "auto"):
+            raise ValueError("store_trajectory must be True, False or 'auto'")
+        self.store_trajectory = store_trajectory
+        self.store_fraction = float(store_fraction)
+        self._store_free: Optional[int] = None
 
     def n_steps(self, n_steps: Optional[int] = None) -> int:
         return self.low.n_steps if n_steps is None else int(n_steps)
 
-    def forward_raw(self, pscale: torch.Tensor, T: int, ckpt: Optional[torch.Tensor] = None):
-        """Runs the forward pass; returns `(rec (T+1, B, n_rec), final state)`."""
+    def trajectory_bytes(self, T: int) -> int:
+        """Device bytes of a stored trajectory of T steps (states and pivots)."""
+        low = self.low
+        item = torch.empty((), dtype=self.model.dtype).element_size()
+        return ((T + 1) * low.n_slots + T * low.n_nodes) * low.batch * item
+
+    def stores_trajectory(self, T: int) -> bool:
+        """Whether a differentiable run of T steps stores its trajectory."""
+        if self.store_trajectory != "auto":
+            return bool(self.store_trajectory)
+        if self.segment is not None:
+            return False
+        if self._store_free is None:  # sampled once, outside any graph capture
+            if torch.cuda.is_current_stream_capturing():
+                return False
+            self._store_free = torch.cuda.mem_get_info(self.model.device)[0]
+        return self.trajectory_bytes(T) <= self.store_fraction * self._store_free
+
+    def forward_raw(self, pscale: torch.Tensor, T: int, ckpt: Optional[torch.Tensor] = None,
+                    traj: Optional[torch.Tensor] = None, piv: Optional[torch.Tensor] = None):
+        """Runs the forward pass; returns `(rec (T+1, B, n_rec), final state)`. With
+        `traj (T+1, B, n_slots)` and `piv (T, B, n_nodes)` it also stores the state
+        before every step (and after the last) and the reciprocal pivots."""
         m = self.model
         low = self.low
         state = m.initial_state()
@@ -380,8 +410,12 @@ class Simulation:
         t = 0
         while t < T:
             k = min(seg, T - t)
-            m.launch_forward(m.args(state, k, t, rec, pscale=pscale, ckpt=ckpt,
-                                    ckpt_every=self.checkpoint if ckpt is not None else 0))
+            a = m.args(state, k, t, rec, pscale=pscale, ckpt=ckpt,
+                       ckpt_every=self.checkpoint if ckpt is not None else 0,
+                       traj=traj[t] if traj is not None else None)
+            if piv is not None:
+                a.traj_piv = piv[t].data_ptr()
+            m.launch_forward(a)
             t += k
         return rec, state
 
@@ -408,6 +442,28 @@ class Simulation:
             m.launch_backward(a)
         return pgrad
 
+    def backward_stored(self, pscale: torch.Tensor, T: int, traj: torch.Tensor, piv: torch.Tensor,
+                        rec_grad: torch.Tensor) -> torch.Tensor:
+        """`backward_raw` on the trajectory the forward stored (`forward_raw` with
+        `traj`, `piv`): one adjoint launch per `checkpoint` steps, no recompute."""
+        m = self.model
+        low = self.low
+        K = self.checkpoint
+        nseg = (T + K - 1) // K
+        adj = torch.zeros((low.batch, low.n_slots), dtype=m.dtype, device=m.device)
+        pgrad = torch.zeros((low.batch, low.n_cols), dtype=torch.float64, device=m.device)
+        rec_grad = rec_grad.contiguous()
+        for sgi in range(nseg - 1, -1, -1):
+            t0 = sgi * K
+            k = min(K, T - t0)
+            a = m.args(traj[t0], k, t0, None, pscale=pscale, traj=traj[t0], adj=adj,
+                       rec_grad=rec_grad, pgrad=pgrad)
+            a.ckpt = traj[t0].data_ptr()
+            a.traj_piv = piv[t0].data_ptr()
+            a.traj_stored = 1
+            m.launch_backward(a)
+        return pgrad
+
     def run(self, n_steps: Optional[int] = None, pscale: Optional[torch.Tensor] = None,
             return_state: bool = False):
         """Recordings `(B, n_rec, T + 1)`; differentiable with respect to `pscale`
@@ -424,9 +480,11 @@ class Simulation:
 
 
 class _IntegrateFn(torch.autograd.Function):
-    """Forward: the fused step kernels with a checkpoint every `sim.checkpoint` steps.
-    Backward: the adjoint kernel per segment, in reverse order (recompute + reverse
-    sweep), instead of autograd through every operation of every step."""
+    """Forward: the fused step kernels, storing the trajectory (states and pivots of
+    every step) or a checkpoint every `sim.checkpoint` steps. Backward: the adjoint
+    kernel per segment of `sim.checkpoint` steps, in reverse order (reverse sweep over
+    the stored trajectory, or recompute + reverse sweep), instead of autograd through
+    every operation of every step."""
 
     @staticmethod
     def forward(ctx, pscale, sim, T):
@@ -434,18 +492,29 @@ class _IntegrateFn(torch.autograd.Function):
         K = sim.checkpoint
         nseg = (T + K - 1) // K
         ps = pscale.detach().to(sim.model.dtype).contiguous()
-        ckpt = torch.empty((nseg, low.batch, low.n_slots), dtype=sim.model.dtype,
-                           device=sim.model.device)
-        rec, _ = sim.forward_raw(ps, T, ckpt=ckpt)
+        dev, dt = sim.model.device, sim.model.dtype
+        ctx.stored = sim.stores_trajectory(T)
+        if ctx.stored:
+            traj = torch.empty((T + 1, low.batch, low.n_slots), dtype=dt, device=dev)
+            piv = torch.empty((T, low.batch, low.n_nodes), dtype=dt, device=dev)
+            rec, _ = sim.forward_raw(ps, T, traj=traj, piv=piv)
+            ctx.save_for_backward(ps, traj, piv)
+        else:
+            ckpt = torch.empty((nseg, low.batch, low.n_slots), dtype=dt, device=dev)
+            rec, _ = sim.forward_raw(ps, T, ckpt=ckpt)
+            ctx.save_for_backward(ps, ckpt)
         ctx.sim, ctx.T = sim, T
-        ctx.save_for_backward(ps, ckpt)
         ctx.in_dtype = pscale.dtype
         return rec.permute(1, 2, 0)
 
     @staticmethod
     def backward(ctx, grad_out):
-        ps, ckpt = ctx.saved_tensors
         sim = ctx.sim
         rec_grad = grad_out.to(sim.model.dtype).permute(2, 0, 1).contiguous()
-        pgrad = sim.backward_raw(ps, ctx.T, ckpt, rec_grad)
+        if ctx.stored:
+            ps, traj, piv = ctx.saved_tensors
+            pgrad = sim.backward_stored(ps, ctx.T, traj, piv, rec_grad)
+        else:
+            ps, ckpt = ctx.saved_tensors
+            pgrad = sim.backward_raw(ps, ctx.T, ckpt, rec_grad)
         return pgrad.to(ctx.in_dtype), None, None
