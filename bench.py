@@ -5,8 +5,10 @@ Workload (per GPU): the synthetic L5PC-like tree (300 branches x 4 compartments,
 compartments + branchpoints, near-balanced, height 35-45), 256 parameter sets with
 every conductance scaled by U[0.5, 1.5], float32, dt = 0.025 ms, 4000 steps; one
 bench step = the simulation of all 256 rows, the MSE to a seeded target trace and its
-gradient with respect to the 256 x 10 conductance scales through the adjoint
-(checkpoint every 100 steps). Compartment-steps count compartments x rows x steps
+gradient with respect to the 256 x 10 conductance scales through the adjoint (the
+forward stores the trajectory, 36 GB, and the adjoint sweeps it back in launches of
+100 steps; `recompute` in the line is the same iteration with a checkpoint every 100
+steps recomputed in the adjoint). Compartment-steps count compartments x rows x steps
 (branchpoints excluded, every simulated step once).
 
 The same JSON line carries `uneven`: the uneven batch of 4096 seeded cells
@@ -57,6 +59,8 @@ def parse():
     ap.add_argument("--tsteps", type=int, default=4000)
     ap.add_argument("--checkpoint", type=int, default=100)
     ap.add_argument("--threads", type=int, default=512)
+    ap.add_argument("--forward-threads", type=int, default=256,
+                    help="CTA size of the forward launches (wide register budget up to 256)")
     ap.add_argument("--rows", type=int, default=1)
     ap.add_argument("--cpu-batch", type=int, default=16)
     ap.add_argument("--cpu-tsteps", type=int, default=200)
@@ -68,6 +72,8 @@ def parse():
     ap.add_argument("--uneven-plain-tsteps", type=int, default=100)
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream measurement")
     ap.add_argument("--no-network", action="store_true", help="skip the network training-step measurement")
+    ap.add_argument("--no-recompute", action="store_true",
+                    help="skip the checkpoint/recompute comparison of the main iteration")
     ap.add_argument("--net-tsteps", type=int, default=2000)
     ap.add_argument("--serve-requests", type=int, default=240)
     ap.add_argument("--serve-capacity-requests", type=int, default=160)
@@ -166,10 +172,15 @@ def workload(rank: int, batch: int, tsteps: int):
     return prob, held_out
 
 
-def algorithmic_bytes(low, itemsize: int):
-    """Per compartment-step: S = state slots per compartment, P = batch-varying
-    parameters per compartment (conductances); forward s(2S+P), adjoint launch
-    (recompute with trajectory store + reverse pass) s(6S+2P)."""
+def algorithmic_bytes(low, itemsize: int, stored: bool):
+    """Per compartment-step, in units of s = itemsize: S = state slots per
+    compartment, P = batch-varying parameters per compartment (conductances),
+    N = tree nodes per compartment (one reciprocal pivot each). Forward: state read
+    and write and the parameters, s(2S+P), plus with a stored trajectory the state
+    and pivot of every step, s(3S+P+N). Adjoint launch: with a stored trajectory,
+    trajectory and pivot read, adjoint state read and write, parameters, s(3S+P+N);
+    with recompute, the forward's traffic, the trajectory and pivot write, then the
+    reverse pass, s(6S+2P+2N)."""
     comps = [i for i in range(low.n_nodes) if low.cls_comp[low.node_class[i]]]
     S = float(np.mean([low.soff[i + 1] - low.soff[i] for i in comps]))
     cls_np = {}
@@ -182,7 +193,10 @@ def algorithmic_bytes(low, itemsize: int):
             n_par += int(e[2])
         P_list.append(int(np.count_nonzero(low.pcol[po:po + n_par])))
     P = float(np.mean(P_list))
-    return S, P, itemsize * (2 * S + P), itemsize * (6 * S + 2 * P)
+    N = low.n_nodes / len(comps)
+    if stored:
+        return S, P, itemsize * (3 * S + P + N), itemsize * (3 * S + P + N)
+    return S, P, itemsize * (2 * S + P), itemsize * (6 * S + 2 * P + 2 * N)
 
 
 def run_ours(args, rank, world, device):
@@ -194,7 +208,8 @@ def run_ours(args, rank, world, device):
     prob, held = workload(rank, args.batch, args.tsteps)
     T = prob.n_steps
     kw = dict(dtype=torch.float32, device=device, checkpoint=args.checkpoint, init_steady=True,
-              keep_currents=False, threads=args.threads, rows_per_item=args.rows)
+              keep_currents=False, threads=args.threads, rows_per_item=args.rows,
+              forward_threads=args.forward_threads, forward_wide=args.forward_threads <= 256)
     sim = Simulation(prob, **kw)
     tsim = Simulation(held, **kw)
     with torch.no_grad():
@@ -272,7 +287,7 @@ def run_ours(args, rank, world, device):
     stored = sim.stores_trajectory(T)
     stored_mode = ("reverse sweep over the trajectory stored by the forward" if stored
                    else "recompute of each segment from its checkpoint")
-    S, P, fwd_b, bwd_b = algorithmic_bytes(low, 4)
+    S, P, fwd_b, bwd_b = algorithmic_bytes(low, 4, stored)
     peak, peak_kind = measured_peak_hbm()
     bwd_ms = float(np.mean([t for t, _ in bwd])) if bwd else None
     fwd_ms = float(np.mean([t for t, _ in fwd])) if fwd else None
@@ -297,7 +312,8 @@ def run_ours(args, rank, world, device):
         "config": {"workload": "l5pc_tree_300x4_b256_t4000_fwd_adjoint", "compartments": n_comp,
                    "nodes": prob.n_nodes, "tree_height": prob.meta["height"], "batch": B,
                    "time_steps": T, "checkpoint": args.checkpoint,
-                   "threads_per_cta": args.threads, "rows_per_cta": args.rows,
+                   "threads_per_cta": args.threads, "forward_threads_per_cta": args.forward_threads,
+                   "rows_per_cta": args.rows,
                    "adjoint": stored_mode,
                    "l2": "working set larger than L2 (%s %d MB)" % (
                        ("stored trajectory", sim.trajectory_bytes(T) // 2**20) if stored
@@ -306,6 +322,31 @@ def run_ours(args, rank, world, device):
         "roofline": roofline, "e2e": e2e, "gpu_launches": int(launches),
         "clocks": clocks.summary(), "loss": float(loss.detach()),
     }
+    if stored and not args.no_recompute:
+        # The same iteration with the checkpoint/recompute adjoint (a checkpoint every
+        # `checkpoint` steps, each segment recomputed in its adjoint launch).
+        del sim
+        rsim = Simulation(prob, store_trajectory=False, **kw)
+
+        def recompute_step(ps):
+            rec = rsim.run(pscale=ps)
+            loss = ((rec[:, 0, :] - target) ** 2).mean()
+            return torch.autograd.grad(loss, ps)[0]
+
+        for _ in range(2):
+            recompute_step(ps)
+        barrier()
+        torch.cuda.synchronize()
+        r0 = torch.cuda.Event(enable_timing=True)
+        r1 = torch.cuda.Event(enable_timing=True)
+        r0.record()
+        for _ in range(args.steps):
+            recompute_step(ps)
+        r1.record()
+        torch.cuda.synchronize()
+        rms = max_over_ranks(r0.elapsed_time(r1), world, device)
+        out["recompute"] = {"value": comp_steps / (rms / 1e3), "unit": UNIT,
+                            "ms_per_step": rms / args.steps, "checkpoint": args.checkpoint}
     return out
 
 

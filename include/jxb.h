@@ -151,7 +151,10 @@ typedef struct JxbSimArgs_ {
   const int32_t* level_ptr;   /* chain offsets relative to the block's chain0 */
   const int32_t* gk;          /* (n_pslots,) gradient rank of a trainable parameter, -1 */
   const int32_t* gbase;       /* (n_nodes,) first gradient slot of a node in its block */
-  int32_t max_gslots, pad4;   /* largest number of gradient slots of a block */
+  int32_t max_gslots;         /* largest number of gradient slots of a block */
+  int32_t wide;               /* float, up to 256 threads, not multi: kernels for two CTAs
+                                 per SM with up to 128 registers a thread (default: four
+                                 CTAs with 64) */
   const int32_t* parent;      /* (n_nodes,) parent (internal order) or -1 */
   const int32_t* kid_ptr;     /* (n_nodes+1,) children CSR */
   const int32_t* kid;         /* children (internal order) */

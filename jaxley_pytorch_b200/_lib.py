@@ -58,7 +58,7 @@ class JxbSimArgs(C.Structure):
         ("blocks", _p), ("items", _p),
         ("chain_top", _p), ("chain_len", _p), ("chain_ptop", _p), ("chain_cptr", _p),
         ("chain_child", _p), ("level_ptr", _p),
-        ("gk", _p), ("gbase", _p), ("max_gslots", C.c_int32), ("pad4", C.c_int32),
+        ("gk", _p), ("gbase", _p), ("max_gslots", C.c_int32), ("wide", C.c_int32),
         ("parent", _p), ("kid_ptr", _p), ("kid", _p),
         ("stim_ptr", _p), ("stim_idx", _p), ("area", _p), ("stim", _p),
         ("n_stim", C.c_int32), ("stim_steps", C.c_int32), ("stim_rows", C.c_int32), ("pad0", C.c_int32),

@@ -866,17 +866,22 @@ __device__ __forceinline__ const JxbSimArgs& item_args(const JxbSimArgs& L, int&
   return L;
 }
 
-// float: at most 64 registers, so that two 512-thread CTAs (four of 256) fit an SM.
-template <typename T, int NT, bool GM, bool MULTI>
-__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 1024 / NT : 1) sim_forward_kernel(JxbSimArgs L) {
+// MINB CTAs of NT threads per SM: float by default at most 64 registers, so that two
+// 512-thread CTAs (four of 256) fit an SM; the wide variant (JxbSimArgs.wide) of the
+// 256-thread kernels allows 128 registers with two CTAs per SM.
+template <typename T, int NT>
+constexpr int kMinBlocks = sizeof(T) == 4 ? 1024 / NT : 1;
+
+template <typename T, int NT, int MINB, bool GM, bool MULTI>
+__global__ void __launch_bounds__(NT, MINB) sim_forward_kernel(JxbSimArgs L) {
   extern __shared__ __align__(16) char smem_raw[];
   int item_idx;
   const JxbSimArgs& a = item_args<T, MULTI>(L, item_idx);
   sim_forward_body<T, GM>(a, L, item_idx, smem_raw);
 }
 
-template <typename T, int NT, bool GM, bool MULTI>
-__global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 1024 / NT : 1) sim_backward_kernel(JxbSimArgs L) {
+template <typename T, int NT, int MINB, bool GM, bool MULTI>
+__global__ void __launch_bounds__(NT, MINB) sim_backward_kernel(JxbSimArgs L) {
   extern __shared__ __align__(16) char smem_raw[];
   int item_idx;
   const JxbSimArgs& a = item_args<T, MULTI>(L, item_idx);
@@ -885,12 +890,24 @@ __global__ void __launch_bounds__(NT, sizeof(T) == 4 ? 1024 / NT : 1) sim_backwa
 
 template <typename T, int NT>
 void (*pick_kernel(bool backward, bool gm, bool multi))(JxbSimArgs) {
+  constexpr int B = kMinBlocks<T, NT>;
   if (multi) {
-    if (gm) return backward ? sim_backward_kernel<T, NT, true, true> : sim_forward_kernel<T, NT, true, true>;
-    return backward ? sim_backward_kernel<T, NT, false, true> : sim_forward_kernel<T, NT, false, true>;
+    if (gm) return backward ? sim_backward_kernel<T, NT, B, true, true> : sim_forward_kernel<T, NT, B, true, true>;
+    return backward ? sim_backward_kernel<T, NT, B, false, true> : sim_forward_kernel<T, NT, B, false, true>;
   }
-  if (gm) return backward ? sim_backward_kernel<T, NT, true, false> : sim_forward_kernel<T, NT, true, false>;
-  return backward ? sim_backward_kernel<T, NT, false, false> : sim_forward_kernel<T, NT, false, false>;
+  if (gm) return backward ? sim_backward_kernel<T, NT, B, true, false> : sim_forward_kernel<T, NT, B, true, false>;
+  return backward ? sim_backward_kernel<T, NT, B, false, false> : sim_forward_kernel<T, NT, B, false, false>;
+}
+
+// Wide float kernels of up to 256 threads (two CTAs per SM, up to 128 registers);
+// null for float64, whose default kernels already have that budget.
+template <typename T>
+void (*pick_wide_kernel(bool backward, bool gm))(JxbSimArgs) {
+  if constexpr (sizeof(T) == 4) {
+    if (gm) return backward ? sim_backward_kernel<T, 256, 2, true, false> : sim_forward_kernel<T, 256, 2, true, false>;
+    return backward ? sim_backward_kernel<T, 256, 2, false, false> : sim_forward_kernel<T, 256, 2, false, false>;
+  }
+  return nullptr;
 }
 
 // Largest dynamic shared memory already granted to a kernel on a device:
@@ -954,8 +971,11 @@ int launch_sim(const JxbSimArgs& a, bool backward, cudaStream_t stream) {
     return JXB_ERR_ARG;
   }
   // Register budget by launch size: up to 256 threads, 512, 1024.
-  void (*kern)(JxbSimArgs);
-  if (threads <= 256)
+  void (*kern)(JxbSimArgs) = nullptr;
+  if (a.wide && threads <= 256 && a.multi == nullptr) kern = pick_wide_kernel<T>(backward, gm);
+  if (kern)
+    ;
+  else if (threads <= 256)
     kern = pick_kernel<T, 256>(backward, gm, a.multi != nullptr);
   else if (threads <= 512)
     kern = pick_kernel<T, 512>(backward, gm, a.multi != nullptr);

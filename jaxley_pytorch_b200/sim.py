@@ -89,7 +89,8 @@ class DeviceModel:
 
     def __init__(self, low: Lowered, dtype: torch.dtype = torch.float32, device="cuda",
                  rows_per_item: int = 1, threads: int = 256, programs: bool = True,
-                 smem_limit: Optional[int] = None, schedule: bool = True):
+                 smem_limit: Optional[int] = None, schedule: bool = True,
+                 forward_threads: Optional[int] = None, forward_wide: bool = False):
         self.low = low
         self.dtype = dtype
         self.device = torch.device(device)
@@ -132,12 +133,25 @@ class DeviceModel:
         self._sides: List[torch.cuda.Stream] = []
         self._scratch: Dict[str, torch.Tensor] = {}
         self.smem_limit = smem_limit if smem_limit is not None else self._device_smem_limit()
+        # Threads per CTA of each launch kind (the forward may use fewer, with the wide
+        # register budget of JxbSimArgs.wide) and a node schedule for each warp count.
+        self.kind_threads = {"forward": int(forward_threads or threads), "backward": int(threads)}
+        self.forward_wide = bool(forward_wide)
         self.sched_warps = 0
-        if schedule and threads % 32 == 0:
-            sp, sc = node_schedule(low, threads // 32)
-            self.t["sched_ptr"] = i(sp)
-            self.t["sched"] = torch.as_tensor(sc, device=dev).contiguous()
-            self.sched_warps = threads // 32
+        self.kind_sched: Dict[str, tuple] = {}
+        if schedule:
+            by_warps: Dict[int, tuple] = {}
+            for kind, th in self.kind_threads.items():
+                if th % 32:
+                    continue
+                w = th // 32
+                if w not in by_warps:
+                    sp, sc = node_schedule(low, w)
+                    by_warps[w] = (w, i(sp), torch.as_tensor(sc, device=dev).contiguous())
+                self.kind_sched[kind] = by_warps[w]
+            if "backward" in self.kind_sched:
+                w, sp_t, sc_t = self.kind_sched["backward"]
+                self.t["sched_ptr"], self.t["sched"], self.sched_warps = sp_t, sc_t, w
         self.set_rows_per_item(rows_per_item)
 
     def _device_smem_limit(self) -> int:
@@ -281,6 +295,12 @@ class DeviceModel:
         a = _lib.JxbSimArgs.from_buffer_copy(args)
         for k, v in group["maxima"].items():
             setattr(a, k, v)
+        if kind in self.kind_threads:
+            a.threads = self.kind_threads[kind]
+            a.wide = int(kind == "forward" and self.forward_wide)
+            ks = self.kind_sched.get(kind)
+            if ks is not None:
+                a.sched_warps, a.sched_ptr, a.sched = ks[0], ks[1].data_ptr(), ks[2].data_ptr()
         a.items = group["items"].data_ptr()
         a.n_items = group["n_items"]
         if group["gm"]:
@@ -350,7 +370,10 @@ class Simulation:
     before every step and the pivots of every step, and the adjoint reads them
     instead of recomputing each segment from a stored state every `checkpoint` steps
     (`"auto"`: for persistent launches, when the trajectory takes at most
-    `store_fraction` of the free device memory).
+    `store_fraction` of the free device memory). `threads` is the CTA size of the
+    launches; `forward_threads` (default: `threads`) that of the forward launches,
+    which with `forward_wide` (float32, up to 256 threads) use kernels of two CTAs per
+    SM with up to 128 registers a thread instead of 64.
     """
 
     def __init__(self, problem: Problem, dtype=torch.float32, device="cuda",
@@ -358,12 +381,14 @@ class Simulation:
                  segment: Optional[int] = None, init_steady: bool = False,
                  low: Optional[Lowered] = None, checkpoint: int = 100, threads: int = 256,
                  keep_currents: bool = True, programs: bool = True, schedule: bool = True,
-                 store_trajectory="auto", store_fraction: float = 0.5):
+                 store_trajectory="auto", store_fraction: float = 0.5,
+                 forward_threads: Optional[int] = None, forward_wide: bool = False):
         self.problem = problem
         self.low = low if low is not None else lower(problem, max_block_nodes=max_block_nodes,
                                                      keep_currents=keep_currents)
         self.model = DeviceModel(self.low, dtype, device, rows_per_item, threads=threads,
-                                 programs=programs, schedule=schedule)
+                                 programs=programs, schedule=schedule,
+                                 forward_threads=forward_threads, forward_wide=forward_wide)
         self.segment = segment
         self.init_steady = init_steady
         self.checkpoint = int(checkpoint)

@@ -90,3 +90,22 @@ def test_stored_trajectory_equals_recompute(cuda_device, dtype, gm):
     scale = g0.abs().max().item()
     assert scale > 0
     assert (g0 - g1).abs().max().item() <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_forward_launch_shape_does_not_change_results(cuda_device, dtype):
+    """Forward launches of another CTA size (own node schedule) and the wide register
+    budget run the same per-node arithmetic: identical recordings, and gradients
+    equal up to the order of the float64 atomics."""
+    prob = synth.config_uneven(n_cells=24, n_steps=60, max_comp=300, seed=5)
+    low = lower(prob, max_block_nodes=256, keep_currents=False)
+    kw = dict(low=low, dtype=dtype, device=cuda_device, checkpoint=25, threads=512)
+    a = Simulation(prob, **kw)
+    b = Simulation(prob, forward_threads=256, forward_wide=True, **kw)
+    assert b.model.kind_threads == {"forward": 256, "backward": 512}
+    r0, g0 = _grad_run(a, 60)
+    r1, g1 = _grad_run(b, 60)
+    torch.cuda.synchronize()
+    assert torch.equal(r0, r1)
+    scale = g0.abs().max().item()
+    assert (g0 - g1).abs().max().item() <= 1e-12 * scale
