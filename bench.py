@@ -364,6 +364,7 @@ def run_uneven(args, device):
     from jaxley_pytorch_b200.sim import Simulation
     from jaxley_pytorch_b200.tune import autotune
 
+    torch.cuda.empty_cache()
     T = args.uneven_tsteps
     prob = synth.config_uneven(n_cells=args.uneven_cells, n_steps=T)
     n_comp = int(len(prob.comp_inds))
@@ -385,8 +386,11 @@ def run_uneven(args, device):
     def loss_of(target):
         return lambda rec: ((rec - target) ** 2).mean()
 
+    wide = dict(forward_threads=args.forward_threads, forward_wide=args.forward_threads <= 256)
     sim = Simulation(prob, low=low, dtype=torch.float32, device=device, threads=choice.threads,
-                     rows_per_item=choice.rows_per_item, checkpoint=choice.checkpoint)
+                     rows_per_item=choice.rows_per_item, checkpoint=choice.checkpoint,
+                     store_fraction=0.6, **wide)
+    stored = sim.stores_trajectory(T)
     ps0 = sim.model.pscale.clone()
     with torch.no_grad():
         target = sim.run(pscale=ps0 * 1.05).detach()
@@ -397,8 +401,9 @@ def run_uneven(args, device):
     del it
     # the plain per-step form: one launch per step, checkpoint every step
     Tp = args.uneven_plain_tsteps
+    torch.cuda.empty_cache()
     plain = Simulation(prob, low=low, dtype=torch.float32, device=device, threads=choice.threads,
-                       rows_per_item=choice.rows_per_item, checkpoint=1, segment=1)
+                       rows_per_item=choice.rows_per_item, checkpoint=1, segment=1, **wide)
     with torch.no_grad():
         tp = plain.run(n_steps=Tp, pscale=ps0 * 1.05).detach()
 
@@ -415,7 +420,10 @@ def run_uneven(args, device):
         "compartments": n_comp, "nodes": prob.n_nodes, "time_steps": T,
         "persistent": {"value": rate, "unit": UNIT, "ms_per_iteration": ms, "graph_launches": launches,
                        "max_block_nodes": choice.max_block_nodes, "threads_per_cta": choice.threads,
-                       "checkpoint": choice.checkpoint, "loss": loss},
+                       "forward_threads_per_cta": args.forward_threads,
+                       "checkpoint": choice.checkpoint, "loss": loss,
+                       "adjoint": "stored trajectory (%d MB)" % (sim.trajectory_bytes(T) // 2**20) if stored
+                       else "recompute from checkpoints"},
         "per_step": {"value": rate_plain, "unit": UNIT, "ms_per_iteration": ms_plain, "time_steps": Tp,
                      "checkpoint": 1},
         "persistent_over_per_step": rate / rate_plain,

@@ -45,6 +45,9 @@ class GraphedIteration:
                 self._body()
         torch.cuda.current_stream(dev).wait_stream(side)
         torch.cuda.synchronize(dev)
+        # The warm-up's buffers (a stored trajectory can take tens of GB) go back to the
+        # device before the capture allocates its own from the graph's pool.
+        torch.cuda.empty_cache()
         self.graph = torch.cuda.CUDAGraph()
         n0 = sim.model.launches
         with torch.cuda.graph(self.graph):
