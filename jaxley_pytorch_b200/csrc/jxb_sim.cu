@@ -232,6 +232,19 @@ __device__ __forceinline__ void chain_eliminate(const SimSmem<T>& sm, int c, T* 
   const int4 dsc = sm.cdesc[c];
   const int top = dsc.x;
   const int bot = dsc.y & ~kManyKids;
+  // The first kSeg nodes above the bottom are loaded together with the bottom and the
+  // child chains (indices clamped to the chain: a shorter chain runs its unused
+  // lanes on copies of its top node and never stores them).
+  const int n0 = min(kSeg, bot - top);
+  T dd[kSeg], ss[kSeg], lo[kSeg], up[kSeg];
+#pragma unroll
+  for (int q = 0; q < kSeg; ++q) {
+    const int i = max(bot - 1 - q, top), i1 = min(i + 1, bot);
+    dd[q] = Dr[i];
+    ss[q] = Sr[i];
+    lo[q] = al[i1];
+    up[q] = au[i1];
+  }
   T d = Dr[bot], s = Sr[bot];
   if (!(dsc.y & kManyKids)) {
     // up to two child chains: their values are loaded together
@@ -260,9 +273,25 @@ __device__ __forceinline__ void chain_eliminate(const SimSmem<T>& sm, int c, T* 
   T id = rcp(d);
   Dr[bot] = id;
   Sr[bot] = s;
-  for (int hi = bot - 1; hi >= top; hi -= kSeg) {
+#pragma unroll
+  for (int q = 0; q < kSeg; ++q) {
+    const T f = up[q] * id;
+    d = dd[q] - lo[q] * f;
+    s = ss[q] - s * f;
+    id = rcp(d);
+    dd[q] = id;
+    ss[q] = s;
+  }
+#pragma unroll
+  for (int q = 0; q < kSeg; ++q)
+    if (q < n0) {
+      Dr[bot - 1 - q] = dd[q];
+      Sr[bot - 1 - q] = ss[q];
+    }
+  // Chains longer than 1 + kSeg continue segment by segment from the recurrence's
+  // state after the first kSeg nodes (all of them real then).
+  for (int hi = bot - 1 - kSeg; hi >= top; hi -= kSeg) {
     const int n = min(kSeg, hi - top + 1);
-    T dd[kSeg], ss[kSeg], lo[kSeg], up[kSeg];
 #pragma unroll
     for (int q = 0; q < kSeg; ++q)
       if (q < n) {
@@ -300,8 +329,32 @@ __device__ __forceinline__ void chain_backsub(const SimSmem<T>& sm, int c, const
   const int top = dsc.x;
   const int bot = dsc.y & ~kManyKids;
   const int pt = dsc.w;
+  // The first kSeg + 1 nodes in one pass, loads first (indices clamped to the chain,
+  // unused lanes never stored), then the rest of a longer chain by segments.
+  constexpr int kB = kSeg + 1;
+  const int n0 = min(kB, bot - top + 1);
+  T db[kB], sb[kB], lb[kB];
+#pragma unroll
+  for (int q = 0; q < kB; ++q) {
+    const int i = min(top + q, bot);
+    db[q] = Dr[i];
+    sb[q] = Sr[i];
+    lb[q] = al[i];
+  }
   T xp = pt >= 0 ? Sr[pt] : T(0);
-  for (int l0 = top; l0 <= bot; l0 += kSeg) {
+#pragma unroll
+  for (int q = 0; q < kB; ++q) {
+    const T x = (sb[q] - lb[q] * xp) * db[q];
+    sb[q] = x;
+    xp = x;
+  }
+#pragma unroll
+  for (int q = 0; q < kB; ++q)
+    if (q < n0) {
+      Sr[top + q] = sb[q];
+      if (Vr) Vr[top + q] += sb[q];
+    }
+  for (int l0 = top + kB; l0 <= bot; l0 += kSeg) {
     const int n = min(kSeg, bot - l0 + 1);
     T dd[kSeg], ss[kSeg], ll[kSeg];
 #pragma unroll
@@ -648,6 +701,16 @@ __device__ __forceinline__ void chain_eliminate_rhs(const SimSmem<T>& sm, int c,
   const int4 dsc = sm.cdesc[c];
   const int top = dsc.x;
   const int bot = dsc.y & ~kManyKids;
+  // First segment loaded with the bottom and the child chains (as chain_eliminate).
+  const int n0 = min(kSeg, bot - top);
+  T ss[kSeg], up[kSeg], dn[kSeg];
+#pragma unroll
+  for (int q = 0; q < kSeg; ++q) {
+    const int i = max(bot - 1 - q, top), i1 = min(i + 1, bot);
+    ss[q] = Sr[i];
+    up[q] = au[i1];
+    dn[q] = Dr[i1];
+  }
   T s = Sr[bot];
   if (!(dsc.y & kManyKids)) {
     const int k0 = dsc.z & 0xFFFF, k1 = (unsigned)dsc.z >> 16;
@@ -663,9 +726,16 @@ __device__ __forceinline__ void chain_eliminate_rhs(const SimSmem<T>& sm, int c,
     }
   }
   Sr[bot] = s;
-  for (int hi = bot - 1; hi >= top; hi -= kSeg) {
+#pragma unroll
+  for (int q = 0; q < kSeg; ++q) {
+    s = ss[q] - s * (up[q] * dn[q]);
+    ss[q] = s;
+  }
+#pragma unroll
+  for (int q = 0; q < kSeg; ++q)
+    if (q < n0) Sr[bot - 1 - q] = ss[q];
+  for (int hi = bot - 1 - kSeg; hi >= top; hi -= kSeg) {
     const int n = min(kSeg, hi - top + 1);
-    T ss[kSeg], up[kSeg], dn[kSeg];
 #pragma unroll
     for (int q = 0; q < kSeg; ++q)
       if (q < n) {
