@@ -390,8 +390,13 @@ __device__ __forceinline__ void block_solve(const JxbBlock& blk, const SimSmem<T
   const int nn = blk.n_nodes;
   const int nlev = blk.n_levels;
   // Elimination, leaf chains first (solver_voltage.py:93-98).
+  // (the level table is static: the next level's bounds are read before the barrier)
+  int la = sm.lp[0], lb = sm.lp[1];
   for (int h = 0; h < nlev; ++h) {
-    const int c0 = sm.lp[h], nch = sm.lp[h + 1] - c0;
+    const int lc = h + 2 <= nlev ? sm.lp[h + 2] : lb;
+    const int c0 = la, nch = lb - la;
+    la = lb;
+    lb = lc;
     for (int w = tid; w < nch * rows; w += NT) {
       const int r = rows == 1 ? 0 : w / nch;  // no division for one row
       chain_eliminate<T>(sm, c0 + (w - r * nch), sm.D + (size_t)r * nn, sm.S + (size_t)r * nn, al, au);
@@ -399,8 +404,12 @@ __device__ __forceinline__ void block_solve(const JxbBlock& blk, const SimSmem<T
     __syncthreads();
   }
   // Back-substitution, root chains first (solver_voltage.py:100-106).
+  int hb = sm.lp[nlev - 1], he = sm.lp[nlev];
   for (int h = nlev - 1; h >= 0; --h) {
-    const int c0 = sm.lp[h], nch = sm.lp[h + 1] - c0;
+    const int hz = h > 0 ? sm.lp[h - 1] : hb;
+    const int c0 = hb, nch = he - hb;
+    he = hb;
+    hb = hz;
     for (int w = tid; w < nch * rows; w += NT) {
       const int r = rows == 1 ? 0 : w / nch;
       chain_backsub<T>(sm, c0 + (w - r * nch), sm.D + (size_t)r * nn, sm.S + (size_t)r * nn, al,
@@ -462,7 +471,7 @@ __device__ __forceinline__ T stim_current(const JxbSimArgs& a, int i, int b, int
   const T* st = (const T*)a.stim + (size_t)t * a.stim_rows * a.n_stim +
                 (size_t)(a.stim_rows == 1 ? 0 : b) * a.n_stim;
   const T area = ((const T*)a.area)[i];
-  for (int q = a.stim_ptr[i]; q < a.stim_ptr[i + 1]; ++q) acc += st[a.stim_idx[q]] / area * T(100000);
+  for (int q = a.stim_ptr[i]; q < a.stim_ptr[i + 1]; ++q) acc += fdiv(st[a.stim_idx[q]], area) * T(100000);
   return acc;
 }
 
@@ -528,9 +537,9 @@ __device__ __forceinline__ void run_steps(const JxbSimArgs& a, const JxbBlock& b
                                           bool record, bool ckpt, T* traj, T* X1, T* piv = nullptr,
                                           bool traj_final = false) {
   const int nn = blk.n_nodes, ns = blk.n_slots, np = blk.n_pslots;
+  const NodeWalk walk(a, blk, rows, item_block);  // the same visits every step
   for (int step = 0; step <= nsteps; ++step) {
     const int t = t0 + step;
-    const NodeWalk walk(a, blk, rows, item_block);
     for (int q = 0; q < walk.n; ++q) {
       int r, j;
       if (!walk.get(q, r, j)) continue;
@@ -587,7 +596,7 @@ __device__ __forceinline__ void run_steps(const JxbSimArgs& a, const JxbBlock& b
       // Delta form of the implicit step: A (v' - v) = rhs - A v, with
       // (A v)_j = d_j v_j + sum over neighbours of the off-diagonals times their v,
       // written with voltage differences (exact algebra, small increments).
-      const T lin_t = dt * (lin / cmv);
+      const T lin_t = dt * fdiv(lin, cmv);
       T axv = T(0);
       const int pj = sm.par[j];
       if (pj >= 0) axv += sm.al[j] * (Vr[pj] - v);
@@ -597,7 +606,7 @@ __device__ __forceinline__ void run_steps(const JxbSimArgs& a, const JxbBlock& b
       }
       const T dgj = sm.dg ? sm.dg[j] : ((f & FLAG_COMP) ? T(1) : T(0)) + dt * ((const T*)a.gsum)[i];
       sm.D[(size_t)r * nn + j] = dgj + lin_t;
-      sm.S[(size_t)r * nn + j] = ((f & FLAG_COMP) ? dt * (cst / cmv) - lin_t * v : T(0)) - axv;
+      sm.S[(size_t)r * nn + j] = ((f & FLAG_COMP) ? dt * fdiv(cst, cmv) - lin_t * v : T(0)) - axv;
     }
     if (step == nsteps) break;
     __syncthreads();
@@ -764,16 +773,24 @@ __device__ __forceinline__ void block_solve_pivots(const JxbBlock& blk, const Si
   const int tid = threadIdx.x, NT = blockDim.x;
   const int nn = blk.n_nodes;
   const int nlev = blk.n_levels;
+  int la = sm.lp[0], lb = sm.lp[1];
   for (int h = 0; h < nlev; ++h) {
-    const int c0 = sm.lp[h], nch = sm.lp[h + 1] - c0;
+    const int lc = h + 2 <= nlev ? sm.lp[h + 2] : lb;
+    const int c0 = la, nch = lb - la;
+    la = lb;
+    lb = lc;
     for (int w = tid; w < nch * rows; w += NT) {
       const int r = rows == 1 ? 0 : w / nch;  // no division for one row
       chain_eliminate_rhs<T>(sm, c0 + (w - r * nch), sm.D + (size_t)r * nn, sm.S + (size_t)r * nn, au);
     }
     __syncthreads();
   }
+  int hb = sm.lp[nlev - 1], he = sm.lp[nlev];
   for (int h = nlev - 1; h >= 0; --h) {
-    const int c0 = sm.lp[h], nch = sm.lp[h + 1] - c0;
+    const int hz = h > 0 ? sm.lp[h - 1] : hb;
+    const int c0 = hb, nch = he - hb;
+    he = hb;
+    hb = hz;
     for (int w = tid; w < nch * rows; w += NT) {
       const int r = rows == 1 ? 0 : w / nch;
       chain_backsub<T>(sm, c0 + (w - r * nch), sm.D + (size_t)r * nn, sm.S + (size_t)r * nn, al,
@@ -822,6 +839,7 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
 
   const T* rec_grad = (const T*)a.rec_grad;
   const int total = nn * rows;
+  const NodeWalk walk(a, blk, rows, item.block);  // the same visits every step
   for (int step = K - 1; step >= 0; --step) {
     const int t = a.t0 + step;
     // Phase 1: recording gradients at t + 1, the pivots of the step's matrix and the
@@ -846,7 +864,6 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
     // the forward elimination.
     block_solve_pivots<T>(blk, sm, rows, sm.au, sm.al);
     // Phase 4: vector-Jacobian products of the step.
-    const NodeWalk walk(a, blk, rows, item.block);
     for (int q = 0; q < walk.n; ++q) {
       int r, j;
       if (!walk.get(q, r, j)) continue;
@@ -861,14 +878,14 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
       const bool comp = (sm.flags[j] & FLAG_COMP) != 0;
       // d = dg + dt * lin / cm,  rhs = v + dt * cst / cm (compartments only; the
       // branchpoints have no channels).
-      const T lrs = T(1000.0) * dt * lr / sm.cm[j];
+      const T lrs = fdiv(T(1000.0) * dt * lr, sm.cm[j]);
       T lv = comp ? lr : T(0);
       if (a.g_syn_lin && a.syn_ptr) {
         // d loss / d (synaptic slope, offset) of node j: the slope enters the
         // diagonal (and, on compartments, the right-hand side as -lin * v), the
         // offset the right-hand side with a minus sign.
         const int i = blk.node0 + j;
-        const T f = lr * dt / sm.cm[j];
+        const T f = fdiv(lr * dt, sm.cm[j]);
         const T gl = comp ? -f * xnew : -f * (xnew - x[0]);
         const T gc = comp ? -f : T(0);
         for (int q = a.syn_ptr[i]; q < a.syn_ptr[i + 1]; ++q) {
