@@ -9,7 +9,7 @@
 
 namespace jxb {
 
-enum ProgramId { PROG_GENERIC = 0, PROG_HH = 1, PROG_L5PC_DEND = 2 };
+enum ProgramId { PROG_GENERIC = 0, PROG_HH = 1, PROG_L5PC_DEND = 2, PROG_L5PC_SOMA = 3 };
 
 // Layout of every channel type in a program: number of state and parameter slots.
 template <int TYPE> struct ChanInfo;
@@ -248,6 +248,241 @@ struct Program {
 };
 
 template <typename T> using ProgHH = Program<T, CH_HH>;
+
+// The L5PC somatic channel set (mech/channels/l5pc.py) in insertion order: NaTs2T,
+// SKv3_1, SKE2, CaNernstReversal, CaPump, CaHVA, CaLVA, Leak, with the reference's
+// calcium coupling: SKE2 reads cai, the reversal is recomputed from cai before the
+// pump integrates the previous step's i_Ca, CaHVA/CaLVA use the reversal and write
+// i_Ca. Node-relative slots: 1-2 NaTs2T m,h; 3 SKv3_1 m; 4 SKE2 z; 5 cai; 6 eca;
+// 7 cao; 8-9 CaHVA m,h; 10-11 CaLVA m,h; 12 i_Ca; parameters 0-16 in entry order
+// (the lowering grants this program only to classes with exactly that layout). The
+// operations and their order are the interpreter's (jxb_node.cuh: channel_update,
+// channel_current, channel_current_vjp, channel_update_vjp and the logged replay),
+// with constant slots and the undo values in registers.
+template <typename T>
+struct ProgL5pcSoma {
+  static __device__ __forceinline__ T pump_target(const T* x, const T* p, T& drive) {
+    drive = T(-10000.0) * x[12] * p[9] / (T(2) * T(96485) * p[11]);
+    return p[12] + p[10] * drive;
+  }
+  static __device__ __forceinline__ T nernst_scale(const T* p) {  // R T / (2 F) in mV
+    return p[8] * p[7] / (T(2) * p[6]) * T(1000);
+  }
+
+  static __device__ __forceinline__ void forward(T* x, const T* p, T dt, T& lin, T& cst) {
+    const T v = x[0];
+    x[1] = gate_step<T, T>(G_NATS2T_M, v, x[1], dt, nullptr);
+    x[2] = gate_step<T, T>(G_NATS2T_H, v, x[2], dt, nullptr);
+    x[3] = gate_step<T, T>(G_SKV31_M, v, x[3], dt, nullptr);
+    {  // SKE2, tau_z = 1 (l5pc.py:488-500)
+      const T zinf = ske2_zinf<T>(x[5]);
+      const T em1 = save_expm1(T(-1.0) / T(1.0) * dt);
+      const T z = x[4];
+      x[4] = z + (z - zinf) * em1;
+    }
+    x[6] = nernst_scale(p) * lg(x[7] / x[5]);  // l5pc.py:891-902
+    {  // CaPump (l5pc.py:842-861)
+      const T cai = x[5];
+      T drive;
+      const T cai_inf = pump_target(x, p, drive);
+      const T em1 = save_expm1(-dt / p[10]);
+      x[5] = cai + (cai - cai_inf) * em1;
+    }
+    x[8] = gate_step<T, T>(G_CAHVA_M, v, x[8], dt, nullptr);
+    x[9] = gate_step<T, T>(G_CAHVA_H, v, x[9], dt, nullptr);
+    x[10] = gate_step<T, T>(G_CALVA_M, v, x[10], dt, nullptr);
+    x[11] = gate_step<T, T>(G_CALVA_H, v, x[11], dt, nullptr);
+    // Linearised currents at the updated state; i_Ca restarts from zero.
+    x[12] = T(0);
+    T slope = T(0), gge = T(0);
+    {
+      const T m = x[1];
+      const T g = p[0] * ((m * m * m) * x[2]);
+      slope += g;
+      gge += g * p[1];
+    }
+    {
+      const T g = p[2] * x[3];
+      slope += g;
+      gge += g * p[3];
+    }
+    {
+      const T g = p[4] * x[4];
+      slope += g;
+      gge += g * p[5];
+    }
+    {
+      const T m = x[8];
+      const T g = p[13] * ((m * m) * x[9]);
+      const T E = x[6];
+      slope += g;
+      gge += g * E;
+      x[12] += g * (v - E);
+    }
+    {
+      const T m = x[10];
+      const T g = p[14] * ((m * m) * x[11]);
+      const T E = x[6];
+      slope += g;
+      gge += g * E;
+      x[12] += g * (v - E);
+    }
+    slope += p[15];
+    gge += p[15] * p[16];
+    lin = slope * T(1000.0);
+    cst = gge * T(1000.0);
+  }
+
+  static __device__ __forceinline__ void adjoint(T* x, const T* p, T dt, AdjCtx<T>& c) {
+    const T v = x[0];
+    // Replay of the updates with the partial derivatives the reverse pass needs.
+    T e1, e2, e3, e8, e9, e10, e11;
+    const T o1 = x[1];
+    const Dual<T> n1 = gate_step<Dual<T>, T>(G_NATS2T_M, Dual<T>(v, T(1)), o1, dt, &e1);
+    x[1] = n1.v;
+    const T o2 = x[2];
+    const Dual<T> n2 = gate_step<Dual<T>, T>(G_NATS2T_H, Dual<T>(v, T(1)), o2, dt, &e2);
+    x[2] = n2.v;
+    const T o3 = x[3];
+    const Dual<T> n3 = gate_step<Dual<T>, T>(G_SKV31_M, Dual<T>(v, T(1)), o3, dt, &e3);
+    x[3] = n3.v;
+    const T ske_em1 = save_expm1(T(-1.0) / T(1.0) * dt);
+    const Dual<T> zi = ske2_zinf<Dual<T>>(Dual<T>(x[5], T(1)));
+    const T o4 = x[4];
+    const T dx4 = T(1) + ske_em1, dy4 = -ske_em1 * zi.d;
+    x[4] = o4 + (o4 - zi.v) * ske_em1;
+    const T o6 = x[6];
+    const T C = nernst_scale(p);
+    x[6] = C * lg(x[7] / x[5]);
+    const T o5 = x[5];
+    {
+      T drive;
+      const T cai_inf = pump_target(x, p, drive);
+      const T em1 = save_expm1(-dt / p[10]);
+      x[5] = o5 + (o5 - cai_inf) * em1;
+    }
+    const T o8 = x[8];
+    const Dual<T> n8 = gate_step<Dual<T>, T>(G_CAHVA_M, Dual<T>(v, T(1)), o8, dt, &e8);
+    x[8] = n8.v;
+    const T o9 = x[9];
+    const Dual<T> n9 = gate_step<Dual<T>, T>(G_CAHVA_H, Dual<T>(v, T(1)), o9, dt, &e9);
+    x[9] = n9.v;
+    const T o10 = x[10];
+    const Dual<T> n10 = gate_step<Dual<T>, T>(G_CALVA_M, Dual<T>(v, T(1)), o10, dt, &e10);
+    x[10] = n10.v;
+    const T o11 = x[11];
+    const Dual<T> n11 = gate_step<Dual<T>, T>(G_CALVA_H, Dual<T>(v, T(1)), o11, dt, &e11);
+    x[11] = n11.v;
+
+    // VJPs of the currents at the updated state, last channel first.
+    const T lr = c.lr, x1 = c.x1;
+    T* lam = c.lam;
+    {  // Leak
+      const T g = p[15], E = p[16];
+      c.grad(15, lr * (E - x1));
+      c.grad(16, g * lr);
+    }
+    const T lI = lam[12];
+    {  // CaLVA
+      const T g = p[14], m = x[10], h = x[11];
+      const T mp = m * m, Gv = mp * h, E = x[6], cc = g * Gv;
+      const T lc = lr * (E - x1) + (v - E) * lI;
+      const T lE = cc * (lr - lI);
+      c.lv += cc * lI;
+      lam[10] += g * (T(2) * m) * h * lc;
+      lam[11] += g * mp * lc;
+      c.grad(14, Gv * lc);
+      lam[6] += lE;
+    }
+    {  // CaHVA
+      const T g = p[13], m = x[8], h = x[9];
+      const T mp = m * m, Gv = mp * h, E = x[6], cc = g * Gv;
+      const T lc = lr * (E - x1) + (v - E) * lI;
+      const T lE = cc * (lr - lI);
+      c.lv += cc * lI;
+      lam[8] += g * (T(2) * m) * h * lc;
+      lam[9] += g * mp * lc;
+      c.grad(13, Gv * lc);
+      lam[6] += lE;
+    }
+    {  // SKE2
+      const T g = p[4], z = x[4], E = p[5];
+      const T lc = lr * (E - x1);
+      lam[4] += g * lc;
+      c.grad(4, z * lc);
+      c.grad(5, (g * z) * lr);
+    }
+    {  // SKv3_1
+      const T g = p[2], m = x[3], E = p[3];
+      const T lc = lr * (E - x1);
+      lam[3] += g * lc;
+      c.grad(2, m * lc);
+      c.grad(3, (g * m) * lr);
+    }
+    {  // NaTs2T
+      const T g = p[0], m = x[1], h = x[2];
+      const T mp = m * m * m, Gv = mp * h, E = p[1];
+      const T lc = lr * (E - x1);
+      lam[1] += g * (T(3) * (m * m)) * h * lc;
+      lam[2] += g * mp * lc;
+      c.grad(0, Gv * lc);
+      c.grad(1, (g * Gv) * lr);
+    }
+    // The step overwrote i_Ca: the adjoint of its previous value starts from zero.
+    lam[12] = T(0);
+
+    // VJPs of the updates, last channel first, restoring the state as it goes.
+    auto gate_back = [&](int s, T old, T e, T d) {
+      x[s] = old;
+      const T ln = lam[s];
+      lam[s] = e * ln;
+      c.lv += d * ln;
+    };
+    gate_back(11, o11, e11, n11.d);
+    gate_back(10, o10, e10, n10.d);
+    gate_back(9, o9, e9, n9.d);
+    gate_back(8, o8, e8, n8.d);
+    x[5] = o5;
+    {  // CaPump
+      const T cai = x[5], ica = x[12];
+      const T gamma = p[9], decay = p[10], depth = p[11];
+      const T F2 = T(2) * T(96485);
+      T drive;
+      const T cai_inf = pump_target(x, p, drive);
+      const T arg = -dt / decay;
+      const T em1 = save_expm1(arg);
+      const T ee = T(1) + em1;
+      const T lnew = lam[5];
+      const T l_inf = -em1 * lnew;
+      const T l_ee = (cai - cai_inf) * lnew;
+      const T l_drive = decay * l_inf;
+      lam[5] = ee * lnew;
+      lam[12] += T(-10000.0) * gamma / (F2 * depth) * l_drive;
+      const T l_decay = drive * l_inf + (arg > T(20) ? T(0) : l_ee * ee * dt / (decay * decay));
+      c.grad(9, T(-10000.0) * ica / (F2 * depth) * l_drive);
+      c.grad(10, l_decay);
+      c.grad(11, -drive / depth * l_drive);
+      c.grad(12, l_inf);
+    }
+    x[6] = o6;
+    {  // CaNernstReversal
+      const T le = lam[6];
+      lam[6] = T(0);
+      lam[5] += -C / x[5] * le;
+      lam[7] += C / x[7] * le;
+    }
+    x[4] = o4;
+    {  // SKE2
+      const T lz = lam[4];
+      lam[4] = dx4 * lz;
+      lam[5] += dy4 * lz;
+    }
+    gate_back(3, o3, e3, n3.d);
+    gate_back(2, o2, e2, n2.d);
+    gate_back(1, o1, e1, n1.d);
+  }
+};
+
 template <typename T> using ProgL5pcDend = Program<T, CH_NATS2T, CH_SKV3_1, CH_M, CH_H, CH_LEAK>;
 
 }  // namespace jxb

@@ -440,6 +440,10 @@ __device__ __forceinline__ void node_channels(const SimSmem<T>& sm, int j, T* x,
       ProgHH<T>::forward(x, pn, dt, lin, cst);
       return;
     }
+    if (prog == PROG_L5PC_SOMA) {
+      ProgL5pcSoma<T>::forward(x, pn, dt, lin, cst);
+      return;
+    }
   }
   if (mode == 2) {
     for (int q = e0; q < e1; ++q) channel_steady<T>(sm.ents[q], x, v);
@@ -673,6 +677,8 @@ __device__ __forceinline__ void node_adjoint(const SimSmem<T>& sm, int j, T* x, 
     AdjCtx<T> c{lam, pb, pk, ga, lr, x1, lv};
     if (prog == PROG_L5PC_DEND)
       ProgL5pcDend<T>::adjoint(x, pn, dt, c);
+    else if (prog == PROG_L5PC_SOMA)
+      ProgL5pcSoma<T>::adjoint(x, pn, dt, c);
     else
       ProgHH<T>::adjoint(x, pn, dt, c);
     lv = c.lv;

@@ -336,9 +336,35 @@ PROGRAMS = {
 }
 
 
+# The somatic L5PC program (ProgL5pcSoma) shares calcium slots between channels; a
+# class runs it only with exactly this layout: (channel, state slots, parameter
+# count, first parameter, current slot) per entry, node-relative.
+SOMA_LAYOUT = [
+    ("NaTs2T", (1, 2), 2, 0, -1), ("SKv3_1", (3,), 2, 2, -1), ("SKE2", (4, 5), 2, 4, -1),
+    ("CaNernstReversal", (6, 5, 7), 3, 6, 12), ("CaPump", (5,), 4, 9, 12),
+    ("CaHVA", (8, 9, 6), 1, 13, 12), ("CaLVA", (10, 11, 6), 1, 14, 12), ("Leak", (), 2, 15, -1),
+]
+PROG_L5PC_SOMA = 3
+
+
+def _is_soma_layout(ents: np.ndarray) -> bool:
+    if len(ents) != len(SOMA_LAYOUT):
+        return False
+    for e, (name, slots, npar, p0, cur) in zip(ents, SOMA_LAYOUT):
+        if int(e[0]) != SPECS[name].type_id or int(e[1]) != len(slots) or int(e[2]) != npar:
+            return False
+        if int(e[3]) != cur or int(e[10]) != p0:
+            return False
+        if any(int(e[4 + q]) != s for q, s in enumerate(slots)):
+            return False
+    return True
+
+
 def program_of(ents: np.ndarray) -> int:
     if len(ents) == 0:
         return 0
+    if _is_soma_layout(ents):
+        return PROG_L5PC_SOMA
     prog = PROGRAMS.get(tuple(int(e[0]) for e in ents), 0)
     if not prog:
         return 0

@@ -88,3 +88,14 @@ def test_float32_expm1_series_bound():
     ref = np.expm1(x.astype(np.float64))
     rel = np.abs(got - ref) / np.maximum(np.abs(ref), 1e-300)
     assert rel.max() < 1e-6, rel.max()
+
+
+def test_somatic_program_needs_its_exact_layout():
+    # the L5PC soma class runs the compile-time somatic program only with the slot
+    # layout it was written for; extra current slots send it back to the interpreter
+    from jaxley_pytorch_b200 import synth
+    from jaxley_pytorch_b200.lower import PROG_L5PC_SOMA, lower as lower_
+
+    prob = synth.config_l5pc_tree(batch=1, n_steps=10, seed=0, scale_seed=1)
+    assert PROG_L5PC_SOMA in set(int(p) for p in lower_(prob, keep_currents=False).cls_prog)
+    assert PROG_L5PC_SOMA not in set(int(p) for p in lower_(prob, keep_currents=True).cls_prog)
