@@ -806,6 +806,33 @@ __device__ __forceinline__ void block_solve_pivots(const JxbBlock& blk, const Si
   }
 }
 
+// Asynchronous element copies global -> shared (cp.async, 4 or 8 bytes: the rows
+// are only element-aligned), committed as one group and awaited with
+// cp_async_wait_all before a barrier.
+template <typename T>
+__device__ __forceinline__ void cp_async_elem(T* smem_dst, const T* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  if constexpr (sizeof(T) == 4)
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
+  else
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Stages the item's rows of a (steps, batch, width) array at `step` (the block's
+// range starting at `off`, `cnt` wide) into shared memory rows of stride `cnt`.
+template <typename T>
+__device__ __forceinline__ void stage_rows_async(T* dst, const T* src, int step, int batch, int width, int off,
+                                                 int cnt, int row0, int rows) {
+  for (int r = 0; r < rows; ++r) {
+    const T* g = src + ((size_t)step * batch + row0 + r) * width + off;
+    T* d = dst + (size_t)r * cnt;
+    for (int q = threadIdx.x; q < cnt; q += blockDim.x) cp_async_elem(d + q, g + q);
+  }
+  cp_async_commit();
+}
+
 // Adjoint launch of one work item (`a`: the problem, `L`: the launch).
 template <typename T, bool GM>
 __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const JxbSimArgs& L, int item_idx,
@@ -846,8 +873,18 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
   const T* rec_grad = (const T*)a.rec_grad;
   const int total = nn * rows;
   const NodeWalk walk(a, blk, rows, item.block);  // the same visits every step
+  // Shared-memory kernels stage each step's pivots (into D, during the previous
+  // step's phase 4, which does not use D) and its states (into st, during phase 1
+  // and the transposed solve, which do not use st) asynchronously, so that the
+  // per-node phases do not wait on global memory.
+  if constexpr (!GM) {
+    stage_rows_async<T>(sm.D, piv, K - 1, a.batch, a.n_nodes, blk.node0, nn, row0, rows);
+    cp_async_wait_all();
+    __syncthreads();
+  }
   for (int step = K - 1; step >= 0; --step) {
     const int t = a.t0 + step;
+    if constexpr (!GM) stage_rows_async<T>(sm.st, traj, step, a.batch, a.n_slots, blk.slot0, ns, row0, rows);
     // Phase 1: recording gradients at t + 1, the pivots of the step's matrix and the
     // right-hand side of the transposed solve.
     for (int w = tid; w < total; w += nthr) {
@@ -862,13 +899,18 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
           if (sl >= 0) lam[sl] += rec_grad[((size_t)(t + 1) * a.batch + b) * a.n_rec + a.rec_col[q]];
         }
       }
-      sm.D[(size_t)r * nn + j] = piv[((size_t)step * a.batch + b) * a.n_nodes + i];
+      if constexpr (GM) sm.D[(size_t)r * nn + j] = piv[((size_t)step * a.batch + b) * a.n_nodes + i];
       sm.S[(size_t)r * nn + j] = lam[0];
     }
     __syncthreads();
     // lambda_r = A^{-T} lambda_v'  (solver_voltage.py:168-187), with the pivots of
     // the forward elimination.
     block_solve_pivots<T>(blk, sm, rows, sm.au, sm.al);
+    if constexpr (!GM) {
+      cp_async_wait_all();  // the step's states
+      __syncthreads();
+      if (step > 0) stage_rows_async<T>(sm.D, piv, step - 1, a.batch, a.n_nodes, blk.node0, nn, row0, rows);
+    }
     // Phase 4: vector-Jacobian products of the step.
     for (int q = 0; q < walk.n; ++q) {
       int r, j;
@@ -877,8 +919,11 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
       T* x = sm.st + (size_t)r * ns + sm.soff[j];
       T* lam = sm.adj + (size_t)r * ns + sm.soff[j];
       const int nslot = (j + 1 < nn ? sm.soff[j + 1] : ns) - sm.soff[j];
-      const T* g = traj + ((size_t)step * a.batch + b) * a.n_slots + blk.slot0 + sm.soff[j];
-      for (int q = 0; q < nslot; ++q) x[q] = g[q];
+      if constexpr (GM) {
+        const T* g = traj + ((size_t)step * a.batch + b) * a.n_slots + blk.slot0 + sm.soff[j];
+        for (int q = 0; q < nslot; ++q) x[q] = g[q];
+      }
+      (void)nslot;
       const T lr = sm.S[(size_t)r * nn + j];
       const T xnew = sm.X1[(size_t)r * nn + j];
       const bool comp = (sm.flags[j] & FLAG_COMP) != 0;
@@ -906,6 +951,7 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
       lam[0] = lv;
       sm.X1[(size_t)r * nn + j] = x[0];
     }
+    if constexpr (!GM) cp_async_wait_all();  // the next step's pivots
     __syncthreads();
   }
   // Fold the nodes' gradient slots into the columns (float64, global), once per
