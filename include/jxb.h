@@ -241,8 +241,10 @@ int jxb_sim_backward(const JxbSimArgs* args, void* stream);
  * be re-entered from a step). The trajectory scratch (args->traj, args->traj_piv are
  * ignored) lives in a fixed 32 MiB device array of the library, held by every GPU
  * that loads it until exit; segments needing more return JXB_ERR_TOO_LARGE. The first
- * call on a device looks up the array's device address (cudaGetSymbolAddress) with
- * that device current and should come before any stream capture. All calls share the
+ * call on a device (and the first after that device's context was reset) looks up the
+ * array's device address (cudaGetSymbolAddress) with that device current and should
+ * come before any stream capture; the look-up is guarded for calls from several host
+ * threads. All calls share the
  * array: calls that overlap on the GPU (other streams, other threads) race. Nothing
  * in the array needs to start at zero: every slot a segment reads was written earlier
  * in the same launch. It calls no cudaMalloc, cudaFree or allocating library routine. */

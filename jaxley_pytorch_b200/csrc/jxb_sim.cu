@@ -1302,7 +1302,55 @@ constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // 32 MiB
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 constexpr int kMaxDevices = 64;
-void* g_noalloc_ptr[kMaxDevices] = {nullptr};  // device address of the array, per device
+
+// Device address of the array per device, together with the context it was looked up
+// in: a context created after cudaDeviceReset loads the array at a new address, so
+// the set-up runs again for it. Guarded by a mutex (calls may come from several host
+// threads).
+struct NoAllocSlot {
+  void* ctx;
+  void* ptr;
+};
+NoAllocSlot g_noalloc_slot[kMaxDevices] = {};
+std::mutex g_noalloc_mu;
+
+typedef int (*CtxGetCurrentFn)(void**);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+std::once_flag g_ctx_fn_once;
+
+// The current context of the calling thread (driver entry point cuCtxGetCurrent,
+// looked up once through the runtime; no link against libcuda).
+void* current_context() {
+  std::call_once(g_ctx_fn_once, [] {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPointByVersion("cuCtxGetCurrent", &fn, 12000, cudaEnableDefault, &q) ==
+            cudaSuccess &&
+        q == cudaDriverEntryPointSuccess)
+      g_ctx_get_current = (CtxGetCurrentFn)fn;
+  });
+  void* ctx = nullptr;
+  if (g_ctx_get_current) g_ctx_get_current(&ctx);
+  return ctx;
+}
+
+// The array's device address on the current device (looked up on the first call in
+// the device's current context).
+cudaError_t noalloc_scratch(int dev, void** out) {
+  void* ctx = current_context();
+  std::lock_guard<std::mutex> lock(g_noalloc_mu);
+  NoAllocSlot& s = g_noalloc_slot[dev];
+  if (!s.ptr || s.ctx != ctx) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+    if (e != cudaSuccess) return e;
+    if (!p) return cudaErrorInvalidSymbol;
+    s.ptr = p;
+    s.ctx = ctx;
+  }
+  *out = s.ptr;
+  return cudaSuccess;
+}
 
 }  // namespace
 
@@ -1327,27 +1375,30 @@ extern "C" int jxb_sim_backward_noalloc(const JxbSimArgs* a, void* stream) {
   }
   int dev = 0;
   cudaError_t e = cudaGetDevice(&dev);
-  if (e != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+  if (e != cudaSuccess) {
     jxb::set_err("cudaGetDevice", e);
     return JXB_ERR_LAUNCH;
   }
-  // One-time set-up per device (the device must be current): the device address of
-  // the array. This first call should happen before any stream capture.
-  if (!g_noalloc_ptr[dev]) {
-    void* p = nullptr;
-    e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
-    if (e != cudaSuccess || !p) {
-      jxb::set_err("cudaGetSymbolAddress", e);
-      return JXB_ERR_LAUNCH;
-    }
-    g_noalloc_ptr[dev] = p;
+  if (dev < 0 || dev >= kMaxDevices) {
+    snprintf(jxb::g_err, sizeof(jxb::g_err),
+             "jxb_sim_backward_noalloc: device %d is beyond the %d devices the library tracks", dev,
+             kMaxDevices);
+    return JXB_ERR_ARG;
+  }
+  // Set-up on the first call per device and context (the device must be current):
+  // the device address of the array. That call should come before any stream capture.
+  void* scratch = nullptr;
+  e = noalloc_scratch(dev, &scratch);
+  if (e != cudaSuccess) {
+    jxb::set_err("cudaGetSymbolAddress", e);
+    return JXB_ERR_LAUNCH;
   }
   // The caller's trajectory pointers are ignored; the rest is checked and launched
   // as by jxb_sim_backward.
   JxbSimArgs b = *a;
   b.traj_stored = 0;  // the segment is recomputed into the library's array
-  b.traj = g_noalloc_ptr[dev];
-  b.traj_piv = (unsigned char*)g_noalloc_ptr[dev] + piv_off;
+  b.traj = scratch;
+  b.traj_piv = (unsigned char*)scratch + piv_off;
   const int rc = jxb::check_sim_args(&b, true);
   if (rc != JXB_OK) return rc;
   if (b.dtype == JXB_F32) return jxb::launch_sim<float>(b, true, (cudaStream_t)stream);

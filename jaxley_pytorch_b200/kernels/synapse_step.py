@@ -22,6 +22,7 @@ import numpy as np
 import torch
 
 from .. import _lib
+from ..lower import presynaptic_lists
 
 KINETIC, SIGMOID_RATE = 0, 1
 _NAMES = {
@@ -38,20 +39,6 @@ def _model_of(synapse_type) -> Optional[int]:
     return {"KineticSynapse": KINETIC, "SigmoidRateSynapse": SIGMOID_RATE}.get(cls)
 
 
-def _transposed_index(pre: np.ndarray):
-    """`(nodes, inv)`: the presynaptic nodes (sorted) and, as `(len(nodes), width)`
-    int32, the synapses of every presynaptic node padded with -1
-    (`synapse_step.py:66-76`)."""
-    nodes, local = np.unique(pre, return_inverse=True)
-    counts = np.bincount(local, minlength=len(nodes))
-    order = np.argsort(local, kind="stable")
-    starts = np.r_[0, np.cumsum(counts)[:-1]]
-    rows = local[order]
-    inv = np.full((len(nodes), max(int(counts.max()), 1)), -1, dtype=np.int32)
-    inv[rows, np.arange(len(pre)) - starts[rows]] = order
-    return nodes.astype(np.int32), inv
-
-
 def kernel_plan(synapse_type, pre: np.ndarray, targets: np.ndarray, n_nodes: int, device) -> Dict:
     """Plan entries of the kernels (empty when they do not apply, `synapse_step.py:79-103`)."""
     if torch.device(device).type != "cuda" or os.environ.get("JAXLEY_PYTORCH_SYNAPSE_KERNEL", "auto") == "off":
@@ -61,7 +48,7 @@ def kernel_plan(synapse_type, pre: np.ndarray, targets: np.ndarray, n_nodes: int
         return {}
     name = getattr(synapse_type, "_name", None) or getattr(synapse_type, "name")
     pre = np.asarray(pre)
-    nodes, inv = _transposed_index(pre)
+    nodes, inv = presynaptic_lists(pre)
     return {
         "kernel_model": model,
         "kernel_params": [f"{name}_{p}" for p in _NAMES[model]],
@@ -73,10 +60,12 @@ def kernel_plan(synapse_type, pre: np.ndarray, targets: np.ndarray, n_nodes: int
 
 
 def kernel_scalars(delta_t: float, diff: float, dtype, device) -> torch.Tensor:
-    """`[delta_t, diff]` filled on the device (no host-to-device copy, capturable)."""
-    scalars = torch.full((2,), diff, dtype=dtype, device=device)
-    scalars[:1].fill_(delta_t)
-    return scalars
+    """`[delta_t, diff]` as a device tensor. Each value is written by a fill on the
+    device and the two are stacked there, so no host-to-device copy is issued and
+    the call can run inside a CUDA-graph capture."""
+    dt_t = torch.full((), float(delta_t), dtype=dtype, device=device)
+    diff_t = torch.full((), float(diff), dtype=dtype, device=device)
+    return torch.stack((dt_t, diff_t))
 
 
 def _code(t):
@@ -216,31 +205,44 @@ def _define_in(ns: str):
         g_s = torch.empty_like(s) if model == KINETIC else v.new_empty(0)
         return torch.empty_like(v), g_s, v.new_empty(bin(need).count("1"), pre.shape[0])
 
-    def _setup(ctx, inputs, output):
-        (v, s, pre, targets, p0, p1, p2, p3, p4, p5, area, scalars, inv, nodes, k, model, tan,
-         store) = inputs
-        ctx.save_for_backward(v, s, pre, targets, p0, p1, p2, p3, p4, p5, area, scalars, inv, nodes)
-        ctx.k, ctx.model, ctx.tan = k, model, tan
+    # Autograd of the forward op: the 18 inputs are (v, s, pre, targets, p0..p5,
+    # area, scalars, inv, pre_nodes, k, model, targets_are_nodes, store_current);
+    # gradients flow to v, to the kinetic state and to the parameters that ask for
+    # them, whose rows the backward op returns in parameter order.
+    n_inputs = 18
 
-    def _bw(ctx, g_s_new, g_current, g_lin, g_const):
-        v, s, pre, targets, p0, p1, p2, p3, p4, p5, area, scalars, inv, nodes = ctx.saved_tensors
-        n_params = 6 if ctx.model == KINETIC else 3
-        need = sum(1 << i for i in range(n_params) if ctx.needs_input_grad[4 + i])
-        B, T = v.shape[0], pre.shape[0] // ctx.k
-        empty = v.new_empty(0)
-        has_gs = ctx.model == KINETIC and g_s_new is not None
-        has_gc = g_current is not None and g_current.numel() > 0
-        g_lin = g_lin.contiguous() if g_lin is not None else v.new_zeros(B, T)
-        g_const = g_const.contiguous() if g_const is not None else v.new_zeros(B, T)
-        g_v, g_s, g_params = _bop(v, s, pre, targets, p0, p1, p2, p3, p4, p5, area, scalars, inv,
-                                  nodes, g_s_new.contiguous() if has_gs else empty,
-                                  g_current.contiguous() if has_gc else empty, g_lin, g_const,
-                                  ctx.k, ctx.model, ctx.tan, has_gs, has_gc, need)
-        rows = [bin(need & ((1 << i) - 1)).count("1") for i in range(6)]
-        g_p = [g_params[rows[i]] if need & (1 << i) else None for i in range(6)]
-        return (g_v, g_s if ctx.model == KINETIC else None, None, None, *g_p) + (None,) * 8
+    def _save(ctx, inputs, output):
+        ctx.save_for_backward(*inputs[:14])
+        ctx.k, ctx.model, ctx.tan = inputs[14], inputs[15], inputs[16]
 
-    _op.register_autograd(_bw, setup_context=_setup)
+    def _grad(ctx, g_s_new, g_current, g_lin, g_const):
+        saved = ctx.saved_tensors
+        v, pre = saved[0], saved[2]
+        kinetic = ctx.model == KINETIC
+        wanted = [q for q in range(len(_NAMES[ctx.model])) if ctx.needs_input_grad[4 + q]]
+        need = 0
+        for q in wanted:
+            need |= 1 << q
+        shape_post = (v.shape[0], pre.shape[0] // ctx.k)
+        none = v.new_empty(0)
+        use_s = kinetic and g_s_new is not None
+        use_cur = g_current is not None and g_current.numel() > 0
+        g_v, g_s, g_rows = _bop(
+            *saved,
+            g_s_new.contiguous() if use_s else none,
+            g_current.contiguous() if use_cur else none,
+            v.new_zeros(shape_post) if g_lin is None else g_lin.contiguous(),
+            v.new_zeros(shape_post) if g_const is None else g_const.contiguous(),
+            ctx.k, ctx.model, ctx.tan, use_s, use_cur, need)
+        grads = [None] * n_inputs
+        grads[0] = g_v
+        if kinetic:
+            grads[1] = g_s
+        for row, q in enumerate(wanted):
+            grads[4 + q] = g_rows[row]
+        return tuple(grads)
+
+    _op.register_autograd(_grad, setup_context=_save)
     synapse_step_op = _op
     synapse_step_backward_op = _bop
 
@@ -257,44 +259,63 @@ def _ensure_ops():
     raise RuntimeError("could not register the synapse ops")
 
 
+def _scatter_to_nodes(per_target: torch.Tensor, targets: torch.Tensor, n: int) -> torch.Tensor:
+    """`(rows, n)` node array holding `per_target (rows, T)` at the target nodes and
+    zero elsewhere (the regular layout has distinct targets)."""
+    out = per_target.new_zeros(per_target.shape[0], n)
+    idx = targets.to(torch.long).reshape(1, -1).expand(per_target.shape[0], -1)
+    return out.scatter_add_(1, idx, per_target)
+
+
 def fused_step(states: Dict, delta_t: float, sp: Dict, gp: Dict) -> Optional[tuple]:
-    """`Network._step_regular_synapses` with the fused kernels
-    (reference `synapse_step.py:451-498`): returns `(states, (lin, -const))` on the
-    nodes, or `None` when the plan has no kernel entries."""
+    """`Network._step_regular_synapses` on the CUDA kernels (the reference's entry,
+    `kernels/synapse_step.py:451-498`, called at `modules/network.py:402-407`).
+
+    Returns `(states, (slope, offset))` with node arrays of the synapse type's
+    summed slope and offset (the offset with the sign the caller adds), or `None`
+    when the kernels do not apply: no kernel entries in the plan, voltages not on a
+    CUDA device or not float32/float64, parameters or areas that are not one value
+    per synapse on that device, a trainable area, or a kinetic state of another
+    shape. The caller then runs its own code, as with the reference."""
     if "kernel_model" not in sp or "kernel_scalars" not in gp:
         return None
-    _ensure_ops()
     v = states["v"]
+    if not v.is_cuda or v.dtype not in (torch.float32, torch.float64) or v.dim() == 0:
+        return None
     model = sp["kernel_model"]
-    num_targets, k = sp["pre_per_target"].shape
-    num_syn = num_targets * k
-    params = [gp["params"][name] for name in sp["kernel_params"]]
-    area = gp["area_post"]
-    params = [torch.broadcast_to(torch.as_tensor(p, dtype=v.dtype, device=v.device), (num_syn,))
-              for p in params]
-    params += [params[0]] * (6 - len(params))
-    batch, n = v.shape[:-1], v.shape[-1]
-    name = sp["synapse_name"] if "synapse_name" in sp else sp["synapse"]._name
-    state = f"{name}_s"
+    n_targets, k = sp["pre_per_target"].shape
+    E = n_targets * k
+    per_syn = [gp["params"][name] for name in sp["kernel_params"]] + [gp["area_post"]]
+    for p in per_syn:
+        if not isinstance(p, torch.Tensor) or tuple(p.shape) != (E,) or p.device != v.device:
+            return None
+    if gp["area_post"].requires_grad:
+        return None
+    lead, n = tuple(v.shape[:-1]), v.shape[-1]
+    name = sp["synapse"]._name if "synapse" in sp else sp["synapse_name"]
+    state_key, current_key = f"{name}_s", f"i_{name}"
     if model == KINETIC:
-        s = states[state].reshape(-1, num_syn).contiguous()
+        s = states[state_key]
+        if tuple(s.shape) != lead + (E,):
+            return None
+        s = s.reshape(-1, E).contiguous()
     else:
         s = v.new_empty(0)
-    store = gp.get("store_current", True)
-    s_new, current, lin, const = synapse_step_op(
-        v.reshape(-1, n).contiguous(), s, sp["kernel_pre"], sp["kernel_targets"], *params,
-        torch.broadcast_to(area, (num_syn,)).to(v.dtype).contiguous(), gp["kernel_scalars"],
-        sp["kernel_inv"], sp["kernel_pre_nodes"], k, model, sp["targets_are_nodes"], store,
-    )
-    states = dict(states)
+    _ensure_ops()
+    cast = [p.to(v.dtype).contiguous() for p in per_syn]
+    area = cast.pop()
+    six = cast + [cast[0]] * (6 - len(cast))  # unused slots of SigmoidRateSynapse
+    keep_current = bool(gp.get("store_current", True))
+    s_new, current, slope, offset = synapse_step_op(
+        v.reshape(-1, n).contiguous(), s, sp["kernel_pre"], sp["kernel_targets"], *six, area,
+        gp["kernel_scalars"], sp["kernel_inv"], sp["kernel_pre_nodes"], k, model,
+        sp["targets_are_nodes"], keep_current)
+    new_states = {**states}
     if model == KINETIC:
-        states[state] = s_new.reshape(*batch, num_syn)
-    if store:
-        states[f"i_{name}"] = current.reshape(*batch, num_syn)
-    lin = lin.reshape(*batch, lin.shape[-1])
-    const = const.reshape(*batch, const.shape[-1])
-    if sp["targets_are_nodes"]:
-        return states, (lin, -const)
-    zeros = torch.zeros_like(v)
-    targets = sp["targets"]
-    return states, (zeros.index_add(-1, targets, lin), zeros.index_add(-1, targets, -const))
+        new_states[state_key] = s_new.view(lead + (E,))
+    if keep_current:
+        new_states[current_key] = current.view(lead + (E,))
+    if not sp["targets_are_nodes"]:
+        slope = _scatter_to_nodes(slope, sp["targets"], n)
+        offset = _scatter_to_nodes(offset, sp["targets"], n)
+    return new_states, (slope.view(lead + (slope.shape[-1],)), -offset.view(lead + (offset.shape[-1],)))

@@ -178,6 +178,34 @@ def _unique_rows(a: np.ndarray):
     return b[new], srt[new], inv
 
 
+def presynaptic_lists(pre: np.ndarray) -> Tuple[np.ndarray, np.ndarray]:
+    """Outgoing synapses of every presynaptic node, for the backward pass of the
+    synapse step (the sum of the presynaptic voltage gradients without atomics).
+
+    The synapses are sorted by presynaptic node (stably, so a node keeps its
+    synapses in index order); a node's run in that order becomes one row, its rank
+    inside the run the column. Returns `(nodes, lists)`: the distinct presynaptic
+    nodes in increasing order (int32) and `lists (len(nodes), width)` int32, the
+    synapse indices of every node followed by -1 up to `width`, the largest
+    out-degree (at least 1)."""
+    pre = np.asarray(pre, dtype=np.int64).reshape(-1)
+    E = len(pre)
+    if E == 0:
+        return np.zeros(0, np.int32), np.full((0, 1), -1, np.int32)
+    by_node = np.argsort(pre, kind="stable")
+    sorted_pre = pre[by_node]
+    run_start = np.empty(E, dtype=bool)
+    run_start[0] = True
+    run_start[1:] = sorted_pre[1:] != sorted_pre[:-1]
+    row = np.cumsum(run_start) - 1
+    # position of the first synapse of the run, carried forward over the run
+    first = np.maximum.accumulate(np.where(run_start, np.arange(E), 0))
+    col = np.arange(E) - first
+    lists = np.full((int(row[-1]) + 1, int(col.max()) + 1), -1, dtype=np.int32)
+    lists[row, col] = by_node
+    return sorted_pre[run_start].astype(np.int32), lists
+
+
 def _pointer_jump(ptr: np.ndarray, dist: np.ndarray):
     """List ranking: follow `ptr` to its fixed point, summing `dist` on the way."""
     while True:

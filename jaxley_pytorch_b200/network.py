@@ -27,7 +27,8 @@ import numpy as np
 import torch
 
 from . import _lib
-from .kernels.synapse_step import KINETIC, _transposed_index
+from .kernels.synapse_step import KINETIC
+from .lower import presynaptic_lists
 from .problem import Problem, SynapseType
 from .sim import Simulation
 
@@ -46,7 +47,7 @@ class _SynType:
         n2i = np.asarray(low.node2int, dtype=np.int64)
         pre_slot = soff[n2i[np.asarray(syn.pre, dtype=np.int64)]].astype(np.int32)
         tgt_slot = soff[n2i[np.asarray(syn.targets, dtype=np.int64)]].astype(np.int32)
-        nodes, inv = _transposed_index(pre_slot)
+        nodes, inv = presynaptic_lists(pre_slot)
         i32 = lambda x: torch.as_tensor(np.ascontiguousarray(x), dtype=torch.int32, device=device)  # noqa: E731
         self.pre = i32(pre_slot)
         self.targets = i32(tgt_slot)

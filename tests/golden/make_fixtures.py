@@ -1,8 +1,8 @@
 """Generate the parity fixtures under tests/golden/ by running the reference.
 
-Run in a container that has jaxley-pytorch's sources at /root/reference:
+Run with the path of a jaxley-pytorch source tree in JXB_REFERENCE:
 
-    python tests/golden/make_fixtures.py
+    JXB_REFERENCE=<path to jaxley-pytorch> python tests/golden/make_fixtures.py [which ...]
 
 The reference imports matplotlib at module level for plotting only; a stand-in
 package (`tests/golden/_mpl_stub`) takes its place. Every fixture is an npz written by
@@ -16,7 +16,9 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 REPO = os.path.dirname(os.path.dirname(HERE))
-REFERENCE = os.environ.get("JXB_REFERENCE", "/root/reference")
+REFERENCE = os.environ.get("JXB_REFERENCE")
+if not REFERENCE:
+    raise SystemExit("set JXB_REFERENCE to the path of a jaxley-pytorch source tree")
 sys.path.insert(0, os.path.join(HERE, "_mpl_stub"))
 sys.path.insert(0, REFERENCE)
 sys.path.insert(0, REPO)

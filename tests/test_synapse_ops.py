@@ -9,6 +9,7 @@ import torch
 
 import oracle
 from jaxley_pytorch_b200.kernels import synapse_step as ss
+from jaxley_pytorch_b200.lower import presynaptic_lists
 
 pytestmark = pytest.mark.gpu
 
@@ -42,7 +43,7 @@ def make(model, k, B, targets_are_nodes, seed=0):
 
 def torch_args(c, model, dev, dtype=torch.float64):
     t = lambda a: torch.as_tensor(a, dtype=dtype, device=dev)  # noqa: E731
-    nodes, inv = ss._transposed_index(c["pre"])
+    nodes, inv = presynaptic_lists(c["pre"])
     params = [t(p) for p in c["params"]] + [t(c["params"][0])] * (6 - len(c["params"]))
     return dict(
         v=t(c["v"]), s=t(c["s"]) if model == 0 else torch.empty(0, dtype=dtype, device=dev),
