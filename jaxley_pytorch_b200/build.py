@@ -5,6 +5,7 @@ import glob
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 _HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(_HERE)
@@ -31,8 +32,29 @@ def _nvcc() -> str:
     return cand if os.path.exists(cand) else "nvcc"
 
 
+INST = "jxb_sim_inst.cu"  # compiled once per (element type, kind, CTA size class)
+
+
 def sources():
     return sorted(glob.glob(os.path.join(CSRC, "*.cu")))
+
+
+def units():
+    """`(source, object, extra flags)` of every compilation unit."""
+    out = []
+    for src in sources():
+        base = os.path.basename(src)[:-3]
+        if os.path.basename(src) != INST:
+            out.append((src, os.path.join(OUT_DIR, base + ".o"), []))
+            continue
+        for tname, tag in (("float", "f32"), ("double", "f64")):
+            for bwd, kind in ((0, "fwd"), (1, "bwd")):
+                for nt in (256, 512, 1024):
+                    fn = f"sim_kernel_{tag}_{kind}_{nt}"
+                    out.append((src, os.path.join(OUT_DIR, f"{base}_{tag}_{kind}_{nt}.o"),
+                                [f"-DJXB_INST_T={tname}", f"-DJXB_INST_BWD={bwd}",
+                                 f"-DJXB_INST_NT={nt}", f"-DJXB_INST_FN={fn}"]))
+    return out
 
 
 def headers():
@@ -50,15 +72,21 @@ def build(force: bool = False, verbose: bool = False, extra=()) -> str:
     if not force and up_to_date():
         return LIB
     os.makedirs(OUT_DIR, exist_ok=True)
-    objs = []
-    for src in sources():
-        obj = os.path.join(OUT_DIR, os.path.basename(src)[:-3] + ".o")
-        cmd = [_nvcc(), *NVCC_FLAGS, *extra, "-I", os.path.join(ROOT, "include"), "-I", CSRC,
+    jobs = []
+    for src, obj, flags in units():
+        cmd = [_nvcc(), *NVCC_FLAGS, *extra, *flags, "-I", os.path.join(ROOT, "include"), "-I", CSRC,
                "-c", src, "-o", obj]
         if verbose:
             print(" ".join(cmd))
-        subprocess.run(cmd, check=True)
-        objs.append(obj)
+        jobs.append(cmd)
+    with ThreadPoolExecutor(max_workers=max(1, os.cpu_count() or 1)) as pool:
+        for r in pool.map(lambda c: subprocess.run(c, capture_output=True, text=True), jobs):
+            if verbose or r.returncode:
+                sys.stdout.write(r.stdout)
+                sys.stderr.write(r.stderr)
+            if r.returncode:
+                raise subprocess.CalledProcessError(r.returncode, r.args)
+    objs = [obj for _, obj, _ in units()]
     tmp = LIB + ".tmp"
     cmd = [_nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", tmp,
            "-lcudart"]
