@@ -93,6 +93,7 @@ class Lowered:
     pscale: np.ndarray  # (B, n_cols)
     col_info: List[Tuple[str, int]]  # (param name, reference node of first use) per column
     col_members: "_ColMembers"  # [col] -> (param name, node, base) of its uses
+    train_cols: np.ndarray  # (n trainable groups,) column of every group (-1 none, -2 several)
     # chains and blocks
     chain_top: np.ndarray
     chain_len: np.ndarray
@@ -558,6 +559,7 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
 
     grp_base: List[np.ndarray] = []
     grp_col: List[np.ndarray] = []
+    group_uses: List[Tuple[np.ndarray, np.ndarray]] = []  # (trainable group, column) per use
     for g in range(G):
         R = int2node[grp_nodes[g]]
         m = len(R)
@@ -586,6 +588,7 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
                 prof = (np.ones((len(idx), B)) if a.ndim == 1
                         else (np.broadcast_to(a[:, R[idx]], (B, len(idx))) / safe[idx]).T)
                 colm[idx, k] = col_ids(b"group|", prof, tag=tg[idx])
+                group_uses.append((tg[idx], colm[idx, k].copy()))
         grp_base.append(base)
         grp_col.append(colm)
 
@@ -617,6 +620,16 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
         col_info.append((grp_pslots[grp_int[i_f]][k_f][1], int(int2node[i_f])))
     col_members = _ColMembers(ncol, new_of[use_c], use_i, use_k, grp_pslots, grp_int,
                               grp_base, row_in_grp, int2node)
+    # The column of every trainable group: -1 if no node of the group has the
+    # parameter, -2 if its nodes span several columns (different batch profiles).
+    n_groups = len(getattr(p, "trainable", []) or [])
+    train_cols = np.full(n_groups, -1, dtype=np.int64)
+    if group_uses:
+        tgs = np.concatenate([t for t, _ in group_uses])
+        cls_ = new_of[np.concatenate([c for _, c in group_uses])]
+        for gi in np.unique(tgs):
+            cs = np.unique(cls_[tgs == gi])
+            train_cols[gi] = cs[0] if len(cs) == 1 else -2
 
     # ---- initial state ----
     L = int(soff[-1])
@@ -763,6 +776,7 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
         pscale=np.ascontiguousarray(pscale),
         col_info=col_info,
         col_members=col_members,
+        train_cols=train_cols,
         chain_top=i32(chain_top),
         chain_len=i32(chain_len),
         chain_ptop=i32(chain_ptop),

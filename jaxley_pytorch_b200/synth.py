@@ -315,7 +315,10 @@ def l5pc_channels(cell: dict, scales: Optional[Dict[str, np.ndarray]] = None, nc
 
 def config_l5pc_tree(batch: int = 256, n_branches: int = 300, ncomp: int = 4, n_steps: int = 4000,
                      seed: int = 0, height_range=(35, 45), stim_amp: float = 0.3,
-                     scale_seed: int = 1) -> Problem:
+                     scale_seed: int = 1, stim_delay: float = 10.0) -> Problem:
+    """The large-batch L5PC-like tree. `prob.meta` keeps what rebuilds the same cell
+    elsewhere: branch parents, lengths and radii, the per-row conductance scales and
+    the stimulus `(delay, duration, amplitude)`."""
     rng = np.random.default_rng(seed)
     for _ in range(1000):
         parents = balanced_random_tree(n_branches, rng)
@@ -338,7 +341,7 @@ def config_l5pc_tree(batch: int = 256, n_branches: int = 300, ncomp: int = 4, n_
     chans = l5pc_channels(cell, scales, ncomp_soma=ncomp)
     t_max = n_steps * 0.025
     prob = assemble([cell], [chans], batch=batch, dt=0.025, n_steps=n_steps, v0=-65.0,
-                    stim=[(0, (0, 0), step_current(10.0, 80.0, stim_amp, 0.025, t_max))],
+                    stim=[(0, (0, 0), step_current(stim_delay, 80.0, stim_amp, 0.025, t_max))],
                     recordings=[("v", 0, (0, 0))])
     prob.states.setdefault("CaCon_e", np.full(prob.n_nodes, 2.0))
     prob.states["CaCon_i"] = np.where(prob.states.get("CaCon_i", np.zeros(prob.n_nodes)) == 0,
@@ -347,7 +350,8 @@ def config_l5pc_tree(batch: int = 256, n_branches: int = 300, ncomp: int = 4, n_
     for k in ["eNa", "eK"]:
         if k in prob.params:
             prob.params[k] = np.full(prob.n_nodes, 50.0 if k == "eNa" else -85.0)
-    prob.meta = {"height": h, "scales": scales}
+    prob.meta = {"height": h, "scales": scales, "parents": parents, "lengths": lengths,
+                 "radius": radius, "ncomp": ncomp, "stim": (stim_delay, 80.0, stim_amp)}
     return prob
 
 
@@ -357,6 +361,7 @@ def config_uneven(n_cells: int = 4096, seed: int = 0, n_steps: int = 2000, min_c
     rng = np.random.default_rng(seed)
     cells, chans, stims, recs = [], [], [], []
     train_local = []  # per cell: [(param name, local node indices)]
+    specs = []  # per cell: what rebuilds it elsewhere
     t_max = n_steps * 0.025
     for c in range(n_cells):
         ncomp_total = int(round(np.exp(rng.uniform(np.log(min_comp), np.log(max_comp)))))
@@ -382,12 +387,17 @@ def config_uneven(n_cells: int = 4096, seed: int = 0, n_steps: int = 2000, min_c
             cl = l5pc_channels(cell, None, ncomp_soma=ncomp)
             chans.append(cl)
             train_local.append([(k, nodes) for _, nodes, _, vals in cl for k in vals if k in L5PC_SCALED])
+            kind = "L5PC"
         else:
             comps = np.nonzero(cell["is_comp"])[0]
             chans.append([("HH", comps, "HH", {})])
             train_local.append([(k, comps) for k in ("HH_gNa", "HH_gK", "HH_gLeak")])
+            kind = "HH"
         delay = float(rng.uniform(1, 5))
         amp = float(rng.uniform(0.05, 0.5))
+        specs.append({"parents": parents, "ncomp": ncomp, "radius": radius, "lengths": lengths,
+                      "kind": kind, "stim": (delay, 1.0, amp),
+                      "train": [k for k, _ in train_local[-1]]})
         stims.append((c, (0, 0), step_current(delay, 1.0, amp, 0.025, t_max)))
         recs.append(("v", c, (0, 0)))
     prob = assemble(cells, chans, batch=1, dt=0.025, n_steps=n_steps, v0=-65.0, stim=stims,
@@ -399,4 +409,5 @@ def config_uneven(n_cells: int = 4096, seed: int = 0, n_steps: int = 2000, min_c
         prob.states["CaCon_i"] = np.where(prob.states["CaCon_i"] == 0, 5e-05, prob.states["CaCon_i"])
     if "CaCon_e" in prob.states:
         prob.states["CaCon_e"] = np.where(prob.states["CaCon_e"] == 0, 2.0, prob.states["CaCon_e"])
+    prob.meta = {"cells": specs}
     return prob
