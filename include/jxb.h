@@ -75,13 +75,15 @@ int jxb_tree_solve_levels(int dtype, const void* d, const void* l, const void* u
                           const void* s, void* x, int64_t batch,
                           const JxbTreeSchedule* sched, void* stream);
 
-/* Register variant: every warp solves one block of whole trees of at most
- * 32 * regs_per_lane nodes for one batch row, the block held in registers and the
- * parent/child exchanges done with warp shuffles. */
+/* Register variant: every block of whole trees of at most 32 * regs_per_lane nodes
+ * is held in registers for one batch row. Up to 256 nodes (regs_per_lane <= 8) one
+ * warp solves it with warp shuffles for the parent/child exchanges; from 512 to 8192
+ * nodes (regs_per_lane 16 .. 256) a CTA of 4 * regs_per_lane threads, 8 nodes a
+ * thread, exchanges through shared memory. */
 typedef struct {
   int32_t n_nodes;
   int32_t n_blocks;
-  int32_t regs_per_lane;      /* 1, 2, 4 or 8 */
+  int32_t regs_per_lane;      /* power of two, 1 .. 256: block width / 32 */
   int32_t num_slots;          /* max children per node */
   const int32_t* block_info;  /* (n_blocks, 4): start, length, height, depth of the block */
   const int32_t* rel_parent;  /* (n_blocks, 32*regs) parent (block-relative), self for roots */
@@ -230,6 +232,20 @@ typedef struct JxbSimArgs_ {
   const int32_t* syn_rs;
   void* g_syn_lin;
   void* g_syn_const;
+  /* Clamps (optional; modules/base.py:3305-3308 and :3396-3398, fed by data_clamps /
+   * Module.clamp, integrate.py:345-375): for q in [clamp_ptr[i], clamp_ptr[i+1]) of
+   * node i (internal order), after step t the node's state slot clamp_slot[q]
+   * (node-relative) takes clamp[t][b][clamp_col[q]] (the row index b is 0 when
+   * clamp_rows is 1). Slot 0 (v) is set after the voltage solve; the node's last slot
+   * then receives the solve output before the clamp, which the adjoint reads. Other
+   * slots are set after the step's channel update, after the currents were taken.
+   * Entries of one node apply in order (the last wins). The adjoint drops the
+   * gradient of every clamped value. */
+  const int32_t* clamp_ptr;   /* (n_nodes+1,) or null */
+  const int32_t* clamp_slot;
+  const int32_t* clamp_col;
+  const void* clamp;          /* (clamp_steps, clamp_rows, n_clamp) */
+  int32_t n_clamp, clamp_steps, clamp_rows, pad6;
 } JxbSimArgs;
 
 int jxb_sim_forward(const JxbSimArgs* args, void* stream);

@@ -75,6 +75,8 @@ class JxbSimArgs(C.Structure):
         ("gacc", _p), ("gacc_stride", C.c_int64),
         ("multi", _p), ("multi_items", _p),
         ("syn_ptr", _p), ("syn_off", _p), ("syn_rs", _p), ("g_syn_lin", _p), ("g_syn_const", _p),
+        ("clamp_ptr", _p), ("clamp_slot", _p), ("clamp_col", _p), ("clamp", _p),
+        ("n_clamp", C.c_int32), ("clamp_steps", C.c_int32), ("clamp_rows", C.c_int32), ("pad6", C.c_int32),
     ]
 
 

@@ -167,6 +167,13 @@ static int check_sim_args(const JxbSimArgs* a, bool backward) {
     snprintf(g_err, sizeof(g_err), "ckpt_every must be positive");
     return JXB_ERR_ARG;
   }
+  if (a->clamp_ptr && (!a->clamp_slot || !a->clamp_col || !a->clamp || a->n_clamp <= 0 ||
+                       (a->clamp_rows != 1 && a->clamp_rows < a->batch) ||
+                       (a->mode == 0 && a->t0 + a->n_steps > a->clamp_steps))) {
+    snprintf(g_err, sizeof(g_err),
+             "clamps: index arrays, values of 1 or batch rows and at least t0 + n_steps time steps needed");
+    return JXB_ERR_ARG;
+  }
   if ((a->syn_lin == nullptr) != (a->syn_const == nullptr)) return JXB_ERR_ARG;
   if (a->syn_lin && a->n_steps != 1) {
     snprintf(g_err, sizeof(g_err), "synaptic terms require one step per launch");

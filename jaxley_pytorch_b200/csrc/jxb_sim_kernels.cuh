@@ -19,6 +19,8 @@ void set_err(const char* what, cudaError_t e);
 
 constexpr int kMaxWrites = 24;  // undo-log entries of one node's channel updates
 constexpr int FLAG_COMP = 1, FLAG_STIM = 2, FLAG_REC = 4;
+constexpr int FLAG_CLAMP = 8;   // the node has clamp entries
+constexpr int FLAG_VCLAMP = 16; // one of them clamps v (its last slot holds the unclamped v)
 
 constexpr int kManyKids = 1 << 30;  // chain descriptor flag: more than two child chains
 
@@ -125,6 +127,11 @@ __device__ __forceinline__ void stage_item(const JxbSimArgs& a, const JxbBlock& 
     unsigned char f = comp ? FLAG_COMP : 0;
     if (a.stim_ptr[i + 1] > a.stim_ptr[i]) f |= FLAG_STIM;
     if (a.n_rec > 0 && a.rec_ptr[i + 1] > a.rec_ptr[i]) f |= FLAG_REC;
+    if (a.clamp_ptr && a.clamp_ptr[i + 1] > a.clamp_ptr[i]) {
+      f |= FLAG_CLAMP;
+      for (int q = a.clamp_ptr[i]; q < a.clamp_ptr[i + 1]; ++q)
+        if (a.clamp_slot[q] == 0) f |= FLAG_VCLAMP;
+    }
     sm.flags[j] = f;
     const int pa = a.parent[i];
     sm.par[j] = (short)(pa >= 0 ? pa - node0 : -1);
@@ -461,6 +468,48 @@ __device__ __forceinline__ T stim_current(const JxbSimArgs& a, int i, int b, int
   return acc;
 }
 
+// Clamp value of entry q for batch row b after step t.
+template <typename T>
+__device__ __forceinline__ T clamp_value(const JxbSimArgs& a, int q, int b, int t) {
+  const T* c = (const T*)a.clamp + ((size_t)t * a.clamp_rows + (a.clamp_rows == 1 ? 0 : b)) * a.n_clamp;
+  return c[a.clamp_col[q]];
+}
+
+// Clamps of the non-voltage states of node i after the step's channel update
+// (modules/base.py:3305-3308): the currents of the step were taken before.
+template <typename T>
+__device__ __forceinline__ void clamp_states(const JxbSimArgs& a, int i, T* x, int b, int t) {
+  for (int q = a.clamp_ptr[i]; q < a.clamp_ptr[i + 1]; ++q) {
+    const int sl = a.clamp_slot[q];
+    if (sl > 0) x[sl] = clamp_value<T>(a, q, b, t);
+  }
+}
+
+// Voltage clamps of a block after the solve of step t (modules/base.py:3396-3398):
+// a clamped node keeps the solve output in its last slot and takes the clamp value.
+template <typename T>
+__device__ __forceinline__ void clamp_voltages(const JxbSimArgs& a, const JxbBlock& blk, const SimSmem<T>& sm,
+                                               int row0, int rows, int t) {
+  const int nn = blk.n_nodes, ns = blk.n_slots;
+  for (int w = threadIdx.x; w < nn * rows; w += blockDim.x) {
+    const int r = w / nn, j = w - r * nn;
+    if (!(sm.flags[j] & FLAG_VCLAMP)) continue;
+    const int i = blk.node0 + j;
+    const int last = (j + 1 < nn ? sm.soff[j + 1] : ns) - 1;
+    T& v = sm.V[(size_t)r * nn + j];
+    sm.st[(size_t)r * ns + last] = v;
+    for (int q = a.clamp_ptr[i]; q < a.clamp_ptr[i + 1]; ++q)
+      if (a.clamp_slot[q] == 0) v = clamp_value<T>(a, q, row0 + r, t);
+  }
+}
+
+// Slot holding the value after the solve of node j: the last slot of a
+// voltage-clamped node, else v.
+template <typename T>
+__device__ __forceinline__ int solve_slot(const SimSmem<T>& sm, int j, int nn, int ns) {
+  return (sm.flags[j] & FLAG_VCLAMP) ? (j + 1 < nn ? sm.soff[j + 1] : ns) - sm.soff[j] - 1 : 0;
+}
+
 // Recordings of node i at time index t (integrate.py:53-84).
 template <typename T>
 __device__ __forceinline__ void record_node(const JxbSimArgs& a, int i, const T* x, int b, int t) {
@@ -524,6 +573,11 @@ __device__ __forceinline__ void run_steps(const JxbSimArgs& a, const JxbBlock& b
                                           bool traj_final = false) {
   const int nn = blk.n_nodes, ns = blk.n_slots, np = blk.n_pslots;
   const NodeWalk walk(a, blk, rows, item_block);  // the same visits every step
+  // Whether any node of the block has a voltage clamp (uniform over the CTA).
+  int mine = 0;
+  if (a.clamp_ptr)
+    for (int j = threadIdx.x; j < nn; j += blockDim.x) mine |= sm.flags[j] & FLAG_VCLAMP;
+  const bool vclamps = __syncthreads_or(mine) != 0;
   for (int step = 0; step <= nsteps; ++step) {
     const int t = t0 + step;
     for (int q = 0; q < walk.n; ++q) {
@@ -550,7 +604,7 @@ __device__ __forceinline__ void run_steps(const JxbSimArgs& a, const JxbBlock& b
           node_channels<T>(sm, j, x, sm.pv + (size_t)r * np, dt, 1, lin, cst);
           if (record && (f & FLAG_REC)) record_node<T>(a, i, x, b, t);
         }
-        if (X1) X1[(size_t)r * nn + j] = x[0];
+        if (X1) X1[(size_t)r * nn + j] = (f & FLAG_VCLAMP) ? x[nslot - 1] : x[0];
         continue;
       }
       if (traj) {
@@ -565,6 +619,7 @@ __device__ __forceinline__ void run_steps(const JxbSimArgs& a, const JxbBlock& b
       const T v = x[0];
       T lin, cst;
       node_channels<T>(sm, j, x, sm.pv + (size_t)r * np, dt, 0, lin, cst);
+      if (f & FLAG_CLAMP) clamp_states<T>(a, i, x, b, t);
       if (f & FLAG_STIM) cst += stim_current<T>(a, i, b, t);
       if (a.syn_lin) {
         if (a.syn_ptr) {  // per-target synapse outputs (modules/network.py:402-407)
@@ -597,6 +652,10 @@ __device__ __forceinline__ void run_steps(const JxbSimArgs& a, const JxbBlock& b
     if (step == nsteps) break;
     __syncthreads();
     block_solve<T>(blk, sm, rows, sm.al, sm.au, sm.V);
+    if (vclamps) {
+      clamp_voltages<T>(a, blk, sm, row0, rows, t);
+      __syncthreads();
+    }
   }
   __syncthreads();
 }
@@ -840,7 +899,8 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
     // voltages are those of entry K.
     for (int w = tid; w < nn * rows; w += nthr) {
       const int r = w / nn, j = w - r * nn;
-      sm.X1[(size_t)r * nn + j] = traj[((size_t)K * a.batch + row0 + r) * a.n_slots + blk.slot0 + sm.soff[j]];
+      sm.X1[(size_t)r * nn + j] = traj[((size_t)K * a.batch + row0 + r) * a.n_slots + blk.slot0 + sm.soff[j] +
+                                       solve_slot<T>(sm, j, nn, ns)];
     }
     sm.cm = (T*)a.cm + blk.node0;  // read only
     __syncthreads();
@@ -882,7 +942,8 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
         }
       }
       if constexpr (GM) sm.D[(size_t)r * nn + j] = piv[((size_t)step * a.batch + b) * a.n_nodes + i];
-      sm.S[(size_t)r * nn + j] = lam[0];
+      // a clamped voltage after the step does not depend on the solve
+      sm.S[(size_t)r * nn + j] = (f & FLAG_VCLAMP) ? T(0) : lam[0];
     }
     __syncthreads();
     // lambda_r = A^{-T} lambda_v'  (solver_voltage.py:168-187), with the pivots of
@@ -928,10 +989,15 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
         }
       }
       lam[0] = T(0);
+      if (sm.flags[j] & FLAG_CLAMP) {  // clamped states after the step are constants
+        const int i = blk.node0 + j;
+        for (int q = a.clamp_ptr[i]; q < a.clamp_ptr[i + 1]; ++q)
+          if (a.clamp_slot[q] > 0) lam[a.clamp_slot[q]] = T(0);
+      }
       node_adjoint<T>(sm, j, x, lam, sm.pv + (size_t)r * np,
                       sm.gacc + (size_t)r * gslots, dt, lrs, xnew, lv);
       lam[0] = lv;
-      sm.X1[(size_t)r * nn + j] = x[0];
+      sm.X1[(size_t)r * nn + j] = x[solve_slot<T>(sm, j, nn, ns)];
     }
     if constexpr (!GM) cp_async_wait_all();  // the next step's pivots
     __syncthreads();

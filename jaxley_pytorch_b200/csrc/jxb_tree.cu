@@ -11,10 +11,12 @@
 //            eliminates a chain (a node and its only child) bottom-up, chains of a
 //            level in parallel, one barrier per chain level; back-substitution
 //            top-down. The solution is written back in the caller's order.
-// registers: one warp per block of whole trees (at most 32 * R nodes) and batch
-//            row; node j lives in lane j % 32, register j / 32. Elimination by node
-//            height and back-substitution by depth exchange values with warp
-//            shuffles; warps never synchronise with each other.
+// registers: one warp per block of whole trees (at most 32 * R nodes, R <= 8) and
+//            batch row; node j lives in lane j % 32, register j / 32. Elimination by
+//            node height and back-substitution by depth exchange values with warp
+//            shuffles; warps never synchronise with each other. Blocks of 512 to 8192
+//            nodes (the reference's largest block, kernels/tree_solve.py:42) use one
+//            CTA per block and row instead, exchanging through shared memory.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -233,6 +235,122 @@ __global__ void tree_registers_kernel(const T* __restrict__ d, const T* __restri
   }
 }
 
+// Blocks of more than 256 nodes: one CTA of NT threads per block and batch row,
+// node j in thread j % NT, register j / NT (R registers a thread). The children's
+// eliminated contributions and the parents' solutions are exchanged through shared
+// memory, one barrier pair per height or depth level.
+template <typename T, int R>
+__global__ void tree_registers_cta_kernel(const T* __restrict__ d, const T* __restrict__ l,
+                                          const T* __restrict__ u, const T* __restrict__ s,
+                                          T* __restrict__ x, JxbRegSchedule sc) {
+  extern __shared__ __align__(16) char smem_raw[];
+  const int blk = blockIdx.x;
+  const int64_t row = blockIdx.y;
+  const int tid = threadIdx.x, NT = blockDim.x;
+  const int W = NT * R;
+  T* A = (T*)smem_raw;  // W: lower * upper / pivot of every node
+  T* Bv = A + W;        // W: rhs * upper / pivot, later the solution
+  const int start = sc.block_info[4 * blk + 0];
+  const int len = sc.block_info[4 * blk + 1];
+  const int levels = sc.block_info[4 * blk + 2];
+  const int depth = sc.block_info[4 * blk + 3];
+  const int* par = sc.rel_parent + (size_t)blk * W;
+  const int* hgt = sc.rel_height + (size_t)blk * W;
+  const int* dep = sc.rel_depth + (size_t)blk * W;
+  const int* kid = sc.rel_children + (size_t)blk * sc.num_slots * W;
+  const int64_t base = row * sc.n_nodes + start;
+  T dv[R], sv[R], lv[R], uv[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int j = tid + NT * r;
+    const bool in = j < len;
+    dv[r] = in ? d[base + j] : T(1);
+    sv[r] = in ? s[base + j] : T(0);
+    lv[r] = in ? l[base + j] : T(0);
+    uv[r] = in ? u[base + j] : T(0);
+  }
+  for (int h = 1; h <= levels; ++h) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int j = tid + NT * r;
+      const T f = uv[r] / dv[r];
+      A[j] = lv[r] * f;
+      Bv[j] = sv[r] * f;
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int j = tid + NT * r;
+      if (j < len && hgt[j] == h) {
+        for (int k = 0; k < sc.num_slots; ++k) {
+          const int c = kid[k * W + j];
+          if (c >= 0) {
+            dv[r] -= A[c];
+            sv[r] -= Bv[c];
+          }
+        }
+      }
+    }
+    __syncthreads();
+  }
+  // Back-substitution by depth from the roots; Bv holds the solution of every node
+  // whose depth is done.
+  T xv[R];
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    xv[r] = sv[r] / dv[r];
+    Bv[tid + NT * r] = xv[r];
+  }
+  __syncthreads();
+  for (int k = 1; k <= depth; ++k) {
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int j = tid + NT * r;
+      if (j < len && dep[j] == k) xv[r] = (sv[r] - lv[r] * Bv[par[j]]) / dv[r];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+      const int j = tid + NT * r;
+      if (j < len && dep[j] == k) Bv[j] = xv[r];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int r = 0; r < R; ++r) {
+    const int j = tid + NT * r;
+    if (j < len) x[base + j] = xv[r];
+  }
+}
+
+template <typename T>
+int launch_registers_cta(const void* d, const void* l, const void* u, const void* s, void* x,
+                         int64_t batch, const JxbRegSchedule& sc, cudaStream_t st) {
+  constexpr int R = 8;
+  const int W = 32 * sc.regs_per_lane;  // 512 .. 8192
+  const int threads = W / R;
+  const size_t smem = 2 * sizeof(T) * (size_t)W;
+  if (batch > 65535) {
+    snprintf(g_err, sizeof(g_err), "batch %lld exceeds the grid", (long long)batch);
+    return JXB_ERR_ARG;
+  }
+  cudaError_t e = cudaFuncSetAttribute(tree_registers_cta_kernel<T, R>,
+                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) {
+    set_err("cudaFuncSetAttribute", e);
+    return JXB_ERR_LAUNCH;
+  }
+  dim3 grid(sc.n_blocks, (unsigned)batch);
+  tree_registers_cta_kernel<T, R><<<grid, threads, smem, st>>>((const T*)d, (const T*)l, (const T*)u,
+                                                               (const T*)s, (T*)x, sc);
+  e = cudaGetLastError();
+  if (e != cudaSuccess) {
+    set_err("tree_registers_cta_kernel", e);
+    return JXB_ERR_LAUNCH;
+  }
+  return JXB_OK;
+}
+
 template <typename T, int R>
 int launch_registers_r(const void* d, const void* l, const void* u, const void* s, void* x,
                        int64_t batch, const JxbRegSchedule& sc, cudaStream_t st) {
@@ -258,8 +376,13 @@ int launch_registers(const void* d, const void* l, const void* u, const void* s,
     case 2: return launch_registers_r<T, 2>(d, l, u, s, x, batch, sc, st);
     case 4: return launch_registers_r<T, 4>(d, l, u, s, x, batch, sc, st);
     case 8: return launch_registers_r<T, 8>(d, l, u, s, x, batch, sc, st);
+    case 16:
+    case 32:
+    case 64:
+    case 128:
+    case 256: return launch_registers_cta<T>(d, l, u, s, x, batch, sc, st);
     default:
-      snprintf(g_err, sizeof(g_err), "regs_per_lane must be 1, 2, 4 or 8");
+      snprintf(g_err, sizeof(g_err), "regs_per_lane must be a power of two from 1 to 256");
       return JXB_ERR_ARG;
   }
 }

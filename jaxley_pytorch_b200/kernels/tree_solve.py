@@ -29,7 +29,7 @@ import torch
 from .. import _lib
 from ..lower import block_schedule, chain_table
 
-MAX_BLOCK = 256  # registers variant: 32 lanes x 8 registers
+MAX_BLOCK = 8192  # registers variant: up to 256 nodes in one warp, larger blocks in a CTA
 LEVEL_BLOCK = 4096  # levels variant: nodes per block of trees (shared memory bound)
 
 
@@ -74,8 +74,9 @@ def _pack(roots, ends, max_nodes):
 
 def build_forest_schedule(parent: np.ndarray, max_block: int = MAX_BLOCK) -> Dict[str, np.ndarray]:
     """Schedule of the registers variant: whole trees packed into blocks of at most
-    `max_block` (<= 256) nodes; per block the parent, height, depth and child slots of
-    every node (block-relative), cf. reference `tree_solve.py:45-138`."""
+    `max_block` (<= 8192) nodes; per block the parent, height, depth and child slots
+    of every node (block-relative), cf. reference `tree_solve.py:45-138`. The block
+    width is a power of two: up to 256 one warp holds a block, above it a CTA."""
     parent, roots, ends = _forest(parent)
     if int((ends - roots).max()) > max_block:
         raise ValueError(f"a tree has more than {max_block} nodes: use the levels variant")

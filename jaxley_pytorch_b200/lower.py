@@ -25,6 +25,7 @@ from .channels import SPECS
 from .problem import Problem
 
 ENTRY_SHORTS = 18  # ChanEntry: type, ns, np, cur, s[6], p[8]
+V_SOLVE = "__v_unclamped"  # last slot of a voltage-clamped node: the solve output before the clamp
 
 
 class _SlotNames:
@@ -106,6 +107,10 @@ class Lowered:
     stim_ptr: np.ndarray
     stim_idx: np.ndarray
     stim: Optional[np.ndarray]  # (steps, rows, n_stim) time-major
+    clamp_ptr: np.ndarray  # (n_nodes + 1,) clamp entries of every internal node
+    clamp_slot: np.ndarray  # node-relative slot of an entry (0 = v)
+    clamp_col: np.ndarray  # column of an entry in `clamp`
+    clamp: Optional[np.ndarray]  # (steps, rows, n_clamp) time-major clamp values
     gk: np.ndarray  # (n_pslots,) rank of a trainable parameter in its run, -1 if fixed
     gbase: np.ndarray  # (n_nodes,) first gradient slot of a node (block-relative)
     max_gslots: int  # largest number of gradient slots of a block
@@ -135,6 +140,23 @@ class Lowered:
     @property
     def n_cols(self) -> int:
         return int(self.pscale.shape[1])
+
+    def group_scale(self) -> Tuple[np.ndarray, np.ndarray]:
+        """`(cols, base)` of every trainable group: its column and the base value its
+        nodes share (parameter = base * scale), so that the gradient with respect to
+        the group's value in row b is `pgrad[b, col] / base`. Groups without one
+        column or without one base value get column -1 and base NaN."""
+        cols = np.asarray(self.train_cols, dtype=np.int64)
+        base = np.full(len(cols), np.nan)
+        for g, c in enumerate(cols):
+            if c < 0:
+                continue
+            vals = {round(b, 15) for _, _, b in self.col_members[int(c)]}
+            if len(vals) == 1:
+                base[g] = vals.pop()
+            else:
+                cols[g] = -1
+        return cols, base
 
 
 @dataclass
@@ -461,7 +483,13 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
     for name, r in p.recordings:
         if name in cur_names:
             rec_cur[int(r), cur_names.index(name)] = True
-    keymat = np.concatenate([is_comp[:, None], ch_member, rec_cur], axis=1)
+    # Nodes with a voltage clamp keep the unclamped solve output in one more slot,
+    # their last (the adjoint needs it; the clamped value replaces v).
+    vclamped = np.zeros(n, dtype=bool)
+    for cname, cnodes, _ in getattr(p, "clamps", []) or []:
+        if cname == "v":
+            vclamped[np.asarray(cnodes, dtype=np.int64)] = True
+    keymat = np.concatenate([is_comp[:, None], ch_member, rec_cur, vclamped[:, None]], axis=1)
     _, grp_rep, grp_of_node = _unique_rows(np.packbits(keymat, axis=1))
     readers = {"CaPump"}  # channels whose update reads their current state
     G = len(grp_rep)
@@ -489,6 +517,8 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
                            for cj in chs))
             if need and cn not in names:
                 names.append(cn)
+        if vclamped[r]:
+            names.append(V_SOLVE)
         ents, pslots, pk = [], [], 0
         for ci in chs:
             ch = p.channels[ci]
@@ -696,6 +726,39 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
     blocks = [[n0, n1 - n0, int(soff[n0]), int(soff[n1] - soff[n0]), pb[0], pb[1], pb[2], pb[3],
                pr[0], pr[1], 0, 0] for (n0, n1), pb, pr in zip(blocks_nodes, per_block, pranges)]
 
+    # ---- clamps: CSR over internal nodes of (node-relative slot, clamp column) ----
+    cl_int, cl_slot, cl_col, cl_vals = [], [], [], []
+    ncl = 0
+    for cname, cnodes, cvals in getattr(p, "clamps", []) or []:
+        cnodes = np.asarray(cnodes, dtype=np.int64).reshape(-1)
+        cvals = np.asarray(cvals, dtype=np.float64)
+        cvals = cvals.reshape(-1, len(cnodes), cvals.shape[-1])
+        for q, node in enumerate(cnodes):
+            i = int(node2int[node])
+            names = grp_names[grp_int[i]]
+            if cname not in names:
+                continue  # the node has no such state: nothing to clamp
+            cl_int.append(i)
+            cl_slot.append(names.index(cname))
+            cl_col.append(ncl + q)
+        cl_vals.append(cvals)
+        ncl += len(cnodes)
+    clamp = None
+    clamp_ptr = np.zeros(n + 1, dtype=np.int32)
+    clamp_slot = np.zeros(0, dtype=np.int32)
+    clamp_col = np.zeros(0, dtype=np.int32)
+    if cl_int:
+        rows = max(v.shape[0] for v in cl_vals)
+        steps = min(v.shape[-1] for v in cl_vals)
+        full = np.concatenate([np.broadcast_to(v[..., :steps], (rows,) + v.shape[1:2] + (steps,))
+                               for v in cl_vals], axis=1)
+        clamp = np.ascontiguousarray(np.transpose(full, (2, 0, 1)))  # (steps, rows, ncl)
+        cl_int = np.asarray(cl_int, dtype=np.int64)
+        by_node = np.argsort(cl_int, kind="stable")  # keeps the given order per node: last wins
+        clamp_slot = np.asarray(cl_slot, dtype=np.int32)[by_node]
+        clamp_col = np.asarray(cl_col, dtype=np.int32)[by_node]
+        clamp_ptr[1:] = np.cumsum(np.bincount(cl_int, minlength=n))
+
     # ---- stimulus CSR (internal node -> stimulus columns) ----
     stim_inds = np.asarray(p.stim_inds, dtype=np.int64)
     s_int = node2int[stim_inds] if len(stim_inds) else np.zeros(0, np.int64)
@@ -785,6 +848,10 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
         level_ptr=i32(level_ptr),
         blocks=i32(blocks),
         stim_ptr=stim_ptr,
+        clamp_ptr=clamp_ptr,
+        clamp_slot=clamp_slot,
+        clamp_col=clamp_col,
+        clamp=clamp,
         stim_idx=stim_idx,
         stim=stim,
         gk=gk,

@@ -74,6 +74,12 @@ class Problem:
     # group share one scale column and so one gradient, like one `make_trainable`
     # call on a view in the reference (`modules/base.py:1625`).
     trainable: List[Tuple[str, np.ndarray]] = field(default_factory=list)
+    # Clamps `(state name, reference nodes (n_c,), values (B or 1, n_c, >= n_steps))`:
+    # after step t the state of node q is set to values[..., q, t]; a voltage clamp
+    # after the voltage solve, any other state after the channel update of the step
+    # (`modules/base.py:3305-3308, 3396-3398`). For a node clamped twice the later
+    # entry wins.
+    clamps: List[Tuple[str, np.ndarray, np.ndarray]] = field(default_factory=list)
 
     def solve_order_system(self):
         """Per solve position `j`: parent, `g_low[j]` (coupling of row `j` to its
@@ -118,6 +124,37 @@ def _flatten_batch(a: np.ndarray) -> np.ndarray:
     return a.reshape(-1, a.shape[-1])
 
 
+def _flatten_to(a: np.ndarray, batch_shape: tuple, core: int = 1) -> np.ndarray:
+    """An array with `core` trailing dimensions and optional leading batch dimensions:
+    unchanged without batch dimensions, else broadcast to `batch_shape` and flattened
+    to one leading dimension."""
+    if a.ndim <= core:
+        return a
+    tail = a.shape[a.ndim - core:]
+    return np.broadcast_to(a, tuple(batch_shape) + tail).reshape((-1,) + tail)
+
+
+def _cpu64(x):
+    """A detached CPU float64 copy of a tensor (other values unchanged)."""
+    import torch
+
+    if isinstance(x, torch.Tensor):
+        return x.detach().to(device="cpu", dtype=torch.float64)
+    return x
+
+
+def _broadcast_last(x) -> bool:
+    """Whether the last dimension of a tensor is a broadcast (stride 0) of one value."""
+    import torch
+
+    return isinstance(x, torch.Tensor) and x.dim() > 0 and x.shape[-1] > 1 and x.stride(-1) == 0
+
+
+# Parameters that enter the axial conductances (`utils/morph_attributes.py:315-436`)
+# or the membrane area rather than a channel: the CUDA adjoint has no gradient for them.
+GEOMETRY_PARAMS = ("radius", "length", "axial_resistivity", "capacitance", "area")
+
+
 def problem_from_module(
     module,
     params: list = [],
@@ -125,14 +162,21 @@ def problem_from_module(
     data_stimuli=None,
     t_max: Optional[float] = None,
     delta_t: float = 0.025,
+    data_clamps=None,
+    all_states: Optional[dict] = None,
 ) -> Problem:
     """Lower a reference `jx.Module` (jaxley-pytorch) into a `Problem`.
 
     Follows `jx.integrate` (`integrate.py:476-622`): the stimulus is padded or
-    truncated to `int(t_max // delta_t + 1)` samples, parameters come from
+    truncated to `int(t_max // delta_t + 1)` samples, clamps truncated (they must be
+    at least that long, `integrate.py:528-545`), parameters come from
     `get_all_parameters`, initial states from `get_all_states` plus the initial
-    currents (`_append_currents_with_plan`). Only the `bwd_euler` step with the DHS
-    solve is covered, with at most one leading batch dimension.
+    currents (`_append_currents_with_plan`), or from `all_states` (a previous run's
+    final states). Every group of the trainable `params` (one per row of
+    `module.indices_set_by_trainables`) that sets a channel parameter of nodes
+    becomes a `Problem.trainable` group; `problem.trainable_source[q] = (entry, group)`
+    names where group q came from. Only the `bwd_euler` step with the DHS solve is
+    covered, with at most one leading batch dimension.
     """
     import torch
 
@@ -144,16 +188,27 @@ def problem_from_module(
     device = torch.device("cpu")
     dtype = torch.float64
     module.to_torch(device=device, dtype=dtype)
+    # Inputs may live on any device and dtype: the problem is assembled from detached
+    # float64 copies on the CPU (which entries ask for gradients is noted first).
+    ps_grad = [(isinstance(e["val"], torch.Tensor) and e["val"].requires_grad, _broadcast_last(e["val"]))
+               for e in (param_state or [])]
+    params = [{k: _cpu64(v) for k, v in e.items()} for e in params]
+    if param_state is not None:
+        param_state = [dict(e, val=_cpu64(e["val"])) for e in param_state]
+    if data_stimuli is not None:
+        data_stimuli = (data_stimuli[0], [_cpu64(v) for v in data_stimuli[1]], data_stimuli[2])
+    if data_clamps is not None:
+        data_clamps = (data_clamps[0], [_cpu64(v) for v in data_clamps[1]], data_clamps[2])
+    if all_states is not None:
+        all_states = {k: _cpu64(v) for k, v in all_states.items()}
 
-    # Externals (stimuli only; clamps are not part of this path).
     externals = {k: torch.as_tensor(v, dtype=dtype) for k, v in module.externals.items()}
     external_inds = dict(module.external_inds)
-    if data_stimuli is not None:
-        from jaxley_pytorch.integrate import add_stimuli
+    from jaxley_pytorch.integrate import add_clamps, add_stimuli
 
-        externals, external_inds = add_stimuli(externals, external_inds, data_stimuli)
-    if any(k != "i" for k in externals):
-        raise NotImplementedError("clamps are not part of the CUDA step path")
+    externals, external_inds = add_stimuli(externals, external_inds, data_stimuli)
+    externals, external_inds = add_clamps(externals, external_inds, data_clamps)
+    clamp_keys = [k for k in externals if k != "i"]
     if "i" in externals:
         stim = externals["i"]
         n_samples = stim.shape[-1]
@@ -166,25 +221,52 @@ def problem_from_module(
                 stim = stim[..., :want]
         n_steps = stim.shape[-1]
         stim_np = _np(stim)
-        if stim_np.ndim == 2:
-            stim_np = stim_np[None]
-        stim_np = stim_np.reshape(-1, *stim_np.shape[-2:])
         stim_inds = np.asarray(external_inds["i"], dtype=np.int64)
     else:
-        assert t_max is not None
-        n_steps = int(t_max // delta_t + 1)
         stim_np, stim_inds = None, np.zeros(0, np.int64)
+        if clamp_keys and t_max is None:
+            n_steps = int(torch.as_tensor(externals[clamp_keys[0]]).shape[-1])
+        else:
+            if t_max is None:
+                raise ValueError("without a stimulus or clamp, t_max is required")
+            n_steps = int(t_max // delta_t + 1)
+    clamps = []
+    for key in clamp_keys:
+        vals = _np(externals[key])
+        if vals.shape[-1] < n_steps:
+            raise NotImplementedError("clamp must be at least as long as simulation.")
+        vals = vals[..., :n_steps]
+        if vals.ndim == 1:
+            vals = vals.reshape(1, -1)
+        clamps.append((str(key), np.asarray(external_inds[key], dtype=np.int64).reshape(-1), vals))
 
     pstate = params_to_pstate(params, module.indices_set_by_trainables)
     if param_state is not None:
         pstate = pstate + list(param_state)
     all_params = module.get_all_parameters(pstate)
-    init_states = module.get_all_states(pstate)
-    batch = _batch_shape(list(tree_tensors(all_params)) + list(tree_tensors(init_states)))
-    init_states = _expand_states(init_states, batch)
+    if all_states is None:
+        init_states = module.get_all_states(pstate)
+        batch = _batch_shape(list(tree_tensors(all_params)) + list(tree_tensors(init_states)))
+        init_states = _expand_states(init_states, batch)
+    else:
+        batch = _batch_shape(list(tree_tensors(all_params)) + list(tree_tensors(all_states)))
+        init_states = _expand_states(all_states, batch)
+    # One batch shape for everything (integrate.py:570-585): the inputs' batch
+    # dimensions broadcast against each other, then flatten to rows.
+    batch_shape = tuple(batch)
+    if stim_np is not None:
+        batch_shape = tuple(np.broadcast_shapes(batch_shape, stim_np.shape[:-2]))
+    for _, _, vals in clamps:
+        batch_shape = tuple(np.broadcast_shapes(batch_shape, vals.shape[:-2]))
+    if stim_np is not None:
+        stim_np = _flatten_to(stim_np, batch_shape, core=2)
+        if stim_np.ndim == 2:
+            stim_np = stim_np[None]
+    clamps = [(k, i, _flatten_to(v, batch_shape, core=2) if v.ndim > 2 else v[None]) for k, i, v in clamps]
     plan = module._get_step_plan(device, "jaxley.dhs.gpu", "bwd_euler")
     gathered = module._gather_step_params(plan, all_params)
-    init_states = module._append_currents_with_plan(init_states, delta_t, plan, gathered)
+    if all_states is None:
+        init_states = module._append_currents_with_plan(init_states, delta_t, plan, gathered)
 
     n = int(base._n_nodes)
     indexer = base._dhs_solve_indexer
@@ -213,12 +295,12 @@ def problem_from_module(
             if isinstance(v, dict):
                 continue
             if isinstance(v, torch.Tensor) and v.ndim >= 1 and v.shape[-1] == n:
-                out[k] = _flatten_batch(_np(v))
+                out[k] = _flatten_to(_np(v), batch_shape)
         return out
 
     params_np = flat(all_params)
     states_np = flat(init_states)
-    axial = _flatten_batch(_np(all_params["axial_conductances"]["v"]))
+    axial = _flatten_to(_np(all_params["axial_conductances"]["v"]), batch_shape)
 
     synapses = []
     for sp, gp in zip(plan["synapses"], gathered["synapses"]):
@@ -235,9 +317,31 @@ def problem_from_module(
         batches.append(stim_np.shape[0])
     if axial.ndim == 2:
         batches.append(axial.shape[0])
+    batches += [c[2].shape[0] for c in clamps]
     B = max(batches) if batches else 1
 
-    return Problem(
+    # Trainable groups of node parameters, in the order of `params` and its groups,
+    # then those of the `param_state` entries whose value requires a gradient (the
+    # source index of the latter is len(params) + their position in param_state).
+    trainable, source = [], []
+    node_keys = set(base.nodes.columns)
+    entries = [(list(e.keys())[0], np.asarray(module.indices_set_by_trainables[q]), True, False)
+               for q, e in enumerate(params)]
+    for ps, (grad, bcast) in zip(param_state or [], ps_grad):
+        entries.append((ps["key"], np.asarray(ps["indices"]), grad, bcast))
+    for q, (key, inds, grad, bcast) in enumerate(entries):
+        if not grad or key not in node_keys or key in GEOMETRY_PARAMS or key not in params_np:
+            continue
+        inds = inds.reshape(inds.shape[0], -1)
+        if bcast and inds.shape[0] > 1:
+            # one value broadcast over the view (data_set of a `(..., 1)` value)
+            inds = inds.reshape(1, -1)
+        for g in range(inds.shape[0]):
+            nodes = inds[g][inds[g] >= 0].astype(np.int64)
+            trainable.append((key, nodes))
+            source.append((q, g))
+
+    prob = Problem(
         n_nodes=n,
         comp_inds=np.asarray(base._internal_node_inds, dtype=np.int64),
         sinks=_np(plan["sinks"], np.int64),
@@ -257,7 +361,12 @@ def problem_from_module(
         synapses=synapses,
         batch=int(B),
         current_names=list(base.membrane_current_names),
+        trainable=trainable,
+        clamps=clamps,
     )
+    prob.trainable_source = source
+    prob.batch_shape = batch_shape
+    return prob
 
 
 def _synapse_from_plan(sp, gp, states) -> SynapseType:
@@ -323,6 +432,10 @@ def save_problem(problem: Problem, path: str, **extra) -> None:
     }
     for q, (_, nodes) in enumerate(problem.trainable):
         arrays[f"trainable/{q}"] = np.asarray(nodes, dtype=np.int64)
+    meta["clamps"] = [name for name, _, _ in problem.clamps]
+    for q, (_, nodes, vals) in enumerate(problem.clamps):
+        arrays[f"clamp/{q}/nodes"] = np.asarray(nodes, dtype=np.int64)
+        arrays[f"clamp/{q}/values"] = np.asarray(vals, dtype=np.float64)
     for k, v in problem.params.items():
         arrays[f"param/{k}"] = v
     for k, v in problem.states.items():
@@ -385,6 +498,7 @@ def load_problem(path: str):
         recordings=[(n, i) for n, i in meta["recordings"]], synapses=synapses,
         batch=meta["batch"], current_names=meta["current_names"],
         trainable=[(n, z[f"trainable/{q}"]) for q, n in enumerate(meta.get("trainable", []))],
+        clamps=[(n, z[f"clamp/{q}/nodes"], z[f"clamp/{q}/values"]) for q, n in enumerate(meta.get("clamps", []))],
     )
     extra = {k[len("extra/"):]: z[k] for k in z.files if k.startswith("extra/")}
     return prob, extra

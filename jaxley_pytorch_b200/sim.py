@@ -126,6 +126,12 @@ class DeviceModel:
             self.t["cls_prog"] = torch.zeros_like(self.t["cls_prog"])
         self.pscale = f(low.pscale)
         self.stim = f(low.stim) if low.stim is not None else None
+        self.clamp = None
+        if getattr(low, "clamp", None) is not None:
+            self.clamp = f(low.clamp)
+            self.t["clamp_ptr"] = i(low.clamp_ptr)
+            self.t["clamp_slot"] = i(low.clamp_slot)
+            self.t["clamp_col"] = i(low.clamp_col)
         self.threads = threads
         self.launches = 0  # kernel launches issued through this model
         self.timed_kind: Optional[str] = None  # "forward"/"backward": record events
@@ -267,6 +273,12 @@ class DeviceModel:
             a.n_stim = self.stim.shape[2]
             a.stim_steps = self.stim.shape[0]
             a.stim_rows = self.stim.shape[1]
+        if self.clamp is not None:
+            a.clamp_ptr = t["clamp_ptr"].data_ptr()
+            a.clamp_slot = t["clamp_slot"].data_ptr()
+            a.clamp_col = t["clamp_col"].data_ptr()
+            a.clamp = self.clamp.data_ptr()
+            a.clamp_steps, a.clamp_rows, a.n_clamp = self.clamp.shape
         a.syn_lin = _ptr(syn_lin)
         a.syn_const = _ptr(syn_const)
         a.rec_out = _ptr(rec_out)
@@ -442,6 +454,7 @@ class Simulation:
                 a.traj_piv = piv[t].data_ptr()
             m.launch_forward(a)
             t += k
+        self.last_state = state  # the final state of the latest forward run (B, n_slots)
         return rec, state
 
     def backward_raw(self, pscale: torch.Tensor, T: int, ckpt: torch.Tensor,

@@ -217,11 +217,13 @@ def assemble(cells: List[dict], channels_per_cell: List[List[Tuple[str, np.ndarr
 
 
 def step_current(i_delay: float, i_dur: float, i_amp, delta_t: float, t_max: float) -> np.ndarray:
-    """Step current of `int(t_max // delta_t) + 2` samples (stimulus.py:8-36)."""
+    """Step current of `int(t_max // delta_t) + 2` samples (stimulus.py:8-36): on for
+    the samples from `int(i_delay / delta_t)` up to, not including,
+    `int((i_delay + i_dur) / delta_t)` (both truncated, as the reference does)."""
     n = int(t_max // delta_t) + 2
-    t = np.arange(n) * delta_t
+    on = np.zeros(n)
+    on[int(i_delay / delta_t):int((i_delay + i_dur) / delta_t)] = 1.0
     amp = np.asarray(i_amp, dtype=np.float64).reshape(-1, 1)
-    on = ((t >= i_delay) & (t < i_delay + i_dur)).astype(np.float64)
     return amp * on[None]
 
 
@@ -409,5 +411,52 @@ def config_uneven(n_cells: int = 4096, seed: int = 0, n_steps: int = 2000, min_c
         prob.states["CaCon_i"] = np.where(prob.states["CaCon_i"] == 0, 5e-05, prob.states["CaCon_i"])
     if "CaCon_e" in prob.states:
         prob.states["CaCon_e"] = np.where(prob.states["CaCon_e"] == 0, 2.0, prob.states["CaCon_e"])
+    # The L5PC cells' reversal potentials, as in the large-batch tree (HH keeps its own
+    # HH_eNa / HH_eK).
+    for k, val in (("eNa", 50.0), ("eK", -85.0)):
+        if k in prob.params:
+            prob.params[k] = np.full(prob.n_nodes, val)
     prob.meta = {"cells": specs}
     return prob
+
+
+def reference_l5pc_cell(jx, parents, ncomp: int, radius, lengths):
+    """The L5PC-like cell of `l5pc_channels` built with the reference's own module
+    API (`jx` is the imported `jaxley_pytorch`): soma = branch 0 (NaTs2T, SKv3_1,
+    SKE2, CaNernstReversal at 307.15 K, CaPump, CaHVA, CaLVA), dendrites = the other
+    branches (NaTs2T, SKv3_1, M, H), Leak everywhere, axial resistivity 100 ohm cm,
+    eNa 50 mV, eK -85 mV, v -65 mV; branch b has radius `radius[b]` and length
+    `lengths[b]` split over its `ncomp` compartments (`examples/paper/
+    fig2_l5pc_synthetic.py:100-152` sets up the same channel sets)."""
+    from jaxley_pytorch.channels.pospischil import Leak
+    from jaxley_pytorch.mech.channels import l5pc as ref_l5pc
+
+    nb = len(parents)
+    cell = jx.Cell([jx.Branch(jx.Compartment(), ncomp)] * nb, parents=list(parents))
+    for b in range(nb):
+        cell.branch(b).set("radius", float(radius[b]))
+        cell.branch(b).set("length", float(lengths[b] / ncomp))
+    cell.set("axial_resistivity", 100.0)
+    for t, name, vals in L5PC_SOMA:
+        if t == "CaNernstReversal":
+            ch = ref_l5pc.CaNernstReversal()
+            ch.channel_constants["T"] = 307.15
+        else:
+            ch = getattr(ref_l5pc, t)().change_name(name)
+        cell.branch(0).insert(ch)
+    cell.branch(0).set("CaCon_i", 5e-05)
+    cell.branch(0).set("CaCon_e", 2.0)
+    if nb > 1:
+        dend = cell.branch(list(range(1, nb)))
+        for t, name, vals in L5PC_DEND:
+            dend.insert(getattr(ref_l5pc, t)().change_name(name))
+    cell.insert(Leak())
+    leak = ("Leak", "Leak", {"Leak_gLeak": 3e-05, "Leak_eLeak": -75.0})
+    for t, name, vals in L5PC_SOMA + (L5PC_DEND if nb > 1 else []) + [leak]:
+        for k, v in vals.items():
+            if k != "__constants__":
+                cell.set(k, v)
+    cell.set("eNa", 50.0)
+    cell.set("eK", -85.0)
+    cell.set("v", -65.0)
+    return cell

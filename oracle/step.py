@@ -550,11 +550,28 @@ class _Stepper:
                 st[f"i_{syn.name}"] = i0
             np.add.at(syn_lin.T, syn.targets, l_t.T)
             np.add.at(syn_const.T, syn.targets, (-c_t).T)
+        # Clamps of channel and synapse states after their step (modules/base.py:3305-3308).
+        for name, nodes, vals in getattr(p, "clamps", []) or []:
+            if name != "v":
+                st[name] = self._clamped(st[name], nodes, vals, t)
         # Assemble (modules/base.py:3257-3264) and solve (solver_voltage.py:250-359).
         lin_t = (lin + syn_lin) / self.cm
         const_t = (const + i_ext + syn_const) / self.cm
         st["v"] = self._solve(v, lin_t, const_t)
+        # Voltage clamps after the solve (modules/base.py:3396-3398).
+        for name, nodes, vals in getattr(p, "clamps", []) or []:
+            if name == "v":
+                st["v"] = self._clamped(st["v"], nodes, vals, t)
         return st
+
+    def _clamped(self, arr, nodes, vals, t):
+        """`arr (B, n)` with the clamp values of step t set at `nodes` (`_set_last`:
+        of repeated nodes the later entry wins)."""
+        out = np.array(arr, dtype=np.float64, copy=True)
+        vt = np.broadcast_to(np.asarray(vals)[..., t], (self.B, len(nodes)))
+        for q, node in enumerate(np.asarray(nodes)):
+            out[:, node] = vt[:, q]
+        return out
 
     def _solve(self, v, lin, const):
         p, B, n, dt = self.p, self.B, self.n, self.p.dt

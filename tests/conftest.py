@@ -34,3 +34,19 @@ def cuda_device():
 
     _lib.load()  # fail loudly if the library is missing on a GPU machine
     return torch.device("cuda:0")
+
+
+def import_reference():
+    """The reference package (jaxley-pytorch) for the drop-in tests: from
+    `JXB_REFERENCE` when set, else the copy installed under `baseline/_ref`; its
+    module-level matplotlib import (plotting only) is served by the stand-in package
+    under `tests/golden/_mpl_stub`. Skips when neither is present."""
+    import importlib
+
+    path = os.environ.get("JXB_REFERENCE") or os.path.join(REPO, "baseline", "_ref")
+    if not os.path.isdir(os.path.join(path, "jaxley_pytorch")):
+        pytest.skip("the reference package is not installed here")
+    for p in (os.path.join(GOLDEN, "_mpl_stub"), path):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    return importlib.import_module("jaxley_pytorch")

@@ -36,7 +36,7 @@ from jaxley_pytorch.mech.channels.l5pc import (  # noqa: E402
 )
 from jaxley_pytorch.synapses import KineticSynapse, SigmoidRateSynapse  # noqa: E402
 
-from jaxley_pytorch_b200.problem import problem_from_module, save_problem  # noqa: E402
+from jaxley_pytorch_b200.problem import load_problem, problem_from_module, save_problem  # noqa: E402
 
 
 def golden_arrays(test_file: str, func: str) -> np.ndarray:
@@ -60,6 +60,45 @@ def save(name, module, **kw):
     path = os.path.join(HERE, f"{name}.npz")
     save_problem(prob, path, ref=ref, **extra)
     print(name, ref.shape, prob.n_nodes, "nodes", prob.batch, "rows")
+    return prob, ref
+
+
+def loss_weights(shape, seed):
+    """Weights of the linear loss `sum(w * recordings)` whose gradient the fixtures
+    hold (seeded; scaled so that the loss is of order one)."""
+    rng = np.random.default_rng(seed)
+    return rng.normal(size=shape) / np.sqrt(np.prod(shape))
+
+
+def reference_grads(module, tensors, loss_w, **kw):
+    """`(recordings, [d loss / d t for t in tensors])` of the reference's `jx.integrate`
+    (autograd through its step and `_DHSSolve.backward`, solver_voltage.py:143-187)
+    for the loss `sum(loss_w * recordings)`."""
+    for t in tensors:
+        t.requires_grad_(True)
+    rec = jx.integrate(module, **kw)
+    (rec * torch.as_tensor(loss_w)).sum().backward()
+    return rec.detach().numpy(), [t.grad.detach().numpy().copy() for t in tensors]
+
+
+def save_with_grads(name, module, params, seed, extra=None, **kw):
+    """A fixture of `module` with the reference's gradients with respect to the
+    trainable `params` (entry q, group g -> `extra/grad_q`) of a linear loss."""
+    extra = dict(extra or {})
+    probe = jx.integrate(module, params=params, **kw).detach().numpy()
+    w = loss_weights(probe.shape, seed)
+    tensors = [list(p.values())[0] for p in params]
+    ref, grads = reference_grads(module, tensors, w, params=params, **kw)
+    prob = problem_from_module(module, params=params, param_state=kw.get("param_state"),
+                               t_max=kw.get("t_max"), delta_t=kw.get("delta_t", 0.025),
+                               data_clamps=kw.get("data_clamps"), data_stimuli=kw.get("data_stimuli"))
+    extra["loss_w"] = w
+    extra["trainable_source"] = np.asarray(prob.trainable_source, dtype=np.int64).reshape(-1, 2)
+    for q, g in enumerate(grads):
+        extra[f"grad_{q}"] = g
+    path = os.path.join(HERE, f"{name}.npz")
+    save_problem(prob, path, ref=ref, **extra)
+    print(name, ref.shape, prob.n_nodes, "nodes", prob.batch, "rows", len(params), "trainables")
     return prob, ref
 
 
@@ -181,7 +220,15 @@ def l5pc_cell():
     pstate = cell.branch(0).data_set("somatic_NaTs2T_gNaTs2T", torch.tensor([[0.9], [1.1], [0.5]]), None)
     pstate = cell.branch(1).data_set("apical_M_gM", torch.tensor([[1e-4], [2e-4], [3e-4]]), pstate)
     pstate = cell.branch(2).data_set("apical_H_gH", torch.tensor([[5e-5], [8e-5], [1.2e-4]]), pstate)
-    save("l5pc_7x4_batch3", cell, param_state=pstate, delta_t=0.025, t_max=15.0)
+    # Trainables (shared over the batch): the reference's gradients pin the adjoint.
+    cell.branch(0).make_trainable("somatic_SKv3_1_gSKv3_1", verbose=False)
+    cell.branch(0).make_trainable("somatic_CaHVA_gCaHVA", verbose=False)
+    cell.make_trainable("apical_NaTs2T_gNaTs2T", verbose=False)
+    cell.make_trainable("Leak_gLeak", verbose=False)
+    cell.branch(5).make_trainable("axonal_KTst_gKTst", verbose=False)
+    cell.branch("all").make_trainable("apical_SKv3_1_gSKv3_1", verbose=False)
+    save_with_grads("l5pc_7x4_batch3", cell, cell.get_parameters(), seed=21, param_state=pstate,
+                    delta_t=0.025, t_max=15.0)
 
 
 def hh_forest():
@@ -229,12 +276,204 @@ def synapse_net():
     for c in range(0, n, 2):
         net.cell(c).branch(0).comp(1).stimulate(jx.step_current(1.0, 3.0, 0.3, 0.025, 15.0))
     save("synapse_net_8", net, delta_t=0.025)
+    # The reference's gradients of a linear loss with respect to every synapse's gS
+    # (per synapse, `edges` order) and the shared HH_gNa of all cells.
+    probe = jx.integrate(net, delta_t=0.025).detach().numpy()
+    w = loss_weights(probe.shape, 31)
+    edges = net.edges
+    gs = {}
+    for syn in ("KineticSynapse", "SigmoidRateSynapse"):
+        sel = edges[edges.type == syn]
+        gs[syn] = torch.tensor(sel[f"{syn}_gS"].to_numpy(), dtype=torch.float64, requires_grad=True)
+    # (data_set broadcasts its value: the leaves must require gradients before it)
+    gna = torch.tensor([float(net.nodes["HH_gNa"].iloc[0])], dtype=torch.float64, requires_grad=True)
+    pstate = None
+    for syn, vals in gs.items():
+        pstate = net.select(edges=edges.index[edges.type == syn].to_numpy()).data_set(f"{syn}_gS", vals, pstate)
+    pstate = net.data_set("HH_gNa", gna, pstate)
+    _, grads = reference_grads(net, [gs["KineticSynapse"], gs["SigmoidRateSynapse"], gna], w,
+                               param_state=pstate, delta_t=0.025)
+    prob, extra = load_problem(os.path.join(HERE, "synapse_net_8.npz"))
+    extra = {k: v for k, v in extra.items() if not k.startswith("grad_")}
+    extra.update(loss_w=w, grad_0=grads[0], grad_1=grads[1], grad_2=grads[2])
+    save_problem(prob, os.path.join(HERE, "synapse_net_8.npz"), **extra)
+    print("synapse_net_8 gradients", [g.shape for g in grads])
+
+
+def clamp_cell():
+    """A branched HH cell with a voltage clamp on one compartment and a gate clamp
+    on another (Module.clamp, modules/base.py:2607), with the reference's gradients."""
+    cell = jx.Cell([jx.Branch(jx.Compartment(), 3)] * 7, parents=binary_parents(7))
+    cell.insert(HH())
+    rng = np.random.default_rng(13)
+    for b in range(7):
+        cell.branch(b).set("radius", float(rng.uniform(0.5, 2.0)))
+        cell.branch(b).set("length", float(rng.uniform(5.0, 40.0)))
+    T = 401
+    t = np.arange(T) * 0.025
+    vc = np.where((t >= 2.0) & (t < 6.0), -20.0, -70.0)
+    cell.branch(3).comp(1).clamp("v", vc, verbose=False)
+    cell.branch(5).comp(0).clamp("HH_m", np.full(T, 0.3), verbose=False)
+    cell.branch(0).comp(0).record()
+    cell.branch(3).comp(1).record()
+    cell.branch(3).comp(2).record()
+    cell.branch(5).comp(0).record("HH_m")
+    cell.branch(6).comp(2).record()
+    cell.branch(0).comp(0).stimulate(jx.step_current(1.0, 2.0, 0.05, 0.025, 10.0))
+    cell.make_trainable("HH_gNa", verbose=False)
+    cell.branch(3).make_trainable("HH_gK", verbose=False)
+    cell.branch("all").make_trainable("HH_gLeak", verbose=False)
+    save_with_grads("hh_clamp_7x3", cell, cell.get_parameters(), seed=41, delta_t=0.025)
+
+
+def reference_l5pc_cell(parents, ncomp, radius, lengths):
+    from jaxley_pytorch_b200 import synth
+
+    return synth.reference_l5pc_cell(jx, parents, ncomp, radius, lengths)
+
+
+def c2_sample():
+    """The large-batch L5PC tree (300 branches x 4 compartments, height 35-45) at 2
+    parameter sets and 400 steps, stimulus from 1 ms, rebuilt with the reference from
+    the generator's morphology; gradients with respect to the per-row conductances."""
+    from jaxley_pytorch_b200 import synth
+
+    B, T = 2, 400
+    prob = synth.config_l5pc_tree(batch=B, n_steps=T, stim_delay=1.0)
+    m = prob.meta
+    cell = reference_l5pc_cell(m["parents"], m["ncomp"], m["radius"], m["lengths"])
+    cell.init_states()
+    cell.branch(0).loc(0.0).record()
+    delay, dur, amp = m["stim"]
+    t_max = (T - 1) * 0.025
+    cell.branch(0).loc(0.0).stimulate(jx.step_current(delay, dur, amp, 0.025, T * 0.025))
+    soma_vals = {k: v for _, _, d in synth.L5PC_SOMA for k, v in d.items() if k != "__constants__"}
+    dend_vals = {k: v for _, _, d in synth.L5PC_DEND for k, v in d.items()}
+    nb = len(m["parents"])
+    pstate, tensors = None, []
+    for k in synth.L5PC_SCALED:
+        vals = torch.tensor(m["scales"][k])[:, None]
+        # (data_set broadcasts its value: the leaf must require gradients before it)
+        if k in soma_vals:
+            val = (vals * soma_vals[k]).requires_grad_(True)
+            pstate = cell.branch(0).data_set(k, val, pstate)
+        elif k in dend_vals:
+            val = (vals * dend_vals[k]).requires_grad_(True)
+            pstate = cell.branch(list(range(1, nb))).data_set(k, val, pstate)
+        else:
+            val = (vals * 3e-05).requires_grad_(True)
+            pstate = cell.data_set(k, val, pstate)
+        tensors.append(val)
+    probe = jx.integrate(cell, param_state=pstate, delta_t=0.025, t_max=t_max).detach().numpy()
+    assert probe.shape[-1] == T + 1, probe.shape
+    w = loss_weights(probe.shape, 51)
+    ref, grads = reference_grads(cell, tensors, w, param_state=pstate, delta_t=0.025, t_max=t_max)
+    extra = {"init_steady": 1, "loss_w": w, "height": m["height"],
+             "grad_names": np.frombuffer(",".join(synth.L5PC_SCALED).encode(), dtype=np.uint8)}
+    for q, g in enumerate(grads):
+        extra[f"grad_{q}"] = g
+    save_problem(prob, os.path.join(HERE, "c2_l5pc_tree_b2.npz"), ref=ref, **extra)
+    print("c2_l5pc_tree_b2", ref.shape, prob.n_nodes, "nodes, height", m["height"])
+
+
+def c3_sample():
+    """The first 8 cells of the uneven batch (HH or L5PC, 4-3000 compartments, depth
+    1-60, own step currents), 200 steps, as one reference network; gradients with
+    respect to every cell's trainable conductances."""
+    from jaxley_pytorch_b200 import synth
+
+    T = 200
+    prob = synth.config_uneven(n_cells=8, n_steps=T, seed=0)
+    cells = []
+    for spec in prob.meta["cells"]:
+        if spec["kind"] == "L5PC":
+            c = reference_l5pc_cell(spec["parents"], spec["ncomp"], spec["radius"], spec["lengths"])
+        else:
+            nb = len(spec["parents"])
+            c = jx.Cell([jx.Branch(jx.Compartment(), spec["ncomp"])] * nb, parents=list(spec["parents"]))
+            for b in range(nb):
+                c.branch(b).set("radius", float(spec["radius"][b]))
+                c.branch(b).set("length", float(spec["lengths"][b] / spec["ncomp"]))
+            c.set("axial_resistivity", 100.0)
+            c.insert(HH())
+            c.set("v", -65.0)
+        cells.append(c)
+    net = jx.Network(cells)
+    net.init_states()
+    for ci, spec in enumerate(prob.meta["cells"]):
+        net.cell(ci).branch(0).comp(0).record()
+        delay, dur, amp = spec["stim"]
+        net.cell(ci).branch(0).comp(0).stimulate(jx.step_current(delay, dur, amp, 0.025, T * 0.025))
+    for ci, spec in enumerate(prob.meta["cells"]):
+        for k in spec["train"]:
+            net.cell(ci).make_trainable(k, verbose=False)
+    params = net.get_parameters()
+    assert len(params) == len(prob.trainable)
+    t_max = (T - 1) * 0.025
+    probe = jx.integrate(net, params=params, delta_t=0.025, t_max=t_max).detach().numpy()
+    assert probe.shape[-1] == T + 1, probe.shape
+    w = loss_weights(probe.shape, 61)
+    tensors = [list(p.values())[0] for p in params]
+    ref, grads = reference_grads(net, tensors, w, params=params, delta_t=0.025, t_max=t_max)
+    extra = {"init_steady": 1, "loss_w": w}
+    for q, g in enumerate(grads):
+        extra[f"grad_{q}"] = g
+    save_problem(prob, os.path.join(HERE, "c3_uneven_8.npz"), ref=ref, **extra)
+    print("c3_uneven_8", ref.shape, prob.n_nodes, "nodes", [s["kind"] for s in prob.meta["cells"]])
+
+
+def c4_sample():
+    """The fixed in-degree network (HH cells of 4 compartments, 64 KineticSynapse and
+    64 SigmoidRateSynapse inputs on compartment 0 of every cell, Poisson input) at 72
+    cells, 4 batch rows and 200 steps, built with the reference; gradients with respect
+    to every synapse's gS and the shared HH_gNa."""
+    from jaxley_pytorch.synapses import KineticSynapse, SigmoidRateSynapse
+    from jaxley_pytorch_b200.network import config_network
+
+    n, k, B, T = 72, 64, 4, 200
+    prob = config_network(n_cells=n, k=k, batch=B, n_steps=T, seed=3)
+    cells = [jx.Cell([jx.Branch(jx.Compartment(), 4)], parents=[-1]) for _ in range(n)]
+    net = jx.Network(cells)
+    net.insert(HH())
+    net.set("v", -65.0)
+    nodes = net.nodes
+    for syn, cls in zip(prob.synapses, (KineticSynapse, SigmoidRateSynapse)):
+        net._append_multiple_synapses(nodes.loc[syn.pre], nodes.loc[syn.post], cls())
+    edges = net.edges
+    for syn in prob.synapses:
+        sel = edges.index[edges.type == syn.name].to_numpy()
+        assert np.array_equal(edges.loc[sel, "pre_index"].to_numpy(), syn.pre)
+        assert np.array_equal(edges.loc[sel, "post_index"].to_numpy(), syn.post)
+        net.select(edges=sel).set(f"{syn.name}_gS", syn.params[0])
+    for c in range(n):
+        net.cell(c).branch(0).comp(0).record()
+    t_max = (T - 1) * 0.025
+    stim = torch.as_tensor(prob.stim)  # (B, n, L)
+    data_stimuli = net.cell(list(range(n))).branch(0).comp(0).data_stimulate(stim)
+    gs = [torch.tensor(s.params[0], dtype=torch.float64, requires_grad=True) for s in prob.synapses]
+    gna = torch.tensor([0.12], dtype=torch.float64, requires_grad=True)
+    pstate = None
+    for syn, vals in zip(prob.synapses, gs):
+        sel = edges.index[edges.type == syn.name].to_numpy()
+        pstate = net.select(edges=sel).data_set(f"{syn.name}_gS", vals, pstate)
+    pstate = net.data_set("HH_gNa", gna, pstate)
+    kw = dict(param_state=pstate, data_stimuli=data_stimuli, delta_t=0.025, t_max=t_max)
+    probe = jx.integrate(net, **kw).detach().numpy()
+    assert probe.shape == (B, n, T + 1), probe.shape
+    w = loss_weights(probe.shape, 71)
+    ref, grads = reference_grads(net, gs + [gna], w, **kw)
+    prob.trainable = [("HH_gNa", np.arange(prob.n_nodes))]
+    extra = {"loss_w": w, "grad_0": grads[0], "grad_1": grads[1], "grad_2": grads[2]}
+    save_problem(prob, os.path.join(HERE, "c4_network_72.npz"), ref=ref, **extra)
+    print("c4_network_72", ref.shape, prob.n_nodes, "nodes", sum(len(s.pre) for s in prob.synapses), "synapses")
 
 
 if __name__ == "__main__":
-    which = [w for w in sys.argv[1:] if w != "synth"] if sys.argv[1:] else ["golden", "small", "tree", "l5pc", "forest", "synapse", "synth"]
+    which = [w for w in sys.argv[1:] if w != "synth"] if sys.argv[1:] else [
+        "golden", "small", "tree", "l5pc", "forest", "synapse", "clamp", "c2", "c3", "c4", "synth"]
     fns = {"golden": golden_cases, "small": config_small, "tree": hh_tree, "l5pc": l5pc_cell,
-           "forest": hh_forest, "synapse": synapse_net}
+           "forest": hh_forest, "synapse": synapse_net, "clamp": clamp_cell, "c2": c2_sample,
+           "c3": c3_sample, "c4": c4_sample}
     for w in which:
         if w in fns:
             fns[w]()

@@ -15,8 +15,11 @@ from jaxley_pytorch_b200.network import NetworkSimulation, config_network
 pytestmark = pytest.mark.gpu
 
 
-def test_fixture_matches_reference_fp64(cuda_device):
-    prob, extra = load_fixture("synapse_net_8")
+@pytest.mark.parametrize("name", ["synapse_net_8", "c4_network_72"])
+def test_fixture_matches_reference_fp64(cuda_device, name):
+    """Reference runs: 8 cells with k = 3, and the fixed in-degree network at 72 cells,
+    k = 64 of each synapse type, 4 rows of Poisson input."""
+    prob, extra = load_fixture(name)
     net = NetworkSimulation(prob, dtype=torch.float64, device=cuda_device, checkpoint=40)
     out = net.run().cpu().numpy()
     ref = extra["ref"].reshape(out.shape)

@@ -27,6 +27,14 @@ def forests():
     out["forest_mixed"] = f
     deep = [-1] + [int(j - 1 if rng.random() < 0.8 else rng.integers(0, j)) for j in range(1, 600)]
     out["deep_600"] = deep
+    # blocks beyond one warp's 256 nodes: the CTA form of the registers variant
+    wide = [-1] + [int(rng.integers(max(0, j - 40), j)) for j in range(1, 5000)]
+    out["tree_5000"] = wide
+    f = []
+    for sz in [300, 1, 900, 40, 2500]:
+        base = len(f)
+        f += [-1] + [base + int(rng.integers(max(0, j - 8), j)) for j in range(1, sz)]
+    out["forest_large"] = f
     return out
 
 
@@ -53,8 +61,10 @@ def test_schedules_on_cpu():
         if max(np.diff(np.append(np.nonzero(np.asarray(parent) < 0)[0], len(parent)))) <= ts.MAX_BLOCK:
             fs = ts.build_forest_schedule(np.asarray(parent))
             assert fs["block_size"] % 32 == 0
+    big = [-1] + list(range(ts.MAX_BLOCK))  # one tree of MAX_BLOCK + 1 nodes
     with pytest.raises(ValueError):
-        ts.build_forest_schedule(np.asarray(forests()["deep_600"]))
+        ts.build_forest_schedule(np.asarray(big))
+    assert ts.build_forest_schedule(np.asarray(forests()["tree_5000"]))["block_size"] == 8192
     with pytest.raises(ValueError):
         ts.build_level_schedule(np.asarray([0, -1]))
 
@@ -64,8 +74,6 @@ def test_schedules_on_cpu():
 @pytest.mark.parametrize("name", list(forests()))
 def test_tree_solve_matches_oracle(cuda_device, mode, name):
     parent = np.asarray(forests()[name])
-    if mode == "registers" and name == "deep_600":
-        pytest.skip("tree larger than the registers variant")
     kern = ts.make_tree_solve_kernel(parent, cuda_device, mode=mode)
     assert isinstance(kern, ts.TreeSolveKernel if mode == "registers" else ts.LevelTreeSolveKernel)
     d, l, u, s = system(parent, 6, np.float64)
