@@ -23,8 +23,11 @@ synapse types, 32 rows of Poisson input, 2000 steps; and `serving`: a Poisson st
 capacity, served with continuous batching: p50/p99 latency and throughput, beside the
 plain one-request-at-a-time path on the same arrivals.
 
-`--impl reference` times the CPU restatement of the reference's torch path (eager
-autograd) on the host cores, on a bounded sample of the same workload.
+`--impl reference` times the reference's own torch path (its `jx.integrate` from the
+copy installed under `baseline/_ref`, eager autograd, float32) on the host cores, on a
+bounded sample of the same workload (the CPU port of that path when the reference is
+not installed); `cpu_baseline` in the line is the same measurement, with the forward
+alone beside it.
 
 Multi-GPU (torchrun): every rank simulates its own 256 parameter sets (weak scaling,
 no collective in the data path); the timing is the maximum over ranks.
@@ -75,6 +78,8 @@ def parse():
     ap.add_argument("--no-recompute", action="store_true",
                     help="skip the checkpoint/recompute comparison of the main iteration")
     ap.add_argument("--net-tsteps", type=int, default=2000)
+    ap.add_argument("--no-fp32-error", action="store_true",
+                    help="skip the float32-against-float64 error of the sampled configurations")
     ap.add_argument("--serve-requests", type=int, default=240)
     ap.add_argument("--serve-capacity-requests", type=int, default=160)
     return ap.parse_args()
@@ -525,6 +530,166 @@ def run_network(args, device):
             "loss": float(it.loss)}
 
 
+def _errors(rec64, rec32, g64, g32, vcols):
+    from jaxley_pytorch_b200.accuracy import gradient_error, voltage_errors
+
+    out = voltage_errors(rec64[:, vcols], rec32[:, vcols])
+    if g64 is not None:
+        out["grad_rel_err"] = gradient_error(g64, g32)
+    return out
+
+
+def fp32_errors(device):
+    """float32 against float64 of the same kernels on samples of the benchmarked
+    configurations: max |dV| of the voltage recordings over the whole trace and over
+    its subthreshold stretches, and the relative error of the adjoint's gradient of
+    an MSE loss (largest deviation over the largest gradient entry)."""
+    import torch
+
+    from jaxley_pytorch_b200 import synth
+    from jaxley_pytorch_b200.network import NetworkSimulation, config_network
+    from jaxley_pytorch_b200.sim import Simulation
+
+    def cell_run(prob, dtype, steady, kw):
+        sim = Simulation(prob, dtype=dtype, device=device, init_steady=steady, **kw)
+        ps = sim.model.pscale.clone().requires_grad_(True)
+        rec = sim.run(pscale=ps)
+        with torch.no_grad():
+            target = rec.detach() * 0 + (-65.0)
+        loss = ((rec - target) ** 2).mean()
+        (g,) = torch.autograd.grad(loss, ps)
+        return rec.detach().double().cpu().numpy(), g.double().cpu().numpy()
+
+    out = {}
+    kw = dict(keep_currents=False, checkpoint=100)
+    prob = synth.config_l5pc_tree(batch=8, n_steps=4000, seed=0, scale_seed=1)
+    r64, g64 = cell_run(prob, torch.float64, True, kw)
+    r32, g32 = cell_run(prob, torch.float32, True, kw)
+    out["C2"] = dict(_errors(r64, r32, g64, g32, [0]), sample="8 parameter sets, 4000 steps")
+    prob = synth.config_uneven(n_cells=64, n_steps=2000)
+    r64, g64 = cell_run(prob, torch.float64, False, kw)
+    r32, g32 = cell_run(prob, torch.float32, False, kw)
+    out["C3"] = dict(_errors(r64, r32, g64, g32, list(range(64))), sample="64 cells, 2000 steps")
+    prob = config_network(n_cells=256, ncomp=4, k=64, batch=4, n_steps=2000, seed=0)
+
+    def net_run(dtype):
+        net = NetworkSimulation(prob, dtype=dtype, device=device, checkpoint=50, threads=256,
+                                max_block_nodes=256)
+        params = [[p.clone().requires_grad_(True)] + p_[1:] for p, p_ in
+                  ((ty.params[0], ty.params) for ty in net.types)]
+        rec = net.run(net.model.pscale, params)
+        loss = ((rec + 65.0) ** 2).mean()
+        grads = torch.autograd.grad(loss, [p[0] for p in params])
+        return rec.detach().double().cpu().numpy(), torch.cat(grads).double().cpu().numpy()
+
+    r64, g64 = net_run(torch.float64)
+    r32, g32 = net_run(torch.float32)
+    out["C4"] = dict(_errors(r64, r32, g64, g32, list(range(256))),
+                     sample="256 cells, k = 64 of each type, 4 rows, 2000 steps; gradient of gS")
+    return out
+
+
+def import_reference():
+    """The reference package (jaxley-pytorch) installed under `baseline/_ref`, or
+    None. Its module-level matplotlib import (plotting only) is served by the
+    stand-in package under `tests/golden/_mpl_stub`."""
+    import importlib
+
+    path = os.path.join(REPO, "baseline", "_ref")
+    if not os.path.isdir(os.path.join(path, "jaxley_pytorch")):
+        return None
+    for p in (os.path.join(REPO, "tests", "golden", "_mpl_stub"), path):
+        if p not in sys.path:
+            sys.path.insert(0, p)
+    try:
+        return importlib.import_module("jaxley_pytorch")
+    except Exception:
+        return None
+
+
+class ReferenceSample:
+    """The reference's own torch path on the host cores: its `jx.integrate`
+    (`voltage_solver="jaxley.dhs"`, float32) on `batch` of the workload's parameter
+    sets and `tsteps` of its steps, the cell rebuilt with the reference's module API
+    from the generator's morphology; `step()` is one forward + `loss.backward()` of
+    the MSE of the somatic voltage to a held-out parameter set's trace, `forward()`
+    the forward alone. Returns seconds."""
+
+    def __init__(self, jx, batch: int, tsteps: int):
+        import torch
+
+        from jaxley_pytorch_b200 import synth
+
+        self.jx, self.torch = jx, torch
+        self.cores = os.cpu_count() or 1
+        torch.set_num_threads(self.cores)
+        prob = synth.config_l5pc_tree(batch=batch, n_steps=tsteps, seed=0, scale_seed=1)
+        held = synth.config_l5pc_tree(batch=1, n_steps=tsteps, seed=0, scale_seed=10_000)
+        m = prob.meta
+        self.cell = synth.reference_l5pc_cell(jx, m["parents"], m["ncomp"], m["radius"], m["lengths"])
+        self.cell.init_states()
+        self.cell.branch(0).loc(0.0).record(verbose=False)
+        delay, dur, amp = m["stim"]
+        self.cell.branch(0).loc(0.0).stimulate(jx.step_current(delay, dur, amp, 0.025, tsteps * 0.025),
+                                               verbose=False)
+        self.t_max = (tsteps - 0.5) * 0.025  # tsteps steps (integrate.py:521)
+        self.nb = len(m["parents"])
+        base = {k: v for _, _, d in synth.L5PC_SOMA + synth.L5PC_DEND for k, v in d.items()}
+        base["Leak_gLeak"] = 3e-05
+        self.soma = {k for _, _, d in synth.L5PC_SOMA for k in d}
+        self.dend = {k for _, _, d in synth.L5PC_DEND for k in d}
+        self.values = {k: np.asarray(m["scales"][k])[:, None] * base[k] for k in synth.L5PC_SCALED}
+        hv = {k: np.asarray(held.meta["scales"][k])[:, None] * base[k] for k in synth.L5PC_SCALED}
+        with torch.no_grad():
+            self.target = self._run(hv, grad=False)[0][..., 0, :]
+        self.comp_steps = len(prob.comp_inds) * batch * tsteps
+
+    def _run(self, values, grad: bool):
+        torch = self.torch
+        ps, leaves = None, []
+        for k, v in values.items():
+            val = torch.tensor(v, dtype=torch.float32, requires_grad=grad)
+            view = (self.cell.branch(0) if k in self.soma
+                    else self.cell.branch(list(range(1, self.nb))) if k in self.dend else self.cell)
+            ps = view.data_set(k, val, ps)
+            leaves.append(val)
+        rec = self.jx.integrate(self.cell, param_state=ps, delta_t=0.025, t_max=self.t_max,
+                                voltage_solver="jaxley.dhs")
+        return rec, leaves
+
+    def step(self) -> float:
+        t0 = time.perf_counter()
+        rec, leaves = self._run(self.values, grad=True)
+        loss = ((rec[..., 0, :] - self.target) ** 2).mean()
+        loss.backward()
+        return time.perf_counter() - t0
+
+    def forward(self) -> float:
+        t0 = time.perf_counter()
+        with self.torch.no_grad():
+            self._run(self.values, grad=False)
+        return time.perf_counter() - t0
+
+
+def reference_baseline(batch: int, tsteps: int, warmup: int = 1, reps: int = 3):
+    """`cpu_baseline` from the reference's own code: one warm-up, then the median of
+    `reps` forward + backward and of `reps` forward-only runs. None without the
+    reference installed."""
+    jx = import_reference()
+    if jx is None:
+        return None
+    smp = ReferenceSample(jx, batch, tsteps)
+    for _ in range(warmup):
+        smp.step()
+    fb = float(np.median([smp.step() for _ in range(reps)]))
+    smp.forward()
+    fw = float(np.median([smp.forward() for _ in range(reps)]))
+    return {"value": smp.comp_steps / fb, "unit": UNIT, "cores": smp.cores, "kind": "reference",
+            "sample": f"{batch} of 256 rows x {tsteps} of 4000 steps, fwd+bwd (MSE), float32, "
+                      f"jx.integrate voltage_solver=jaxley.dhs, median of {reps} after {warmup} warm-up",
+            "seconds_fwd_bwd": fb, "forward": {"value": smp.comp_steps / fw, "unit": UNIT, "seconds": fw}}
+
+
 def cpu_sample(batch: int, tsteps: int, reps: int = 1):
     """Times the torch CPU restatement of the reference path (forward + autograd
     backward) on `batch` rows x `tsteps` steps of the workload."""
@@ -562,20 +727,33 @@ def main():
     if args.impl == "reference":
         if rank != 0:
             return 0
-        vals = []
-        for _ in range(args.warmup):
-            cpu_sample(args.cpu_batch, args.cpu_tsteps, reps=0)
-        for _ in range(args.steps):
-            v, cores, t = cpu_sample(args.cpu_batch, args.cpu_tsteps, reps=0)
-            vals.append(v)
-        value = float(np.median(vals))
-        sample = f"{args.cpu_batch} of 256 rows x {args.cpu_tsteps} of 4000 steps per step, fwd+bwd"
+        jx = import_reference()
+        sample = (f"{args.cpu_batch} of 256 rows x {args.cpu_tsteps} of 4000 steps per step, fwd+bwd "
+                  f"(MSE), float32")
+        if jx is not None:  # the reference's own jx.integrate on the host cores
+            smp = ReferenceSample(jx, args.cpu_batch, args.cpu_tsteps)
+            for _ in range(args.warmup):
+                smp.step()
+            secs = [smp.step() for _ in range(args.steps)]
+            value = smp.comp_steps / float(np.median(secs))
+            cores, kind = smp.cores, "reference"
+            sample += ", jx.integrate voltage_solver=jaxley.dhs from baseline/_ref"
+        else:  # the CPU port of the reference's path
+            for _ in range(args.warmup):
+                cpu_sample(args.cpu_batch, args.cpu_tsteps, reps=0)
+            vals, secs = [], []
+            for _ in range(args.steps):
+                v, cores, t = cpu_sample(args.cpu_batch, args.cpu_tsteps, reps=0)
+                vals.append(v)
+                secs.append(t)
+            value, kind = float(np.median(vals)), "port"
+            sample += ", CPU port of the reference path (reference not installed)"
         out = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT,
                "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-               "ms_per_step": t * 1e3, "higher_is_better": True, "scaling": "weak",
+               "ms_per_step": float(np.median(secs)) * 1e3, "higher_is_better": True, "scaling": "weak",
                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                "config": {"workload": "l5pc_tree_300x4_b256_t4000_fwd_adjoint"},
-               "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+               "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind,
                                 "sample": sample},
                "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0,
                        "d2h_bytes_per_step": 0}}
@@ -594,12 +772,18 @@ def main():
         out["serving"] = run_serving(args, device)
     if world == 1 and not args.no_network:
         out["network"] = run_network(args, device)
+    if world == 1 and not args.no_fp32_error:
+        out["fp32_error"] = fp32_errors(device)
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
-            v, cores, t = cpu_sample(args.cpu_batch, args.cpu_tsteps, reps=0)
-            out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                                   "sample": f"{args.cpu_batch} of 256 rows x {args.cpu_tsteps} of "
-                                             f"4000 steps, fwd+bwd, {t:.1f} s"}
+            ref = reference_baseline(args.cpu_batch, args.cpu_tsteps)
+            if ref is not None:
+                out["cpu_baseline"] = ref
+            else:
+                v, cores, t = cpu_sample(args.cpu_batch, args.cpu_tsteps, reps=0)
+                out["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                                       "sample": f"{args.cpu_batch} of 256 rows x {args.cpu_tsteps} of "
+                                                 f"4000 steps, fwd+bwd, {t:.1f} s (reference not installed)"}
         print(json.dumps(out))
     if world > 1:
         torch.distributed.destroy_process_group()

@@ -749,6 +749,36 @@ __device__ __forceinline__ void node_adjoint(const SimSmem<T>& sm, int j, T* x, 
   }
 }
 
+// Adjoint of the initial channel currents of node j: the current slots of the
+// initial state are the channel currents at that state (`_append_currents_with_plan`,
+// modules/base.py:2375-2383, inside the reference's differentiated integrate), so
+// their adjoint (from the first step's reads, e.g. the calcium pump's, and from the
+// recordings at t = 0) flows to the channel parameters. The slots' adjoint is then
+// consumed: they are outputs of this computation, not inputs.
+template <typename T>
+__device__ __forceinline__ void node_initial_current_adjoint(const SimSmem<T>& sm, int j, const T* x, T* lam,
+                                                             const T* pv, T* gacc) {
+  const int cls = sm.cls[j];
+  const int e0 = sm.cptr[cls], e1 = sm.cptr[cls + 1];
+  const T* pn = pv + sm.poff[j];
+  const T* pb = sm.pb + sm.poff[j];
+  const int* pk = sm.gk + sm.poff[j];
+  T* ga = gacc + sm.gbase[j];
+  const T v = x[0];
+  T lv = T(0);
+  for (int q = e0; q < e1; ++q) {
+    const ChanEntry& e = sm.ents[q];
+    if (e.cur < 0) continue;
+    PGradSink<T> G{pb + e.p[0], pk + e.p[0], ga};
+    channel_current_vjp<T>(e, x, lam, Prm<T>{pn + e.p[0]}, G, v, T(0), v, lv);
+  }
+  lam[0] += lv;
+  for (int q = e0; q < e1; ++q) {
+    const int c = sm.ents[q].cur;
+    if (c >= 0) lam[c] = T(0);
+  }
+}
+
 // Elimination of chain c for the transposed system with the stored reciprocal
 // pivots: only the right-hand side is eliminated.
 template <typename T>
@@ -1000,6 +1030,30 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
       sm.X1[(size_t)r * nn + j] = x[solve_slot<T>(sm, j, nn, ns)];
     }
     if constexpr (!GM) cp_async_wait_all();  // the next step's pivots
+    __syncthreads();
+  }
+  if (a.t0 == 0) {
+    // The segment that starts the run: the recordings of t = 0 and the adjoint of the
+    // initial currents (the state in `st` is the initial state now).
+    for (int w = tid; w < total; w += nthr) {
+      const int r = w / nn, j = w - r * nn;
+      const int i = blk.node0 + j;
+      const int b = row0 + r;
+      T* x = sm.st + (size_t)r * ns + sm.soff[j];
+      T* lam = sm.adj + (size_t)r * ns + sm.soff[j];
+      if constexpr (GM) {
+        const int nslot = (j + 1 < nn ? sm.soff[j + 1] : ns) - sm.soff[j];
+        const T* g = traj + ((size_t)b) * a.n_slots + blk.slot0 + sm.soff[j];
+        for (int q = 0; q < nslot; ++q) x[q] = g[q];
+      }
+      if (rec_grad && (sm.flags[j] & FLAG_REC)) {
+        for (int q = a.rec_ptr[i]; q < a.rec_ptr[i + 1]; ++q) {
+          const int sl = a.rec_slot[q];
+          if (sl >= 0) lam[sl] += rec_grad[(size_t)b * a.n_rec + a.rec_col[q]];
+        }
+      }
+      node_initial_current_adjoint<T>(sm, j, x, lam, sm.pv + (size_t)r * np, sm.gacc + (size_t)r * gslots);
+    }
     __syncthreads();
   }
   // Fold the nodes' gradient slots into the columns (float64, global), once per
