@@ -78,6 +78,9 @@ def parse():
     ap.add_argument("--no-recompute", action="store_true",
                     help="skip the checkpoint/recompute comparison of the main iteration")
     ap.add_argument("--net-tsteps", type=int, default=2000)
+    ap.add_argument("--no-lm", action="store_true",
+                    help="skip the language-model network shape (1024 and 2048 HH neurons x 100 synapses)")
+    ap.add_argument("--lm-tokens", type=int, default=10, help="tokens of 200 solver steps per training step")
     ap.add_argument("--no-fp32-error", action="store_true",
                     help="skip the float32-against-float64 error of the sampled configurations")
     ap.add_argument("--serve-requests", type=int, default=240)
@@ -690,6 +693,61 @@ def reference_baseline(batch: int, tsteps: int, warmup: int = 1, reps: int = 3):
             "seconds_fwd_bwd": fb, "forward": {"value": smp.comp_steps / fw, "unit": UNIT, "seconds": fw}}
 
 
+# Published H100 figures of the reference's language-model HH networks (float32,
+# 100 KineticSynapse inputs per neuron, 32 streams): ms per solver step, forward,
+# recomputation and backward together (examples/language_modeling/README.md:115-116).
+H100_MS_PER_SOLVER_STEP = {1024: 0.21, 2048: 0.33}
+
+
+def run_lm(args, device, n_cells: int):
+    """The reference's language-model Hodgkin-Huxley network shape (`n_cells` point
+    neurons, 100 KineticSynapse inputs each, 80 % excitatory, 32 streams, float32,
+    dt 0.025 ms): one training step = the simulation of 10 tokens x 200 solver steps,
+    the MSE of the voltages to a target, the adjoint, and Adam (capturable) on the
+    synaptic weights, replayed as one CUDA graph; reported per solver step beside
+    the published H100 figure."""
+    import torch
+
+    from jaxley_pytorch_b200.graphs import GraphedIteration
+    from jaxley_pytorch_b200.network import NetworkSimulation, config_lm
+
+    prob = config_lm(n_cells=n_cells, n_tokens=args.lm_tokens)
+    T = prob.n_steps
+    net = NetworkSimulation(prob, dtype=torch.float32, device=device, checkpoint=50, threads=256,
+                            max_block_nodes=256, init_steady=True)
+    (ty,) = net.types
+    with torch.no_grad():
+        target = net.run(net.model.pscale, [[ty.params[0] * 1.2] + ty.params[1:]]).detach()
+
+    def run(w):
+        return net.run(net.model.pscale, [[w] + ty.params[1:]])
+
+    def loss_fn(rec):
+        return ((rec - target) ** 2).mean()
+
+    w = ty.params[0].clone().requires_grad_(True)
+    it = GraphedIteration(net, loss_fn, w, optimizer=torch.optim.Adam([w], lr=1e-6, capturable=True),
+                          warmup=1, run=run)
+    it.replay()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    reps = 2
+    e0.record()
+    for _ in range(reps):
+        it.replay()
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / reps
+    per_step = ms / T
+    h100 = H100_MS_PER_SOLVER_STEP.get(n_cells)
+    return {"workload": f"lm_hh_{n_cells}x100_b32_t{T}_train_step", "neurons": n_cells,
+            "synapses": int(ty.E), "batch": 32, "time_steps": T,
+            "ms_per_training_step": ms, "ms_per_solver_step": per_step,
+            "h100_ms_per_solver_step": h100, "speedup_over_h100": h100 / per_step if h100 else None,
+            "synapse_steps_per_s": ty.E * 32 * T / (ms / 1e3),
+            "value": n_cells * 32 * T / (ms / 1e3), "unit": UNIT, "loss": float(it.loss)}
+
+
 def cpu_sample(batch: int, tsteps: int, reps: int = 1):
     """Times the torch CPU restatement of the reference path (forward + autograd
     backward) on `batch` rows x `tsteps` steps of the workload."""
@@ -772,6 +830,8 @@ def main():
         out["serving"] = run_serving(args, device)
     if world == 1 and not args.no_network:
         out["network"] = run_network(args, device)
+    if world == 1 and not args.no_lm:
+        out["lm_network"] = [run_lm(args, device, n) for n in (1024, 2048)]
     if world == 1 and not args.no_fp32_error:
         out["fp32_error"] = fp32_errors(device)
     if rank == 0:

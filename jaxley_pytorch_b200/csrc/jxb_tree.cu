@@ -236,19 +236,22 @@ __global__ void tree_registers_kernel(const T* __restrict__ d, const T* __restri
 }
 
 // Blocks of more than 256 nodes: one CTA of NT threads per block and batch row,
-// node j in thread j % NT, register j / NT (R registers a thread). The children's
-// eliminated contributions and the parents' solutions are exchanged through shared
-// memory, one barrier pair per height or depth level.
+// node j in thread j % NT, register j / NT (R registers a thread for the pivot and
+// the right-hand side). A node's eliminated contribution (lower * upper / pivot and
+// rhs * upper / pivot) goes to shared memory once, on the level after its own
+// elimination, where its parent gathers it; the back-substitution passes the
+// parents' solutions through shared memory the same way. One barrier per height
+// and per depth level.
 template <typename T, int R>
-__global__ void tree_registers_cta_kernel(const T* __restrict__ d, const T* __restrict__ l,
-                                          const T* __restrict__ u, const T* __restrict__ s,
-                                          T* __restrict__ x, JxbRegSchedule sc) {
+__global__ void __launch_bounds__(1024) tree_registers_cta_kernel(const T* __restrict__ d, const T* __restrict__ l,
+                                                                  const T* __restrict__ u, const T* __restrict__ s,
+                                                                  T* __restrict__ x, JxbRegSchedule sc) {
   extern __shared__ __align__(16) char smem_raw[];
   const int blk = blockIdx.x;
   const int64_t row = blockIdx.y;
   const int tid = threadIdx.x, NT = blockDim.x;
   const int W = NT * R;
-  T* A = (T*)smem_raw;  // W: lower * upper / pivot of every node
+  T* A = (T*)smem_raw;  // W: lower * upper / pivot of eliminated nodes
   T* Bv = A + W;        // W: rhs * upper / pivot, later the solution
   const int start = sc.block_info[4 * blk + 0];
   const int len = sc.block_info[4 * blk + 1];
@@ -259,29 +262,31 @@ __global__ void tree_registers_cta_kernel(const T* __restrict__ d, const T* __re
   const int* dep = sc.rel_depth + (size_t)blk * W;
   const int* kid = sc.rel_children + (size_t)blk * sc.num_slots * W;
   const int64_t base = row * sc.n_nodes + start;
-  T dv[R], sv[R], lv[R], uv[R];
+  T dv[R], sv[R];
+  int hv[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int j = tid + NT * r;
     const bool in = j < len;
     dv[r] = in ? d[base + j] : T(1);
     sv[r] = in ? s[base + j] : T(0);
-    lv[r] = in ? l[base + j] : T(0);
-    uv[r] = in ? u[base + j] : T(0);
+    hv[r] = in ? hgt[j] : -1;
   }
   for (int h = 1; h <= levels; ++h) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int j = tid + NT * r;
-      const T f = uv[r] / dv[r];
-      A[j] = lv[r] * f;
-      Bv[j] = sv[r] * f;
+      if (hv[r] == h - 1) {  // eliminated on the previous level (leaves: height 0)
+        const T f = u[base + j] / dv[r];
+        A[j] = l[base + j] * f;
+        Bv[j] = sv[r] * f;
+      }
     }
     __syncthreads();
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int j = tid + NT * r;
-      if (j < len && hgt[j] == h) {
+      if (hv[r] == h) {
         for (int k = 0; k < sc.num_slots; ++k) {
           const int c = kid[k * W + j];
           if (c >= 0) {
@@ -291,35 +296,24 @@ __global__ void tree_registers_cta_kernel(const T* __restrict__ d, const T* __re
         }
       }
     }
-    __syncthreads();
   }
-  // Back-substitution by depth from the roots; Bv holds the solution of every node
-  // whose depth is done.
-  T xv[R];
-#pragma unroll
-  for (int r = 0; r < R; ++r) {
-    xv[r] = sv[r] / dv[r];
-    Bv[tid + NT * r] = xv[r];
-  }
-  __syncthreads();
-  for (int k = 1; k <= depth; ++k) {
+  __syncthreads();  // every contribution read before Bv holds solutions
+  for (int k = 0; k <= depth; ++k) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int j = tid + NT * r;
-      if (j < len && dep[j] == k) xv[r] = (sv[r] - lv[r] * Bv[par[j]]) / dv[r];
-    }
-    __syncthreads();
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-      const int j = tid + NT * r;
-      if (j < len && dep[j] == k) Bv[j] = xv[r];
+      if (j < len && dep[j] == k) {
+        const T xp = k > 0 ? Bv[par[j]] : T(0);
+        sv[r] = (sv[r] - l[base + j] * xp) / dv[r];
+        Bv[j] = sv[r];
+      }
     }
     __syncthreads();
   }
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int j = tid + NT * r;
-    if (j < len) x[base + j] = xv[r];
+    if (j < len) x[base + j] = sv[r];
   }
 }
 

@@ -109,7 +109,8 @@ class NetworkSimulation:
     parameters (lists of `(E,)` tensors per synapse type, in the reference order)."""
 
     def __init__(self, problem: Problem, dtype=torch.float32, device="cuda", checkpoint: int = 50,
-                 threads: int = 256, max_block_nodes: int = 256, rows_per_item: int = 1):
+                 threads: int = 256, max_block_nodes: int = 256, rows_per_item: int = 1,
+                 init_steady: bool = False):
         if not problem.synapses:
             raise ValueError("the problem has no synapses (use Simulation)")
         self.problem = problem
@@ -118,6 +119,7 @@ class NetworkSimulation:
                               rows_per_item=rows_per_item)
         self.low = low = self.sim.low
         self.model = self.sim.model
+        self.init_steady = bool(init_steady)  # channel gates start at their steady state
         self.dtype, self.device = dtype, torch.device(device)
         self.B = low.batch
         self.checkpoint = int(checkpoint)
@@ -172,7 +174,7 @@ class NetworkSimulation:
         m, low, B = self.model, self.low, self.B
         state = m.initial_state()
         rec = self._zeros(T + 1, B, low.n_rec)
-        m.launch_forward(m.args(state, 0, 0, rec, mode=1, pscale=pscale))
+        m.launch_forward(m.args(state, 0, 0, rec, mode=2 if self.init_steady else 1, pscale=pscale))
         lin = self._zeros(self.syn_size)
         cst = self._zeros(self.syn_size)
         K = self.checkpoint
@@ -351,4 +353,56 @@ def config_network(n_cells: int = 2048, ncomp: int = 4, k: int = 64, batch: int 
                                 params=params, param_names=[f"{name}_{p}" for p in pnames],
                                 state=np.zeros((1, n_cells * k)) if model == 0 else None))
     prob.synapses = syns
+    return prob
+
+
+def config_lm(n_cells: int = 2048, k_in: int = 100, exc_frac: float = 0.8, batch: int = 32,
+              n_tokens: int = 10, steps_per_token: int = 200, seed: int = 0, dt: float = 0.025,
+              input_scale: float = 6.0, w_exc: float = 0.02, w_inh: float = 0.1) -> Problem:
+    """The Hodgkin-Huxley network of the reference's character-level language model
+    (`examples/language_modeling/models.py:66-72, 74-100, 128-215`, published H100
+    throughput in its README:94-116): `n_cells` point neurons (one compartment,
+    radius 10 um, length 20 um, HH, v = -65 mV at steady state), `k_in`
+    KineticSynapse inputs per neuron on its compartment, `exc_frac` of the neurons
+    excitatory and `exc_frac * k_in` of every neuron's inputs drawn from them
+    (distinct presynaptic cells, no autapses), excitatory inputs first; excitatory
+    synapses e_syn 0 mV, beta 0.2 /ms, inhibitory -80 mV, 0.1 /ms (alpha 1 /ms, v_th
+    -20 mV, delta 2 mV); gS = w * (100 / k_in) mS/cm^2 times a log-normal(0, 0.5)
+    factor, converted to uS on the target's area. Input: `batch` streams of
+    `n_tokens` random tokens, each held for `steps_per_token` steps as a constant
+    current of N(0, input_scale) uA/cm^2 per neuron (converted to nA)."""
+    from . import synth
+
+    rng = np.random.default_rng(seed)
+    radius, length = 10.0, 20.0
+    cells = [synth.morphology([-1], [1], [np.full(1, radius)], [np.full(1, length)]) for _ in range(n_cells)]
+    chans = [[("HH", np.arange(1), "HH", {})] for _ in range(n_cells)]
+    T = n_tokens * steps_per_token
+    prob = synth.assemble(cells, chans, batch=1, dt=dt, n_steps=T, v0=-65.0,
+                          recordings=[("v", c, (0, 0)) for c in range(n_cells)])
+    area_cm2 = 2 * np.pi * radius * length * 1e-8
+    n_exc = int(round(exc_frac * n_cells))
+    k_exc = int(round(exc_frac * k_in))
+    pre_cells = np.empty((n_cells, k_in), dtype=np.int64)
+    for j in range(n_cells):
+        for lo, hi, kk, col in ((0, n_exc, k_exc, 0), (n_exc, n_cells, k_in - k_exc, k_exc)):
+            pool = np.arange(lo, hi)
+            pool = pool[pool != j]
+            pre_cells[j, col:col + kk] = rng.choice(pool, size=kk, replace=False)
+    pre = pre_cells.reshape(-1)
+    post = np.repeat(np.arange(n_cells), k_in)
+    exc = pre < n_exc
+    w = np.where(exc, w_exc, w_inh) * (100.0 / k_in) * np.exp(rng.normal(0.0, 0.5, len(pre)))
+    gs = w * area_cm2 * 1e3  # mS/cm^2 over the target's area -> uS
+    params = [gs, np.where(exc, 0.0, -80.0), np.ones(len(pre)), np.where(exc, 0.2, 0.1),
+              np.full(len(pre), -20.0), np.full(len(pre), 2.0)]
+    names = ["gS", "e_syn", "alpha", "beta", "v_th", "delta"]
+    prob.synapses = [SynapseType(model=KINETIC, name="KineticSynapse", pre=pre, post=post, k=k_in,
+                                 targets=np.arange(n_cells), params=params,
+                                 param_names=[f"KineticSynapse_{p}" for p in names],
+                                 state=np.zeros((1, len(pre))))]
+    tokens = rng.normal(0.0, input_scale, size=(batch, n_cells, n_tokens)) * area_cm2 * 1e3  # nA
+    prob.stim_inds = np.arange(n_cells, dtype=np.int64)
+    prob.stim = np.repeat(tokens, steps_per_token, axis=-1)
+    prob.batch = batch
     return prob
