@@ -246,7 +246,14 @@ typedef struct JxbSimArgs_ {
   const int32_t* clamp_col;
   const void* clamp;          /* (clamp_steps, clamp_rows, n_clamp) */
   int32_t n_clamp, clamp_steps, clamp_rows, pad6;
+  /* Optional failure flag (device int32, may be null): a launch whose final states
+   * (forward) or state adjoints and parameter gradients (adjoint) hold a value that is
+   * not finite ORs JXB_NONFINITE into it. The host reads and clears it between
+   * launches; the kernels never stop or fault on a non-finite value. */
+  int32_t* status;
 } JxbSimArgs;
+
+enum { JXB_NONFINITE = 1 };
 
 int jxb_sim_forward(const JxbSimArgs* args, void* stream);
 int jxb_sim_backward(const JxbSimArgs* args, void* stream);
@@ -316,7 +323,11 @@ typedef struct {
   void* g_pre;                /* (n_syn, batch) scratch for the presynaptic sum */
   void* g_post;               /* (batch, n_syn / k) scratch for the postsynaptic sum */
   int32_t need;               /* bit mask of parameters that need gradients */
-  int32_t inv_width, n_pre_nodes, pad;
+  int32_t inv_width, n_pre_nodes;
+  int32_t accumulate;         /* 0: g_v and g_params are overwritten (the op); 1: the step's
+                                 voltage gradient is added to g_v (presynaptic and target
+                                 nodes) and its parameter gradients to g_params, as an adjoint
+                                 that sums over steps does; g_post is then unused */
   const int32_t* inv;         /* (n_pre_nodes, inv_width) synapses of every pre node */
   const int32_t* pre_nodes;   /* (n_pre_nodes,) */
 } JxbSynArgs;

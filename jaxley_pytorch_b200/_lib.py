@@ -14,6 +14,7 @@ _HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(_HERE, "_build", "libjxb.so")
 
 JXB_OK = 0
+JXB_NONFINITE = 1  # bit of JxbSimArgs.status: a launch produced a value that is not finite
 F32, F64 = 0, 1
 
 _p = C.c_void_p
@@ -77,6 +78,7 @@ class JxbSimArgs(C.Structure):
         ("syn_ptr", _p), ("syn_off", _p), ("syn_rs", _p), ("g_syn_lin", _p), ("g_syn_const", _p),
         ("clamp_ptr", _p), ("clamp_slot", _p), ("clamp_col", _p), ("clamp", _p),
         ("n_clamp", C.c_int32), ("clamp_steps", C.c_int32), ("clamp_rows", C.c_int32), ("pad6", C.c_int32),
+        ("status", _p),
     ]
 
 
@@ -90,7 +92,7 @@ class JxbSynArgs(C.Structure):
         ("s_new", _p), ("current", _p), ("lin", _p), ("cst", _p),
         ("g_s_new", _p), ("g_current", _p), ("g_lin", _p), ("g_const", _p),
         ("g_s", _p), ("g_v", _p), ("g_params", _p), ("g_pre", _p), ("g_post", _p),
-        ("need", C.c_int32), ("inv_width", C.c_int32), ("n_pre_nodes", C.c_int32), ("pad", C.c_int32),
+        ("need", C.c_int32), ("inv_width", C.c_int32), ("n_pre_nodes", C.c_int32), ("accumulate", C.c_int32),
         ("inv", _p), ("pre_nodes", _p),
     ]
 

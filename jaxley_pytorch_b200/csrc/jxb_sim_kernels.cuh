@@ -660,6 +660,12 @@ __device__ __forceinline__ void run_steps(const JxbSimArgs& a, const JxbBlock& b
   __syncthreads();
 }
 
+// ORs JXB_NONFINITE into the launch's status flag when any thread of the CTA saw a
+// value that is not finite (all threads of the CTA call this).
+__device__ __forceinline__ void report_nonfinite(const JxbSimArgs& a, int bad) {
+  if (__syncthreads_or(bad) && threadIdx.x == 0 && a.status) atomicOr(a.status, JXB_NONFINITE);
+}
+
 // Work areas of the CTA: dynamic shared memory, or (GM) the item's range of the
 // caller's global scratch for blocks too large for shared memory.
 template <bool GM>
@@ -689,13 +695,19 @@ __device__ __forceinline__ void sim_forward_body(const JxbSimArgs& a, const JxbS
   // adjoint that then skips its recompute (`traj_stored`).
   run_steps<T>(a, blk, item.block, row0, rows, sm, dt, a.t0, nsteps, a.mode, a.n_rec > 0, a.ckpt != nullptr,
                (T*)a.traj, nullptr, (T*)a.traj_piv, a.traj != nullptr && nsteps > 0);
-  // Write the resident states back.
+  // Write the resident states back (and flag values that are not finite).
   const int ns = blk.n_slots;
+  int bad = 0;
   for (int r = 0; r < rows; ++r) {
     T* g = (T*)a.state + (size_t)(row0 + r) * a.n_slots + blk.slot0;
     const T* s = sm.st + (size_t)r * ns;
-    for (int q = threadIdx.x; q < ns; q += blockDim.x) g[q] = s[q];
+    for (int q = threadIdx.x; q < ns; q += blockDim.x) {
+      const T val = s[q];
+      g[q] = val;
+      bad |= !isfinite(val);
+    }
   }
+  report_nonfinite(a, bad);
 }
 
 // Adjoint of one node and row for one step: replays the channel updates from the
@@ -1056,6 +1068,7 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
     }
     __syncthreads();
   }
+  int bad = 0;  // a value that is not finite seen by this thread
   // Fold the nodes' gradient slots into the columns (float64, global), once per
   // launch: a shared per-column buffer would scale with the number of columns,
   // which is large when every cell has its own trainable group.
@@ -1069,15 +1082,23 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
     double* pg = a.pgrad + (size_t)(row0 + r) * a.n_cols;
     for (int k = 0; k < npar; ++k) {
       const int q = sm.gk[po + k];
-      if (q >= 0 && ga[q] != T(0)) atomicAdd(pg + sm.pc[po + k], (double)ga[q]);
+      if (q >= 0 && ga[q] != T(0)) {
+        bad |= !isfinite(ga[q]);
+        atomicAdd(pg + sm.pc[po + k], (double)ga[q]);
+      }
     }
   }
   // Adjoint of the segment's initial state.
   for (int r = 0; r < rows; ++r) {
     T* ga = (T*)a.adj + (size_t)(row0 + r) * a.n_slots + blk.slot0;
     const T* sa = sm.adj + (size_t)r * ns;
-    for (int q = tid; q < ns; q += nthr) ga[q] = sa[q];
+    for (int q = tid; q < ns; q += nthr) {
+      const T val = sa[q];
+      ga[q] = val;
+      bad |= !isfinite(val);
+    }
   }
+  report_nonfinite(a, bad);
 }
 
 // Arguments of a request in a multi-request launch, copied into shared memory.

@@ -203,9 +203,13 @@ __global__ void syn_backward_kernel(JxbSynArgs a, SynP<T> P) {
       else g_pre[(int64_t)e * a.batch + b] = g_vpre;
     }
     gvp_sum = warp_sum(gvp_sum);
-    // The postsynaptic voltage gradient of this row, added to g_v at the target by
+    // The postsynaptic voltage gradient of this row: added to g_v at the target here
+    // when accumulating (one warp owns the (row, target) pair), else by
     // syn_post_kernel.
-    if (lane == 0) ((T*)a.g_post)[b * nt + tgt] = gvp_sum;
+    if (lane == 0) {
+      if (a.accumulate) ((T*)a.g_v)[b * a.n_nodes + node] += gvp_sum;
+      else ((T*)a.g_post)[b * nt + tgt] = gvp_sum;
+    }
   }
   // Sum the parameter gradients over the warps (batch slices), fixed order.
   __syncthreads();
@@ -220,7 +224,8 @@ __global__ void syn_backward_kernel(JxbSynArgs a, SynP<T> P) {
     for (int kk = threadIdx.x; kk < a.k; kk += blockDim.x) {
       T acc = T(0);
       for (int w = 0; w < kBwdWarps; ++w) acc += red[((size_t)w * 6 + q) * a.k + kk];
-      ((T*)a.g_params)[(int64_t)row * a.n_syn + tgt * a.k + kk] = acc;
+      T& out = ((T*)a.g_params)[(int64_t)row * a.n_syn + tgt * a.k + kk];
+      out = a.accumulate ? out + acc : acc;
     }
     ++row;
   }
@@ -240,7 +245,8 @@ __global__ void syn_presum_kernel(JxbSynArgs a) {
     const int e = a.inv[(int64_t)j * a.inv_width + q];
     if (e >= 0) acc += g_pre[(int64_t)e * a.batch + b];
   }
-  ((T*)a.g_v)[b * a.n_nodes + a.pre_nodes[j]] = acc;
+  T& out = ((T*)a.g_v)[b * a.n_nodes + a.pre_nodes[j]];
+  out = a.accumulate ? out + acc : acc;
 }
 
 template <typename T>
@@ -275,10 +281,13 @@ int bwd(const JxbSynArgs& a, cudaStream_t st) {
   SynP<T> P;
   for (int q = 0; q < 6; ++q) P.p[q] = (const T*)a.p[q];
   const int nt = a.n_syn / a.k;
-  cudaError_t e = cudaMemsetAsync(a.g_v, 0, sizeof(T) * (size_t)a.batch * a.n_nodes, st);
-  if (e != cudaSuccess) {
-    set_err("cudaMemsetAsync", e);
-    return JXB_ERR_LAUNCH;
+  cudaError_t e = cudaSuccess;
+  if (!a.accumulate) {  // the op's g_v: zero where neither sum writes
+    e = cudaMemsetAsync(a.g_v, 0, sizeof(T) * (size_t)a.batch * a.n_nodes, st);
+    if (e != cudaSuccess) {
+      set_err("cudaMemsetAsync", e);
+      return JXB_ERR_LAUNCH;
+    }
   }
   const size_t stage = sizeof(T) * (size_t)a.k * a.batch;
   const size_t smem = sizeof(T) * (size_t)kBwdWarps * 6 * a.k + (stage <= (size_t)kStageBytes ? stage : 0);
@@ -296,7 +305,7 @@ int bwd(const JxbSynArgs& a, cudaStream_t st) {
   const int64_t n1 = (int64_t)a.n_pre_nodes * a.batch;
   if (n1 > 0) syn_presum_kernel<T><<<(unsigned)((n1 + threads - 1) / threads), threads, 0, st>>>(a);
   const int64_t n2 = (int64_t)nt * a.batch;
-  syn_post_kernel<T><<<(unsigned)((n2 + threads - 1) / threads), threads, 0, st>>>(a);
+  if (!a.accumulate) syn_post_kernel<T><<<(unsigned)((n2 + threads - 1) / threads), threads, 0, st>>>(a);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_err("syn_backward_kernel", e);
@@ -318,7 +327,9 @@ int check(const JxbSynArgs* a, bool backward) {
     if (a->model == 0 && !a->s_new) return JXB_ERR_ARG;
     if (a->store_current && !a->current) return JXB_ERR_ARG;
   } else {
-    if (!a->g_post || !a->g_lin || !a->g_const || !a->g_v || !a->g_pre || !a->inv || !a->pre_nodes) return JXB_ERR_ARG;
+    if ((!a->accumulate && !a->g_post) || !a->g_lin || !a->g_const || !a->g_v || !a->g_pre || !a->inv ||
+        !a->pre_nodes)
+      return JXB_ERR_ARG;
     if (a->model == 0 && !a->g_s) return JXB_ERR_ARG;
     if (a->need && !a->g_params) return JXB_ERR_ARG;
   }

@@ -214,11 +214,10 @@ class NetworkSimulation:
         s_seg = [self._zeros(K + 1, B, ty.E) if ty.kinetic else None for ty in self.types]
         g_s = [self._zeros(B, ty.E) if ty.kinetic else None for ty in self.types]
         g_s2 = [self._zeros(B, ty.E) if ty.kinetic else None for ty in self.types]
-        g_v = self._zeros(B, low.n_slots)
         g_pre = [self._zeros(ty.E, B) for ty in self.types]
-        g_post = [self._zeros(B, ty.T) for ty in self.types]
         n_par = [len(p) for p in syn_params]
-        g_par = [self._zeros(n_par[q], ty.E) for q, ty in enumerate(self.types)]
+        # the synapse adjoint adds every step's parameter gradients here and its
+        # voltage gradients straight into the state adjoint (accumulate mode)
         g_par_acc = [self._zeros(n_par[q], ty.E) for q, ty in enumerate(self.types)]
         states = saved["states"]
         rec_grad = rec_grad.contiguous()
@@ -253,15 +252,13 @@ class NetworkSimulation:
                     b.g_lin = g_lin.data_ptr() + off * g_lin.element_size()
                     b.g_const = g_cst.data_ptr() + off * g_cst.element_size()
                     b.g_s = g_s2[q].data_ptr() if ty.kinetic else None
-                    b.g_v = g_v.data_ptr()
+                    b.g_v = adj.data_ptr()
+                    b.accumulate = 1
                     b.need = (1 << n_par[q]) - 1
-                    b.g_params = g_par[q].data_ptr()
+                    b.g_params = g_par_acc[q].data_ptr()
                     b.g_pre = g_pre[q].data_ptr()
-                    b.g_post = g_post[q].data_ptr()
                     _lib.check(_lib.load().jxb_synapse_backward(C.byref(b), _stream()), "jxb_synapse_backward")
                     self.syn_launches += 1
-                    adj.add_(g_v)
-                    g_par_acc[q].add_(g_par[q])
                     if ty.kinetic:
                         g_s[q], g_s2[q] = g_s2[q], g_s[q]
         return pgrad, g_par_acc
@@ -279,6 +276,8 @@ class NetworkSimulation:
         if torch.is_grad_enabled() and (pscale.requires_grad or any(p.requires_grad for p in flat)):
             return _NetFn.apply(self, T, [len(ps) for ps in syn_params], pscale, *flat)
         rec, _ = self.forward_raw(pscale.detach().contiguous(), [[p.detach() for p in ps] for ps in syn_params], T)
+        if self.sim.check_finite:
+            self.model.check_finite("network simulation")
         return rec.permute(1, 2, 0)
 
 
@@ -291,6 +290,8 @@ class _NetFn(torch.autograd.Function):
             params.append([p.detach().to(net.dtype).contiguous() for p in flat[q:q + c]])
             q += c
         rec, saved = net.forward_raw(ps, params, T, keep=True)
+        if net.sim.check_finite:
+            net.model.check_finite("network simulation")
         ctx.net, ctx.T, ctx.counts, ctx.saved_data = net, T, counts, saved
         ctx.params = params
         ctx.save_for_backward(ps)
@@ -303,6 +304,8 @@ class _NetFn(torch.autograd.Function):
         net = ctx.net
         rec_grad = grad_out.to(net.dtype).permute(2, 0, 1).contiguous()
         pgrad, g_par = net.backward_raw(ps, ctx.params, ctx.T, ctx.saved_data, rec_grad)
+        if net.sim.check_finite:
+            net.model.check_finite("network adjoint")
         out = [None, None, None, pgrad.to(ctx.dtypes[0])]
         dts = ctx.dtypes[1]
         q = 0

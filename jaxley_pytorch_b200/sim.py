@@ -133,6 +133,8 @@ class DeviceModel:
             self.t["clamp_slot"] = i(low.clamp_slot)
             self.t["clamp_col"] = i(low.clamp_col)
         self.threads = threads
+        # Failure flag of the launches (JXB_NONFINITE when a result is not finite).
+        self.status = torch.zeros(1, dtype=torch.int32, device=dev)
         self.launches = 0  # kernel launches issued through this model
         self.timed_kind: Optional[str] = None  # "forward"/"backward": record events
         self.events: List = []
@@ -292,6 +294,7 @@ class DeviceModel:
         a.rec_grad = _ptr(rec_grad)
         a.pgrad = _ptr(pgrad)
         a.mode = mode
+        a.status = self.status.data_ptr()
         if self.sched_warps:
             a.sched_ptr = t["sched_ptr"].data_ptr()
             a.sched = t["sched"].data_ptr()
@@ -359,6 +362,18 @@ class DeviceModel:
             e1.record(st)
             self.events.append((e0, e1, args.n_steps))
 
+    def check_finite(self, what: str) -> None:
+        """Raises `FloatingPointError` when a launch since the last check produced a value
+        that is not finite (the kernels' status flag; reading it synchronises the
+        device). Skipped while a CUDA graph is being captured: the flag stays set until
+        the next check outside a capture."""
+        if torch.cuda.is_current_stream_capturing():
+            return
+        flag = int(self.status.item())
+        if flag:
+            self.status.zero_()
+            raise FloatingPointError(f"the {what} produced values that are not finite (NaN or inf)")
+
     def launch_forward(self, args: _lib.JxbSimArgs, stream=None) -> None:
         self._launch("forward", _lib.load().jxb_sim_forward, args, stream)
 
@@ -385,7 +400,9 @@ class Simulation:
     `store_fraction` of the free device memory). `threads` is the CTA size of the
     launches; `forward_threads` (default: `threads`) that of the forward launches,
     which with `forward_wide` (float32, up to 256 threads) use kernels of two CTAs per
-    SM with up to 128 registers a thread instead of 64.
+    SM with up to 128 registers a thread instead of 64. With `check_finite`, a run
+    whose final states or gradients hold a NaN or an infinity raises
+    `FloatingPointError` (the kernels flag it on the device).
     """
 
     def __init__(self, problem: Problem, dtype=torch.float32, device="cuda",
@@ -394,7 +411,8 @@ class Simulation:
                  low: Optional[Lowered] = None, checkpoint: int = 100, threads: int = 256,
                  keep_currents: bool = True, programs: bool = True, schedule: bool = True,
                  store_trajectory="auto", store_fraction: float = 0.5,
-                 forward_threads: Optional[int] = None, forward_wide: bool = False):
+                 forward_threads: Optional[int] = None, forward_wide: bool = False,
+                 check_finite: bool = True):
         self.problem = problem
         self.low = low if low is not None else lower(problem, max_block_nodes=max_block_nodes,
                                                      keep_currents=keep_currents)
@@ -409,6 +427,10 @@ class Simulation:
         self.store_trajectory = store_trajectory
         self.store_fraction = float(store_fraction)
         self._store_free: Optional[int] = None
+        # Raise FloatingPointError when a run's final states or gradients are not
+        # finite (as the reference's trainer does for a non-finite loss,
+        # training/engine.py:229-230); one device synchronisation per run.
+        self.check_finite = bool(check_finite)
 
     def n_steps(self, n_steps: Optional[int] = None) -> int:
         return self.low.n_steps if n_steps is None else int(n_steps)
@@ -513,6 +535,8 @@ class Simulation:
             out = _IntegrateFn.apply(pscale, self, T)
             return out
         rec, state = self.forward_raw(pscale.detach().contiguous(), T)
+        if self.check_finite:
+            self.model.check_finite("simulation")
         out = rec.permute(1, 2, 0)
         return (out, state) if return_state else out
 
@@ -543,6 +567,8 @@ class _IntegrateFn(torch.autograd.Function):
             ctx.save_for_backward(ps, ckpt)
         ctx.sim, ctx.T = sim, T
         ctx.in_dtype = pscale.dtype
+        if sim.check_finite:
+            sim.model.check_finite("simulation")
         return rec.permute(1, 2, 0)
 
     @staticmethod
@@ -555,4 +581,6 @@ class _IntegrateFn(torch.autograd.Function):
         else:
             ps, ckpt = ctx.saved_tensors
             pgrad = sim.backward_raw(ps, ctx.T, ckpt, rec_grad)
+        if sim.check_finite:
+            sim.model.check_finite("adjoint")
         return pgrad.to(ctx.in_dtype), None, None
