@@ -409,3 +409,60 @@ def config_lm(n_cells: int = 2048, k_in: int = 100, exc_frac: float = 0.8, batch
     prob.stim = np.repeat(tokens, steps_per_token, axis=-1)
     prob.batch = batch
     return prob
+
+
+# --------------------------------------------------------------------------------------
+# Several GPUs: the batch rows are sharded over the ranks; parameters shared by all rows
+# (the synaptic weights of a training step) get one summed gradient.
+# --------------------------------------------------------------------------------------
+def shard_rows(problem: Problem, rank: int, world: int) -> Problem:
+    """The rows `[rank * B // world, (rank + 1) * B // world)` of a problem's batch as a
+    problem of their own: every array with a batch dimension (parameters, states,
+    stimuli, clamps, kinetic synapse states) is sliced, shared arrays are kept."""
+    import copy
+
+    B = int(problem.batch)
+    lo, hi = rank * B // world, (rank + 1) * B // world
+    if hi <= lo:
+        raise ValueError(f"rank {rank} of {world} gets no rows of a batch of {B}")
+
+    def rows(a, core: int):
+        a = np.asarray(a)
+        return a[lo:hi] if a.ndim > core and a.shape[0] == B and B > 1 else a
+
+    p = copy.copy(problem)
+    p.params = {k: rows(v, 1) for k, v in problem.params.items()}
+    p.states = {k: rows(v, 1) for k, v in problem.states.items()}
+    p.axial = rows(problem.axial, 1)
+    p.stim = rows(problem.stim, 2) if problem.stim is not None else None
+    p.clamps = [(k, i, rows(v, 2)) for k, i, v in problem.clamps]
+    syns = []
+    for syn in problem.synapses:
+        s = copy.copy(syn)
+        if syn.state is not None:
+            s.state = rows(syn.state, 1)
+        if syn.current is not None:
+            s.current = rows(syn.current, 1)
+        syns.append(s)
+    p.synapses = syns
+    p.batch = hi - lo
+    return p
+
+
+def allreduce_gradients(grads: Sequence[torch.Tensor], group=None) -> None:
+    """Sums gradients over the ranks of `group` in place with one collective: the
+    tensors are packed into one buffer, all-reduced (sum) and unpacked. A rank's
+    gradients must come from a loss that is its rows' share of the whole batch's
+    loss (e.g. the squared errors of its rows divided by the number of rows of all
+    ranks), so that the sum is the whole batch's gradient."""
+    import torch.distributed as dist
+
+    if not dist.is_initialized() or dist.get_world_size(group) == 1 or not grads:
+        return
+    flat = torch.cat([g.reshape(-1) for g in grads])
+    dist.all_reduce(flat, op=dist.ReduceOp.SUM, group=group)
+    q = 0
+    for g in grads:
+        n = g.numel()
+        g.copy_(flat[q:q + n].view_as(g))
+        q += n

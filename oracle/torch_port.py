@@ -165,10 +165,40 @@ def _current(ch, st, v, prm):
     return torch.zeros_like(v)
 
 
+def _synapse_terms(syn, prm, s, v, area_post, dt):
+    """One synapse type's step (modules/network.py:434-478, synapses/kinetic.py:37-63,
+    synapses/sigmoid_rate.py:43-50) in torch: the new kinetic state and the per-target
+    slope and offset of the summed synaptic current, `(B, E)`, `(B, T)`, `(B, T)`."""
+    pre = torch.as_tensor(np.asarray(syn.pre, dtype=np.int64))
+    tgt = torch.as_tensor(np.repeat(np.asarray(syn.targets, dtype=np.int64), syn.k))
+    vpre, vp = v[:, pre], v[:, tgt]
+    gs = prm[0]
+    if syn.model == 0:
+        e_syn, alpha, beta, v_th, delta = prm[1:6]
+        a = alpha * torch.sigmoid((vpre - v_th) / delta)
+        rate = a + beta
+        s_inf = a / rate
+        s = s_inf + (s - s_inf) * torch.exp(-dt * rate)
+        i0 = gs * s * (vp - e_syn)
+        i1 = gs * s * ((vp + DIFF) - e_syn)
+    else:
+        x_off, slope = prm[1:3]
+        i0 = -gs * torch.sigmoid((vpre - x_off) * slope)
+        i1 = -gs * torch.sigmoid(((vpre + DIFF) - x_off) * slope)
+    d0 = i0 / area_post * 100_000
+    d1 = i1 / area_post * 100_000
+    vt = (d1 - d0) / DIFF
+    B = v.shape[0]
+    return s, vt.reshape(B, -1, syn.k).sum(-1), (d0 - vt * vp).reshape(B, -1, syn.k).sum(-1)
+
+
 def integrate(problem, params: Dict[str, torch.Tensor], n_steps: Optional[int] = None,
-              dtype=torch.float32, init_steady: bool = False) -> torch.Tensor:
+              dtype=torch.float32, init_steady: bool = False,
+              syn_params: Optional[List[List[torch.Tensor]]] = None) -> torch.Tensor:
     """Recordings `(B, n_rec, T + 1)`; `params` maps parameter names to `(B, n)` or
-    `(n,)` tensors (autograd flows into them)."""
+    `(n,)` tensors, `syn_params` gives every synapse type's parameters as `(E,)`
+    tensors in the reference order (default: the problem's); autograd flows into
+    both."""
     p = problem
     B, n = p.batch, p.n_nodes
     T = p.n_steps if n_steps is None else int(n_steps)
@@ -246,6 +276,13 @@ def integrate(problem, params: Dict[str, torch.Tensor], n_steps: Optional[int] =
             s = s.index_add(1, lev, -s[:, parent_t[lev]] * ln[:, lev])
         return s[:, inv_order]
 
+    syns = []
+    for q, syn in enumerate(p.synapses):
+        prm = (syn_params[q] if syn_params is not None
+               else [torch.as_tensor(np.asarray(x), dtype=dtype) for x in syn.params])
+        s0 = (torch.as_tensor(np.broadcast_to(np.asarray(syn.state), (B, len(syn.pre))).copy(), dtype=dtype)
+              if syn.model == 0 else None)
+        syns.append([syn, prm, s0, area[:, np.asarray(syn.post, dtype=np.int64)]])
     currents(st, st["v"])
     recs = [torch.stack([st[nm][:, i] for nm, i in p.recordings], dim=1)]
     for t in range(T):
@@ -257,6 +294,13 @@ def integrate(problem, params: Dict[str, torch.Tensor], n_steps: Optional[int] =
             for key, val in _update(ch, chs, dt, v[:, inds], prm).items():
                 st[key] = st[key].index_copy(1, inds, val)
         lin, const = currents(st, v)
+        for entry in syns:
+            syn, prm, s_old, area_post = entry
+            s_new, l_t, c_t = _synapse_terms(syn, prm, s_old, v, area_post, dt)
+            entry[2] = s_new
+            tg = torch.as_tensor(np.asarray(syn.targets, dtype=np.int64))
+            lin = lin + torch.zeros(B, n, dtype=dtype).index_add(1, tg, l_t)
+            const = const + torch.zeros(B, n, dtype=dtype).index_add(1, tg, -c_t)
         i_ext = torch.zeros(B, n, dtype=dtype)
         if stim is not None and len(stim_inds):
             cur = torch.broadcast_to(stim[:, :, t], (B, len(stim_inds))) / area[:, stim_inds] * 100_000
