@@ -27,6 +27,11 @@ CaLVA                 ``mech/channels/l5pc.py:737``             11
 CaPump                ``mech/channels/l5pc.py:814``             12
 CaNernstReversal      ``mech/channels/l5pc.py:872``             13
 H                     ``mech/channels/l5pc.py:919``             14
+Na                    ``channels/pospischil.py:74``              15
+K                     ``channels/pospischil.py:143``             16
+Km                    ``channels/pospischil.py:197``             17
+CaL                   ``channels/pospischil.py:252``             18
+CaT                   ``channels/pospischil.py:318``             19
 ====================  =======================================  ====
 """
 from __future__ import annotations
@@ -101,13 +106,23 @@ SPECS: Dict[str, ChannelSpec] = {
     ),
     "H": ChannelSpec(14, _p(("gH", 1e-5), ("/eH", -45.0)), _p(("m", 0.0),), "i_H",
                      ohmic_g=(0,)),
+    "Na": ChannelSpec(15, _p(("gNa", 50e-3), ("/eNa", 50.0), ("/vt", -60.0)),
+                      _p(("m", 0.2), ("h", 0.2)), "i_Na", ohmic_g=(0,)),
+    "K": ChannelSpec(16, _p(("gK", 5e-3), ("/eK", -90.0), ("/vt", -60.0)),
+                     _p(("n", 0.2),), "i_K", ohmic_g=(0,)),
+    "Km": ChannelSpec(17, _p(("gKm", 0.004e-3), ("taumax", 4000.0), ("/eK", -90.0)),
+                      _p(("p", 0.2),), "i_K", ohmic_g=(0,)),
+    "CaL": ChannelSpec(18, _p(("gCaL", 0.1e-3), ("/eCa", 120.0)),
+                       _p(("q", 0.2), ("r", 0.2)), "i_Ca", ohmic_g=(0,)),
+    "CaT": ChannelSpec(19, _p(("gCaT", 0.4e-4), ("vx", 2.0), ("/eCa", 120.0)),
+                       _p(("u", 0.2),), "i_Ca"),
 }
 
 # Reference modules whose classes of the same name are the ones restated here (the
 # `pumps/` package has different classes called `CaPump` and `CaNernstReversal`).
 _REFERENCE_MODULES = {
     "HH": "jaxley_pytorch.channels.hh",
-    "Leak": "jaxley_pytorch.channels.pospischil",
+    **{k: "jaxley_pytorch.channels.pospischil" for k in ("Leak", "Na", "K", "Km", "CaL", "CaT")},
 }
 _L5PC_MODULE = "jaxley_pytorch.mech.channels.l5pc"
 

@@ -12,7 +12,9 @@ namespace jxb {
 enum ChannelType {
   CH_HH = 0, CH_LEAK = 1, CH_NATAT = 2, CH_NATS2T = 3, CH_NAPET2 = 4, CH_KPST = 5,
   CH_KTST = 6, CH_SKE2 = 7, CH_SKV3_1 = 8, CH_M = 9, CH_CAHVA = 10, CH_CALVA = 11,
-  CH_CAPUMP = 12, CH_CANERNST = 13, CH_H = 14
+  CH_CAPUMP = 12, CH_CANERNST = 13, CH_H = 14,
+  // channels/pospischil.py: Na, K, Km, CaL, CaT
+  CH_PNA = 15, CH_PK = 16, CH_PKM = 17, CH_PCAL = 18, CH_PCAT = 19
 };
 
 // One channel of a node class: its type and the node-relative slots of its states
@@ -27,13 +29,15 @@ struct ChanEntry {
 enum GateId {
   G_HH_M, G_HH_H, G_HH_N, G_NATAT_M, G_NATAT_H, G_NATS2T_M, G_NATS2T_H, G_NAP_M,
   G_NAP_H, G_KPST_M, G_KPST_H, G_KTST_M, G_KTST_H, G_SKV31_M, G_M_M, G_CAHVA_M,
-  G_CAHVA_H, G_CALVA_M, G_CALVA_H, G_H_M
+  G_CAHVA_H, G_CALVA_M, G_CALVA_H, G_H_M,
+  G_PNA_M, G_PNA_H, G_PK_N, G_PKM_P, G_PCAL_Q, G_PCAL_R, G_PCAT_U
 };
 
 // Gates in alpha/beta form (`solve_gate_exponential`, solver_gate.py:45-53) versus
 // x_inf/tau form (`solve_inf_gate_exponential`, solver_gate.py:67-87).
 __device__ __forceinline__ bool gate_is_alpha_beta(int g) {
-  return g == G_HH_M || g == G_HH_H || g == G_HH_N || g == G_CAHVA_M || g == G_CAHVA_H;
+  return g == G_HH_M || g == G_HH_H || g == G_HH_N || g == G_CAHVA_M || g == G_CAHVA_H ||
+         g == G_PNA_M || g == G_PNA_H || g == G_PK_N || g == G_PCAL_Q || g == G_PCAL_R;
 }
 
 template <typename S> struct Pair { S a, b; };
@@ -157,6 +161,40 @@ __device__ __forceinline__ Pair<S> gate_rates(int g, S v) {
       r.b = fdiv(S(qt), B(20.0) + B(50.0) * rcp(B(1) + save_exp((vs + B(40)) * B(1.0 / 7.0))));
       break;
     }
+    // channels/pospischil.py. The Na and K gates take v - vt and the CaT gate v + vx
+    // (their parameters), passed as `v` by the caller; efun(x) = x_over_expm1(x, 1).
+    case G_PNA_M:  // pospischil.py:124-131
+      r.a = B(0.32) * x_over_expm1(B(-0.25) * (v - B(13)), B(1)) * B(4);
+      r.b = B(0.28) * x_over_expm1(B(0.2) * (v - B(40)), B(1)) * B(5);
+      break;
+    case G_PNA_H:  // pospischil.py:133-140
+      r.a = B(0.128) * save_exp(-(v - B(17)) * B(1.0 / 18.0));
+      r.b = fdiv(S(B(4)), save_exp(-(v - B(40)) * B(0.2)) + B(1));
+      break;
+    case G_PK_N:  // pospischil.py:186-193
+      r.a = B(0.032) * x_over_expm1(B(-0.2) * (v - B(15)), B(1)) * B(5);
+      r.b = B(0.5) * save_exp(-(v - B(10)) * B(1.0 / 40.0));
+      break;
+    case G_PKM_P: {  // pospischil.py:242-249: (p_inf, 1 / tau * taumax); the caller scales
+      S vp = v + B(35);
+      r.a = rcp(B(1) + save_exp(B(-0.1) * vp));
+      r.b = B(3.3) * save_exp(B(0.05) * vp) + save_exp(B(-0.05) * vp);
+      break;
+    }
+    case G_PCAL_Q:  // pospischil.py:301-308
+      r.a = B(0.055) * x_over_expm1((-v - B(27)) * B(1.0 / 3.8), B(1)) * B(3.8);
+      r.b = B(0.94) * save_exp((-v - B(75)) * B(1.0 / 17.0));
+      break;
+    case G_PCAL_R:  // pospischil.py:310-317
+      r.a = B(0.000457) * save_exp((-v - B(13)) * B(1.0 / 50.0));
+      r.b = fdiv(S(B(0.0065)), save_exp((-v - B(15)) * B(1.0 / 28.0)) + B(1));
+      break;
+    case G_PCAT_U: {  // pospischil.py:366-375 (u_inf, 1 / tau)
+      r.a = rcp(B(1) + save_exp((v + B(81)) * B(0.25)));
+      S den = B(3.7) * (B(1) + save_exp((v + B(84)) * B(1.0 / 3.2)));
+      r.b = fdiv(den, B(30.8) + (B(211.4) + save_exp((v + B(113.2)) * B(0.2))));
+      break;
+    }
     default: {  // G_H_M, l5pc.py:973-984
       S ma = B(0.001 * 6.43) * x_over_expm1(v + B(154.9) + B(1e-6), B(11.9));
       S mb = B(0.001 * 193) * save_exp(v * B(1.0 / 33.1));
@@ -175,10 +213,12 @@ template <typename S> __device__ __forceinline__ S save_expm1(S x) { return exm1
 // One exponential-Euler gate step. Returns x'; `e` receives d x'/d x.
 // x * e + x_inf * (1 - e) (solver_gate.py:56-64) is evaluated as
 // x + (x - x_inf) * (e - 1) with e - 1 from expm1: the same value, without the
-// cancellation of 1 - e for slow gates in float32.
+// cancellation of 1 - e for slow gates in float32. `rate_scale` multiplies the
+// 1 / tau of an x_inf/tau gate (Km's 1 / taumax).
 template <typename S, typename B>
-__device__ __forceinline__ S gate_step(int g, S v, B x, B dt, B* e_out) {
+__device__ __forceinline__ S gate_step(int g, S v, B x, B dt, B* e_out, S rate_scale = S(B(1))) {
   Pair<S> r = gate_rates<S>(g, v);
+  if (!gate_is_alpha_beta(g)) r.b = r.b * rate_scale;
   S xinf, em1;
   if (gate_is_alpha_beta(g)) {  // solver_gate.py:45-53: tau = 1/(a+b), x_inf = a*tau
     S sum = r.a + r.b;
@@ -198,6 +238,23 @@ __device__ __forceinline__ B gate_steady(int g, B v) {
   Pair<B> r = gate_rates<B>(g, v);
   if (gate_is_alpha_beta(g)) return fdiv(r.a, r.a + r.b);
   return r.a;
+}
+
+// `init_state` of the Pospischil Km and CaT gates (pospischil.py:232-237, 360-364),
+// which pass their (x_inf, tau) pair to the alpha / (alpha + beta) of the alpha/beta
+// gates: x_inf / (x_inf + tau). `tau_scale` is Km's taumax (1 for CaT).
+template <typename B>
+__device__ __forceinline__ B gate_init_inf_tau(int g, B v, B tau_scale) {
+  Pair<B> r = gate_rates<B>(g, v);
+  const B tau = tau_scale / r.b;
+  return r.a / (r.a + tau);
+}
+
+// The CaT activation s_inf(v + vx) of its current (pospischil.py:350-357).
+template <typename S>
+__device__ __forceinline__ S pcat_sinf(S w) {
+  typedef typename Base<S>::type B;
+  return rcp(B(1) + save_exp(-(w + B(57)) * B(1.0 / 6.2)));
 }
 
 // SKE2 z gate, a function of the calcium concentration (l5pc.py:519-530).
@@ -222,6 +279,11 @@ __device__ __forceinline__ GateLayout gate_layout(int type) {
     case CH_SKV3_1: return {G_SKV31_M, -1, 1};
     case CH_M: return {G_M_M, -1, 1};
     case CH_H: return {G_H_M, -1, 1};
+    case CH_PNA: return {G_PNA_M, G_PNA_H, 3};
+    case CH_PK: return {G_PK_N, -1, 4};
+    case CH_PKM: return {G_PKM_P, -1, 1};
+    case CH_PCAL: return {G_PCAL_Q, G_PCAL_R, 2};
+    case CH_PCAT: return {G_PCAT_U, -1, 1};
     default: return {-1, -1, 0};
   }
 }

@@ -49,7 +49,22 @@ __device__ __forceinline__ void channel_update(const ChanEntry& e, T* x, const P
       x[e.s[0]] = C * lg(x[e.s[2]] / x[e.s[1]]);
       break;
     }
-    default: {  // gated ohmic channels (l5pc.py update_states)
+    case CH_PNA: {  // pospischil.py:91-104, gates of v - vt
+      const T u = v - P(2);
+      x[e.s[0]] = gate_step<T, T>(G_PNA_M, u, x[e.s[0]], dt, nullptr);
+      x[e.s[1]] = gate_step<T, T>(G_PNA_H, u, x[e.s[1]], dt, nullptr);
+      break;
+    }
+    case CH_PK:  // pospischil.py:158-169
+      x[e.s[0]] = gate_step<T, T>(G_PK_N, v - P(2), x[e.s[0]], dt, nullptr);
+      break;
+    case CH_PKM:  // pospischil.py:212-225, tau = taumax / (...)
+      x[e.s[0]] = gate_step<T, T>(G_PKM_P, v, x[e.s[0]], dt, nullptr, T(1) / P(1));
+      break;
+    case CH_PCAT:  // pospischil.py:334-347, gate of v + vx
+      x[e.s[0]] = gate_step<T, T>(G_PCAT_U, v + P(1), x[e.s[0]], dt, nullptr);
+      break;
+    default: {  // gated ohmic channels (l5pc.py update_states; Pospischil CaL)
       GateLayout gl = gate_layout(e.type);
       x[e.s[0]] = gate_step<T, T>(gl.g0, v, x[e.s[0]], dt, nullptr);
       if (gl.g1 >= 0) x[e.s[1]] = gate_step<T, T>(gl.g1, v, x[e.s[1]], dt, nullptr);
@@ -60,8 +75,21 @@ __device__ __forceinline__ void channel_update(const ChanEntry& e, T* x, const P
 
 // `init_state` of one channel entry (steady state at the node voltage).
 template <typename T>
-__device__ __forceinline__ void channel_steady(const ChanEntry& e, T* x, T v) {
+__device__ __forceinline__ void channel_steady(const ChanEntry& e, T* x, const Prm<T>& P, T v) {
   switch (e.type) {
+    case CH_PNA:  // pospischil.py:117-125
+      x[e.s[0]] = gate_steady<T>(G_PNA_M, v - P(2));
+      x[e.s[1]] = gate_steady<T>(G_PNA_H, v - P(2));
+      break;
+    case CH_PK:  // pospischil.py:180-184
+      x[e.s[0]] = gate_steady<T>(G_PK_N, v - P(2));
+      break;
+    case CH_PKM:  // pospischil.py:232-237
+      x[e.s[0]] = gate_init_inf_tau<T>(G_PKM_P, v, P(1));
+      break;
+    case CH_PCAT:  // pospischil.py:360-364
+      x[e.s[0]] = gate_init_inf_tau<T>(G_PCAT_U, v + P(1), T(1));
+      break;
     case CH_HH:  // channels/hh.py:69-86
       x[e.s[0]] = gate_steady<T>(G_HH_M, v);
       x[e.s[1]] = gate_steady<T>(G_HH_H, v);
@@ -128,7 +156,26 @@ __device__ __forceinline__ void channel_current(const ChanEntry& e, T* x, const 
     case CH_CAPUMP:
     case CH_CANERNST:
       return;
-    default: {  // l5pc.py compute_current of the gated channels
+    case CH_PKM: {  // pospischil.py:227-230: E = eK, the third parameter
+      T g = P(0) * x[e.s[0]];
+      slope += g;
+      gge += g * P(2);
+      cur = g * (v - P(2));
+      break;
+    }
+    case CH_PCAT: {  // pospischil.py:349-357: not linear in v, the reference's finite
+      // difference of 1e-3 mV (modules/base.py:3522-3539) gives slope and offset
+      const T g = P(0) * x[e.s[0]], vx = P(1), E = P(2);
+      const T s0 = pcat_sinf<T>(v + vx), s1 = pcat_sinf<T>((v + T(1e-3)) + vx);
+      const T i0 = g * (s0 * s0) * (v - E);
+      const T i1 = g * (s1 * s1) * ((v + T(1e-3)) - E);
+      const T vt = (i1 - i0) * T(1000.0);
+      slope += vt;
+      gge += vt * v - i0;
+      cur = i0;
+      break;
+    }
+    default: {  // l5pc.py compute_current of the gated channels; Pospischil Na, K, CaL
       GateLayout gl = gate_layout(e.type);
       T g = P(0) * gated_G(e, x, gl.e0, gl.g1 >= 0);
       T E = (e.type == CH_CAHVA || e.type == CH_CALVA) ? x[e.s[2]] : P(1);
@@ -222,6 +269,38 @@ __device__ __forceinline__ void channel_current_vjp(const ChanEntry& e, const T*
     case CH_CAPUMP:
     case CH_CANERNST:
       break;
+    case CH_PKM: {
+      T g = P(0), p = x[e.s[0]];
+      T lc, lE;
+      ohmic(g * p, P(2), lc, lE);
+      lam[e.s[0]] += g * lc;
+      G.add(0, p * lc);
+      G.add(2, lE);
+      break;
+    }
+    case CH_PCAT: {
+      // slope s = (i1 - i0) / d and offset q = s v - i0 of the finite difference,
+      // with adjoints -lr x1 and lr; the current slot holds i0.
+      const T d = T(1e-3);
+      const T g = P(0), u = x[e.s[0]], vx = P(1), E = P(2);
+      const Dual<T> a0 = pcat_sinf<Dual<T>>(Dual<T>(v + vx, T(1)));
+      const Dual<T> a1 = pcat_sinf<Dual<T>>(Dual<T>((v + d) + vx, T(1)));
+      const T w0 = v - E, w1 = (v + d) - E;
+      const T i0 = g * u * a0.v * a0.v * w0, i1 = g * u * a1.v * a1.v * w1;
+      const T slope = (i1 - i0) * T(1000.0);
+      const T l_s = lr * (v - x1);  // adjoint of s, q's share included
+      const T l_i1 = l_s * T(1000.0);
+      const T l_i0 = -l_s * T(1000.0) - lr + lI;
+      // d i / d (g, u, E) and d i / d (v + vx) at both voltages
+      const T c0 = u * a0.v * a0.v, c1 = u * a1.v * a1.v;
+      const T dw0 = g * u * T(2) * a0.v * a0.d * w0, dw1 = g * u * T(2) * a1.v * a1.d * w1;
+      G.add(0, l_i0 * c0 * w0 + l_i1 * c1 * w1);
+      G.add(1, l_i0 * dw0 + l_i1 * dw1);
+      G.add(2, -(l_i0 * g * c0 + l_i1 * g * c1));
+      lam[e.s[0]] += l_i0 * g * a0.v * a0.v * w0 + l_i1 * g * a1.v * a1.v * w1;
+      lv += l_i0 * (dw0 + g * c0) + l_i1 * (dw1 + g * c1) + lr * slope;
+      break;
+    }
     default: {
       GateLayout gl = gate_layout(e.type);
       bool ca = e.type == CH_CAHVA || e.type == CH_CALVA;
@@ -315,6 +394,43 @@ __device__ __forceinline__ void channel_update_vjp(const ChanEntry& e, const T* 
       lam[e.s[2]] += C / x[e.s[2]] * le;
       break;
     }
+    case CH_PNA:
+    case CH_PK:
+    case CH_PCAT: {
+      // gates of u = v - vt (Na, K) or v + vx (CaT): d/d vt = -d/du, d/d vx = d/du
+      const bool cat = e.type == CH_PCAT;
+      const int ps = cat ? 1 : 2;
+      const T u = cat ? v + P(1) : v - P(2);
+      const T sgn = cat ? T(1) : T(-1);
+      GateLayout gl = gate_layout(e.type);
+      T lo, lu = T(0);
+      gate_vjp<T>(gl.g0, u, x[e.s[0]], dt, lam[e.s[0]], lo, lu);
+      lam[e.s[0]] = lo;
+      if (gl.g1 >= 0) {
+        gate_vjp<T>(gl.g1, u, x[e.s[1]], dt, lam[e.s[1]], lo, lu);
+        lam[e.s[1]] = lo;
+      }
+      lv += lu;
+      G.add(ps, sgn * lu);
+      break;
+    }
+    case CH_PKM: {
+      T lo, lvk = T(0);
+      const T taumax = P(1);
+      const T pold = x[e.s[0]], ln = lam[e.s[0]];
+      T ee;
+      Dual<T> xn = gate_step<Dual<T>, T>(G_PKM_P, Dual<T>(v, T(1)), pold, dt, &ee,
+                                         Dual<T>(T(1) / taumax));
+      lo = ee * ln;
+      lvk = xn.d * ln;
+      // d x' / d taumax through the rate scale 1 / taumax
+      Dual<T> xt = gate_step<Dual<T>, T>(G_PKM_P, Dual<T>(v), pold, dt, nullptr,
+                                         Dual<T>(T(1) / taumax, -T(1) / (taumax * taumax)));
+      lam[e.s[0]] = lo;
+      lv += lvk;
+      G.add(1, xt.d * ln);
+      break;
+    }
     default: {
       GateLayout gl = gate_layout(e.type);
       T lo;
@@ -405,9 +521,19 @@ __device__ __forceinline__ void channel_update_logged(const ChanEntry& e, T* x, 
     }
     case CH_CAPUMP:
     case CH_CANERNST:
+    case CH_PKM:  // (its reverse pass recomputes the derivatives from the restored state)
       L.push(e.s[0], x[e.s[0]], T(0), T(0));
       channel_update<T>(e, x, P, v, dt);
       break;
+    case CH_PNA:
+    case CH_PK:
+    case CH_PCAT: {  // gates of the shifted voltage; the log holds d x' / d u
+      const T u = e.type == CH_PCAT ? v + P(1) : v - P(2);
+      GateLayout gl = gate_layout(e.type);
+      gate_logged<T, N>(gl.g0, u, x, e.s[0], dt, L);
+      if (gl.g1 >= 0) gate_logged<T, N>(gl.g1, u, x, e.s[1], dt, L);
+      break;
+    }
     default: {
       GateLayout gl = gate_layout(e.type);
       gate_logged<T, N>(gl.g0, v, x, e.s[0], dt, L);
@@ -436,10 +562,33 @@ __device__ __forceinline__ void channel_update_vjp_logged(const ChanEntry& e, T*
     }
     case CH_CAPUMP:
     case CH_CANERNST:
+    case CH_PKM:
       --L.n;
       x[L.slot[L.n]] = L.old[L.n];
       channel_update_vjp<T>(e, x, lam, P, G, v, dt, lv);
       break;
+    case CH_PNA:
+    case CH_PK:
+    case CH_PCAT: {
+      // as the default gates, with the shifted voltage's parameter: d/d vt = -d/du
+      // (Na, K), d/d vx = d/du (CaT)
+      const int ng = gate_layout(e.type).g1 >= 0 ? 2 : 1;
+      T lu = T(0);
+      for (int k = 0; k < ng; ++k) {
+        --L.n;
+        const short s = L.slot[L.n];
+        x[s] = L.old[L.n];
+        const T ln = lam[s];
+        lam[s] = L.dx[L.n] * ln;
+        lu += L.dy[L.n] * ln;
+      }
+      lv += lu;
+      if (e.type == CH_PCAT)
+        G.add(1, lu);
+      else
+        G.add(2, -lu);
+      break;
+    }
     default: {
       // Gates: pop in reverse order of the pushes.
       int ng = e.type == CH_HH ? 3 : (gate_layout(e.type).g1 >= 0 ? 2 : 1);

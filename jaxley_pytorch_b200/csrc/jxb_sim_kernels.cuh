@@ -435,7 +435,7 @@ __device__ __forceinline__ void node_channels(const SimSmem<T>& sm, int j, T* x,
     }
   }
   if (mode == 2) {
-    for (int q = e0; q < e1; ++q) channel_steady<T>(sm.ents[q], x, v);
+    for (int q = e0; q < e1; ++q) channel_steady<T>(sm.ents[q], x, Prm<T>{pn + sm.ents[q].p[0]}, v);
     return;
   }
   if (mode == 0) {

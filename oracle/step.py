@@ -186,6 +186,42 @@ _INF_TAU_2 = {  # (m gate, h gate, m exponent, h exponent) of x_inf/tau channels
 _INF_TAU_1 = {"SKv3_1": _skv31_m, "M": _mm_m, "H": _h_m}
 
 
+# Pospischil channels (channels/pospischil.py). efun(x) = x / (exp(x) - 1).
+def _efun(x):
+    return x_over_expm1(x)
+
+
+def _pna_m(v, vt):  # pospischil.py:124-131
+    return 0.32 * _efun(-0.25 * (v - vt - 13.0)) / 0.25, 0.28 * _efun(0.2 * (v - vt - 40.0)) / 0.2
+
+
+def _pna_h(v, vt):  # pospischil.py:133-140
+    return 0.128 * save_exp(-(v - vt - 17.0) / 18.0), 4.0 / (save_exp(-(v - vt - 40.0) / 5.0) + 1.0)
+
+
+def _pk_n(v, vt):  # pospischil.py:186-193
+    return 0.032 * _efun(-0.2 * (v - vt - 15.0)) / 0.2, 0.5 * save_exp(-(v - vt - 10.0) / 40.0)
+
+
+def _pkm_p(v, taumax):  # pospischil.py:242-249: (p_inf, tau_p)
+    vp = v + 35.0
+    return 1.0 / (1.0 + save_exp(-0.1 * vp)), taumax / (3.3 * save_exp(0.05 * vp) + save_exp(-0.05 * vp))
+
+
+def _pcal_q(v):  # pospischil.py:301-308
+    return 0.055 * _efun((-v - 27.0) / 3.8) * 3.8, 0.94 * save_exp((-v - 75.0) / 17.0)
+
+
+def _pcal_r(v):  # pospischil.py:310-317
+    return 0.000457 * save_exp((-v - 13.0) / 50), 0.0065 / (save_exp((-v - 15.0) / 28.0) + 1)
+
+
+def _pcat_u(v, vx):  # pospischil.py:366-375: (u_inf, tau_u)
+    u_inf = 1.0 / (1.0 + save_exp((v + vx + 81.0) / 4))
+    tau = (30.8 + (211.4 + save_exp((v + vx + 113.2) / 5.0))) / (3.7 * (1 + save_exp((v + vx + 84.0) / 3.2)))
+    return u_inf, tau
+
+
 def channel_update(ch, st: Dict[str, np.ndarray], dt, v, prm: Dict[str, np.ndarray]):
     """`Channel.update_states` of every supported channel. `st` maps the reference
     state names (and current names) to arrays at the channel's nodes."""
@@ -227,6 +263,20 @@ def channel_update(ch, st: Dict[str, np.ndarray], dt, v, prm: Dict[str, np.ndarr
         Cai, Cao = st[S[1]], st[S[2]]
         C = R * T / (2 * F) * 1000
         return {S[0]: C * np.log(Cao / Cai), S[1]: Cai, S[2]: Cao}
+    P = ch.params
+    if t == "Na":  # pospischil.py:91-104
+        vt = prm[P[2]]
+        return {S[0]: solve_gate_exponential(st[S[0]], dt, *_pna_m(v, vt)),
+                S[1]: solve_gate_exponential(st[S[1]], dt, *_pna_h(v, vt))}
+    if t == "K":  # pospischil.py:158-169
+        return {S[0]: solve_gate_exponential(st[S[0]], dt, *_pk_n(v, prm[P[2]]))}
+    if t == "Km":  # pospischil.py:212-225
+        return {S[0]: solve_inf_gate_exponential(st[S[0]], dt, *_pkm_p(v, prm[P[1]]))}
+    if t == "CaL":  # pospischil.py:271-284
+        return {S[0]: solve_gate_exponential(st[S[0]], dt, *_pcal_q(v)),
+                S[1]: solve_gate_exponential(st[S[1]], dt, *_pcal_r(v))}
+    if t == "CaT":  # pospischil.py:334-347
+        return {S[0]: solve_inf_gate_exponential(st[S[0]], dt, *_pcat_u(v, prm[P[1]]))}
     raise NotImplementedError(t)
 
 
@@ -254,6 +304,17 @@ def channel_current(ch, st, v, prm):
         return prm[P[0]] * (st[S[0]] ** 2) * st[S[1]] * (v - st[S[2]])
     if t in ("CaPump", "CaNernstReversal"):  # l5pc.py:863-865, 904-906
         return np.zeros_like(v)
+    if t == "Na":  # pospischil.py:106-115
+        return prm[P[0]] * (st[S[0]] ** 3) * st[S[1]] * (v - prm[P[1]])
+    if t == "K":  # pospischil.py:171-178
+        return prm[P[0]] * (st[S[0]] ** 4) * (v - prm[P[1]])
+    if t == "Km":  # pospischil.py:227-230
+        return prm[P[0]] * st[S[0]] * (v - prm[P[2]])
+    if t == "CaL":  # pospischil.py:286-292
+        return prm[P[0]] * (st[S[0]] ** 2) * st[S[1]] * (v - prm[P[1]])
+    if t == "CaT":  # pospischil.py:349-357
+        s_inf = 1.0 / (1.0 + save_exp(-(v + prm[P[1]] + 57.0) / 6.2))
+        return prm[P[0]] * (s_inf**2) * st[S[0]] * (v - prm[P[2]])
     raise NotImplementedError(t)
 
 
@@ -277,6 +338,15 @@ def channel_init(ch, v, prm):
         am, bm = _cahva_m(v)
         ah, bh = _cahva_h(v)
         return {S[0]: am / (am + bm), S[1]: ah / (ah + bh)}
+    P = ch.params
+    # Pospischil init_state (pospischil.py:117-125, 180-184, 232-237, 294-303, 360-364):
+    # alpha / (alpha + beta) of each gate's pair, also for the (x_inf, tau) pairs of Km
+    # and CaT.
+    pairs = {"Na": lambda: [_pna_m(v, prm[P[2]]), _pna_h(v, prm[P[2]])],
+             "K": lambda: [_pk_n(v, prm[P[2]])], "Km": lambda: [_pkm_p(v, prm[P[1]])],
+             "CaL": lambda: [_pcal_q(v), _pcal_r(v)], "CaT": lambda: [_pcat_u(v, prm[P[1]])]}
+    if t in pairs:
+        return {s_: a / (a + b) for s_, (a, b) in zip(S, pairs[t]())}
     return {}
 
 

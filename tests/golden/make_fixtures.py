@@ -326,6 +326,54 @@ def clamp_cell():
     save_with_grads("hh_clamp_7x3", cell, cell.get_parameters(), seed=41, delta_t=0.025)
 
 
+def pospischil_cell():
+    """A branched cell with the Pospischil channels (channels/pospischil.py: Na, K, Km,
+    CaL, CaT, Leak), a regular-spiking and a fast-spiking region, two stimuli, and
+    the reference's gradients with respect to conductances, the shared threshold vt,
+    Km's taumax and CaT's vx."""
+    from jaxley_pytorch.channels.pospischil import CaL, CaT, K, Km, Na
+
+    cell = jx.Cell([jx.Branch(jx.Compartment(), 3)] * 7, parents=binary_parents(7))
+    rng = np.random.default_rng(17)
+    for b in range(7):
+        cell.branch(b).set("radius", float(rng.uniform(0.5, 2.0)))
+        cell.branch(b).set("length", float(rng.uniform(5.0, 40.0)))
+    cell.insert(Na())
+    cell.insert(K())
+    cell.insert(Leak())
+    rs = cell.branch([0, 1, 3, 4])
+    rs.insert(Km())
+    cell.branch([0, 2, 5]).insert(CaL())
+    cell.branch([0, 2, 6]).insert(CaT())
+    cell.set("Na_gNa", 5e-2)
+    cell.set("vt", -60.0)
+    cell.set("Leak_eLeak", -70.0)
+    cell.branch([0, 1, 3, 4]).set("K_gK", 5e-3)
+    cell.branch([2, 5, 6]).set("K_gK", 1e-2)
+    cell.branch([0, 1, 3, 4]).set("Km_gKm", 7e-5)
+    cell.branch([0, 1, 3, 4]).set("Km_taumax", 1000.0)
+    cell.branch([0, 2, 5]).set("CaL_gCaL", 2e-4)
+    cell.branch([0, 2, 6]).set("CaT_gCaT", 4e-4)
+    cell.set("v", -70.0)
+    cell.init_states()
+    cell.branch(0).comp(0).record(verbose=False)
+    cell.branch(4).comp(2).record(verbose=False)
+    cell.branch(6).comp(1).record(verbose=False)
+    cell.branch(0).comp(0).record("Na_m", verbose=False)
+    cell.branch(2).comp(1).record("i_Ca", verbose=False)
+    cell.branch(6).comp(0).record("CaT_u", verbose=False)
+    cell.branch(0).comp(0).stimulate(jx.step_current(1.0, 4.0, 0.15, 0.025, 12.0), verbose=False)
+    cell.branch(5).comp(2).stimulate(jx.step_current(3.0, 3.0, 0.1, 0.025, 12.0), verbose=False)
+    cell.make_trainable("Na_gNa", verbose=False)
+    cell.make_trainable("vt", verbose=False)
+    cell.branch([0, 1, 3, 4]).make_trainable("Km_taumax", verbose=False)
+    cell.branch("all").make_trainable("K_gK", verbose=False)
+    cell.make_trainable("CaT_vx", verbose=False)
+    cell.make_trainable("CaT_gCaT", verbose=False)
+    cell.make_trainable("CaL_gCaL", verbose=False)
+    save_with_grads("pospischil_7x3", cell, cell.get_parameters(), seed=81, delta_t=0.025)
+
+
 def reference_l5pc_cell(parents, ncomp, radius, lengths):
     from jaxley_pytorch_b200 import synth
 
@@ -470,9 +518,11 @@ def c4_sample():
 
 if __name__ == "__main__":
     which = [w for w in sys.argv[1:] if w != "synth"] if sys.argv[1:] else [
-        "golden", "small", "tree", "l5pc", "forest", "synapse", "clamp", "c2", "c3", "c4", "synth"]
+        "golden", "small", "tree", "l5pc", "forest", "synapse", "clamp", "pospischil", "c2", "c3", "c4",
+        "synth"]
     fns = {"golden": golden_cases, "small": config_small, "tree": hh_tree, "l5pc": l5pc_cell,
-           "forest": hh_forest, "synapse": synapse_net, "clamp": clamp_cell, "c2": c2_sample,
+           "forest": hh_forest, "synapse": synapse_net, "clamp": clamp_cell, "pospischil": pospischil_cell,
+           "c2": c2_sample,
            "c3": c3_sample, "c4": c4_sample}
     for w in which:
         if w in fns:
