@@ -72,7 +72,7 @@ def parse():
                     help="skip the uneven-batch persistent vs per-step measurement")
     ap.add_argument("--uneven-cells", type=int, default=4096)
     ap.add_argument("--uneven-tsteps", type=int, default=2000)
-    ap.add_argument("--uneven-plain-tsteps", type=int, default=100)
+    ap.add_argument("--uneven-plain-tsteps", type=int, default=2000)
     ap.add_argument("--no-serving", action="store_true", help="skip the serving-stream measurement")
     ap.add_argument("--no-network", action="store_true", help="skip the network training-step measurement")
     ap.add_argument("--no-recompute", action="store_true",
@@ -364,7 +364,8 @@ def run_uneven(args, device):
     forward + adjoint of an MSE loss. The persistent form (autotuned block size,
     threads and checkpoint interval; the whole iteration replayed as one CUDA graph)
     against the plain per-step form (one launch per step and per adjoint step,
-    checkpoint every step) on the same cells, the latter on a 100-step horizon."""
+    checkpoint every step) on the same cells and horizon; the time of every size group
+    of the persistent form (shared-memory classes and global work areas)."""
     import torch
 
     from jaxley_pytorch_b200 import synth
@@ -423,6 +424,28 @@ def run_uneven(args, device):
     ms_plain = timed(plain_step, 2)
     rate = n_comp * T / (ms / 1e3)
     rate_plain = n_comp * Tp / (ms_plain / 1e3)
+    del plain
+    torch.cuda.empty_cache()
+    # Per size group: one eager iteration of the persistent form with an event pair
+    # around every group launch (the groups run concurrently on their own streams).
+    sim.model.group_timing = True
+    sim.model.group_events = []
+    ps = ps0.clone().requires_grad_(True)
+    torch.autograd.grad(loss_of(target)(sim.run(pscale=ps)), ps)
+    torch.cuda.synchronize()
+    sim.model.group_timing = False
+    per_group = {}
+    names = {-1: "global work areas", 0: "up to 1/4 of the shared memory", 1: "up to 1/2", 2: "up to all"}
+    for kind, key, n_items, a, b in sim.model.group_events:
+        ent = per_group.setdefault(f"{kind}/{names.get(key[1], key[1])}",
+                                   {"items": n_items, "launches": 0, "ms": 0.0})
+        ent["launches"] += 1
+        ent["ms"] += a.elapsed_time(b)
+    for g in sim.model.groups["forward"]:
+        ent = per_group.get(f"forward/{names.get(g['key'][1], g['key'][1])}")
+        if ent is not None:
+            items = g["items"].cpu().numpy()
+            ent["nodes_largest_block"] = int(sim.low.blocks[items[:, 0], 1].max())
     return {
         "workload": f"uneven_{args.uneven_cells}cells_t{T}_fwd_adjoint", "cells": args.uneven_cells,
         "compartments": n_comp, "nodes": prob.n_nodes, "time_steps": T,
@@ -435,6 +458,7 @@ def run_uneven(args, device):
         "per_step": {"value": rate_plain, "unit": UNIT, "ms_per_iteration": ms_plain, "time_steps": Tp,
                      "checkpoint": 1},
         "persistent_over_per_step": rate / rate_plain,
+        "per_group": per_group,
         "tuning": table,
     }
 
@@ -442,41 +466,54 @@ def run_uneven(args, device):
 def run_serving(args, device):
     """Serving stream: seeded single-cell requests from the uneven-batch generator
     (8-3000 compartments), horizons U[5, 200] ms, 30 % with gradients, float32.
-    For each scheduling policy (equal progress: every request advances by 1/16 of
-    its work per tick; fixed: 200 steps per tick) the capacity is measured on a
-    closed batch (all requests waiting), then Poisson arrivals at 80 % of that
-    capacity give p50/p99 latency and compartment-steps/s. The plain per-request
-    path (one request at a time) runs on the same arrivals, bounded to the same wall
-    time."""
-    from jaxley_pytorch_b200.serve import Request, Server, make_stream, serve_plain
+    For each scheduling policy (time slice: every request advances per tick by the
+    steps that take about 2 ms of GPU time; equal progress: by 1/16 of its work;
+    fixed: by 200 steps) the capacity is measured on a closed batch (all requests
+    waiting), then Poisson arrivals at 80 % of that capacity give p50/p99 latency,
+    compartment-steps/s and every request's slowdown (latency over its latency when
+    served alone, measured on the plain per-request path). The plain per-request path
+    itself (one request at a time, same kernels) on the same arrivals is the FIFO
+    queue of those alone latencies."""
+    from jaxley_pytorch_b200.serve import Request, Server, fifo_latencies, make_stream, serve_plain
 
     def copy(reqs, zero=False):
         return [Request(problem=r.problem, n_steps=r.n_steps, grad=r.grad, arrival=0.0 if zero else r.arrival,
                         rid=r.rid) for r in reqs]
 
-    policies = {"equal_progress_16": dict(progress_ticks=16, chunk=200, checkpoint=200),
+    policies = {"time_slice_2ms": dict(slice_ms=2.0, checkpoint=200, min_chunk=20),
+                "equal_progress_16": dict(progress_ticks=16, chunk=200, checkpoint=200),
                 "fixed_chunk_200": dict(progress_ticks=0, chunk=200, checkpoint=200)}
     Server(device=device, threads=256, **policies["fixed_chunk_200"]).run(make_stream(8, seed=99, rate=1e6))
-    closed = make_stream(args.serve_capacity_requests, seed=7, rate=1e9)
+    closed = make_stream(args.serve_requests // 3 * 2, seed=7, rate=1e9)
+    base = make_stream(args.serve_requests, seed=8, rate=1.0)  # problems and horizons (rate-free)
+    # alone latencies: every request on its own, one after the other
+    alone = copy(base, zero=True)
+    pl = serve_plain(alone, device=device, threads=256, checkpoint=200)
+    service = {r.rid: r.service for r in alone}
     out = {"workload": "serving_stream_8_3000comp_5_200ms_30pct_grad", "unit": UNIT, "policies": {}}
-    stream = None
     for name, pol in policies.items():
         cap = Server(device=device, threads=256, **pol).run(copy(closed, zero=True))
         capacity = cap["requests"] / cap["makespan_s"]
         stream = make_stream(args.serve_requests, seed=8, rate=0.8 * capacity)
+        for r in stream:
+            r.service = service[r.rid]
         st = Server(device=device, threads=256, **pol).run(stream)
+        plain_lat = fifo_latencies([r.arrival for r in stream], [service[r.rid] for r in stream])
         out["policies"][name] = {
             "capacity_rps": capacity, "closed_batch_throughput": cap["throughput"],
             "arrival_rate_rps": 0.8 * capacity, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
-            "p99_over_p50": st["p99_over_p50"], "throughput": st["throughput"], "requests": st["requests"],
-            "ticks": st["ticks"], "launches": st["launches"], "makespan_s": st["makespan_s"]}
-    first = out["policies"]["equal_progress_16"]
-    out.update({k: first[k] for k in ("p50_ms", "p99_ms", "p99_over_p50", "throughput", "capacity_rps",
-                                      "arrival_rate_rps")})
-    stream = make_stream(args.serve_requests, seed=8, rate=first["arrival_rate_rps"])
-    pl = serve_plain(copy(stream), device=device, threads=256, checkpoint=200, time_limit=first["makespan_s"])
-    out["plain_per_request"] = {"p50_ms": pl["p50_ms"], "p99_ms": pl["p99_ms"], "throughput": pl["throughput"],
-                                "requests_done": pl["requests"], "of": len(stream), "wall_s": pl["makespan_s"]}
+            "p99_over_p50": st["p99_over_p50"], "slowdown_p50": st.get("slowdown_p50"),
+            "slowdown_p99": st.get("slowdown_p99"), "throughput": st["throughput"],
+            "requests": st["requests"], "ticks": st["ticks"], "launches": st["launches"],
+            "makespan_s": st["makespan_s"],
+            "plain_per_request_same_arrivals": {"p50_ms": float(np.percentile(plain_lat, 50) * 1e3),
+                                                "p99_ms": float(np.percentile(plain_lat, 99) * 1e3)}}
+    first = out["policies"]["time_slice_2ms"]
+    out.update({k: first[k] for k in ("p50_ms", "p99_ms", "p99_over_p50", "slowdown_p50", "slowdown_p99",
+                                      "throughput", "capacity_rps", "arrival_rate_rps")})
+    out["policy"] = "time_slice_2ms"
+    out["plain_per_request"] = {"throughput": pl["throughput"], "alone_p50_ms": pl["p50_ms"],
+                                "requests": pl["requests"], "wall_s": pl["makespan_s"]}
     out["throughput_over_plain"] = first["throughput"] / pl["throughput"] if pl["throughput"] else None
     return out
 

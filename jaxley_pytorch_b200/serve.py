@@ -30,6 +30,18 @@ from .problem import Problem
 from .sim import DeviceModel, Simulation
 
 
+def step_cost_us(low: Lowered, threads: int = 256) -> float:
+    """Estimated microseconds of one forward step of a lowered problem's largest work
+    item on an SM of its own: a fixed part, the chain levels of the tree solve (one
+    pass down and one up each) and the per-node channel work spread over the CTA's
+    threads (coefficients from per-phase timings of the fused kernel on the 300 x 4
+    L5PC tree: solve 0.55 us per level and pass, channels 0.9 us per node a thread)."""
+    blocks = np.asarray(low.blocks)
+    levels = int(blocks[:, 7].max()) if len(blocks) else 1
+    nodes = int(blocks[:, 1].max()) if len(blocks) else 1
+    return 2.0 + 1.1 * levels + 0.9 * -(-nodes // max(1, threads))
+
+
 @dataclass
 class Request:
     """A simulation request. `grad`: also return d(sum of recordings)/d(parameter
@@ -45,10 +57,16 @@ class Request:
     gradient: Optional[np.ndarray] = None
     admitted: float = float("nan")
     finished: float = float("nan")
+    service: float = float("nan")  # seconds of the request served alone (per-request path)
 
     @property
     def latency(self) -> float:
         return self.finished - self.arrival
+
+    @property
+    def slowdown(self) -> float:
+        """Latency over the request's own latency when served alone."""
+        return self.latency / self.service
 
 
 def request_bytes(low: Lowered, n_steps: int, grad: bool, checkpoint: int, itemsize: int = 4) -> int:
@@ -87,14 +105,20 @@ class _Active:
         self.group_f = self.group_b = group
         m, low = self.model, self.low
         self.T = int(req.n_steps)
-        if server.progress_ticks:
+        if server.slice_us:
+            # time slice: every request gets about the same GPU time per tick, so a
+            # request of fast steps advances by more of them and short requests are
+            # not held to the pace of long ones
+            self.chunk = int(min(self.T, max(server.min_chunk,
+                                             round(server.slice_us / step_cost_us(low, server.threads)))))
+        elif server.progress_ticks:
             # equal progress: every request needs about `progress_ticks` ticks (a gradient
             # request half of them forward, half adjoint), whatever its horizon
             n = max(1, server.progress_ticks // (2 if req.grad else 1))
             self.chunk = max(server.min_chunk, -(-self.T // n))
         else:
             self.chunk = server.chunk
-        self.K = min(self.chunk if server.progress_ticks else server.checkpoint, self.T)
+        self.K = min(self.chunk if (server.progress_ticks or server.slice_us) else server.checkpoint, self.T)
         self.nseg = (self.T + self.K - 1) // self.K
         self.state = m.initial_state()
         self.rec = torch.zeros((self.T + 1, low.batch, low.n_rec), dtype=dtype, device=dev)
@@ -192,7 +216,7 @@ class Server:
     def __init__(self, device="cuda", dtype=torch.float32, hbm_budget: Optional[int] = None,
                  chunk: int = 200, threads: int = 256, checkpoint: int = 100,
                  max_block_nodes: int = 4096, max_active: int = 4096, progress_ticks: int = 0,
-                 min_chunk: int = 20):
+                 min_chunk: int = 20, slice_ms: float = 0.0):
         self.device = torch.device(device)
         self.dtype = dtype
         self.code = _lib.F32 if dtype == torch.float32 else _lib.F64
@@ -201,7 +225,11 @@ class Server:
             hbm_budget = int(free * 0.5)
         self.hbm_budget = int(hbm_budget)
         self.chunk = int(chunk)
-        self.progress_ticks = int(progress_ticks)  # 0: fixed chunk of `chunk` steps per tick
+        # Scheduling policy: with `slice_ms`, every request advances per tick by the
+        # steps that take about `slice_ms` of GPU time (step_cost_us); else with
+        # `progress_ticks`, by 1 / progress_ticks of its horizon; else by `chunk` steps.
+        self.slice_us = float(slice_ms) * 1e3
+        self.progress_ticks = int(progress_ticks)
         self.min_chunk = int(min_chunk)
         self.threads = int(threads)
         self.checkpoint = int(checkpoint)
@@ -367,8 +395,22 @@ def summarize(done: Sequence[Request], makespan: float, comp_steps: int, **extra
            "mean_ms": float(lat.mean() * 1e3), "compartment_steps": int(comp_steps),
            "throughput": comp_steps / makespan if makespan > 0 else 0.0}
     out["p99_over_p50"] = out["p99_ms"] / out["p50_ms"] if out["p50_ms"] > 0 else float("nan")
+    slow = np.asarray([r.slowdown for r in done if np.isfinite(r.service) and r.service > 0])
+    if len(slow):
+        out["slowdown_p50"] = float(np.percentile(slow, 50))
+        out["slowdown_p99"] = float(np.percentile(slow, 99))
     out.update(extra)
     return out
+
+
+def fifo_latencies(arrivals: Sequence[float], service: Sequence[float]) -> np.ndarray:
+    """Latencies of one server that takes requests one at a time in arrival order
+    (the per-request path), from their arrival and service times."""
+    done, out = 0.0, []
+    for a, s in sorted(zip(arrivals, service)):
+        done = max(done, a) + s
+        out.append(done - a)
+    return np.asarray(out)
 
 
 def serve_plain(requests: Sequence[Request], device="cuda", dtype=torch.float32, threads: int = 256,
@@ -397,6 +439,7 @@ def serve_plain(requests: Sequence[Request], device="cuda", dtype=torch.float32,
                 rec = sim.run(n_steps=r.n_steps)
         r.recordings = rec.detach().cpu().numpy()
         r.finished = time.perf_counter() - t0
+        r.service = r.finished - max(now, r.arrival)
         comp_steps += r.n_steps * len(r.problem.comp_inds) * r.problem.batch
         done.append(r)
     return summarize(done, time.perf_counter() - t0, comp_steps)

@@ -138,6 +138,10 @@ class DeviceModel:
         self.launches = 0  # kernel launches issued through this model
         self.timed_kind: Optional[str] = None  # "forward"/"backward": record events
         self.events: List = []
+        # With `group_timing`, every group launch records (kind, group key, items,
+        # start, end) events on the stream it runs on, in `group_events`.
+        self.group_timing = False
+        self.group_events: List = []
         self._sides: List[torch.cuda.Stream] = []
         self._scratch: Dict[str, torch.Tensor] = {}
         self.smem_limit = smem_limit if smem_limit is not None else self._device_smem_limit()
@@ -351,8 +355,16 @@ class DeviceModel:
                 side.wait_stream(st)
         for gi, g in enumerate(groups):
             a = self.group_args(args, kind, g)
-            s = self._sides[gi].cuda_stream if (fork and gi < len(groups) - 1) else main
+            side = self._sides[gi] if (fork and gi < len(groups) - 1) else None
+            s = side.cuda_stream if side is not None else main
+            ev = None
+            if self.group_timing and stream is None:
+                ev = (torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True))
+                ev[0].record(side if side is not None else st)
             _lib.check(fn(C.byref(a), C.c_void_p(s)), f"jxb_sim_{kind}")
+            if ev is not None:
+                ev[1].record(side if side is not None else st)
+                self.group_events.append((kind, g["key"], g["n_items"], ev[0], ev[1]))
             self.launches += 1
         if fork:
             for side in self._sides[:len(groups) - 1]:

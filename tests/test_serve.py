@@ -52,3 +52,24 @@ def test_summary_percentiles():
     s = summarize(reqs, 0.1, 1000)
     assert abs(s["p50_ms"] - 50.5) < 1e-6 and abs(s["p99_ms"] - 99.01) < 1e-6
     assert s["throughput"] == 1000 / 0.1 and s["requests"] == 100
+
+
+def test_fifo_latencies_and_slowdown():
+    from jaxley_pytorch_b200.serve import fifo_latencies
+
+    # arrivals 0, 1, 1.5; service 2, 1, 1: done at 2, 3, 4
+    lat = fifo_latencies([0.0, 1.0, 1.5], [2.0, 1.0, 1.0])
+    assert np.allclose(lat, [2.0, 2.0, 2.5])
+    r = Request(problem=None, n_steps=1, arrival=1.0)
+    r.finished, r.service = 4.0, 1.5
+    assert r.slowdown == 2.0
+    s = summarize([r], 1.0, 10)
+    assert s["slowdown_p50"] == 2.0
+
+
+def test_step_cost_grows_with_levels_and_nodes():
+    from jaxley_pytorch_b200.serve import step_cost_us
+
+    small = lower(synth.config_uneven(n_cells=1, seed=1, n_steps=10, min_comp=8, max_comp=9), keep_currents=False)
+    big = lower(synth.config_l5pc_tree(batch=1, n_steps=10), keep_currents=False)
+    assert 2.0 < step_cost_us(small) < step_cost_us(big) < 60.0

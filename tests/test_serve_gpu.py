@@ -26,12 +26,13 @@ def _check_same(a, b, rtol=1e-12):
         assert np.abs(a.gradient - b.gradient).max() <= rtol * s
 
 
-@pytest.mark.parametrize("force_global", [False, True])
-def test_served_results_equal_the_per_request_path(cuda_device, force_global):
+@pytest.mark.parametrize("force_global,policy", [(False, "fixed"), (True, "fixed"), (False, "slice")])
+def test_served_results_equal_the_per_request_path(cuda_device, force_global, policy):
     reqs = make_stream(10, seed=3, rate=2000.0, grad_fraction=0.4, min_comp=8, max_comp=600,
                        t_range=(2.0, 12.0))
     assert any(r.grad for r in reqs) and not all(r.grad for r in reqs)
-    server = Server(device=cuda_device, chunk=64, threads=256, checkpoint=50)
+    kw = dict(chunk=64, checkpoint=50) if policy == "fixed" else dict(slice_ms=0.3, min_chunk=8)
+    server = Server(device=cuda_device, threads=256, **kw)
     if force_global:
         server.smem_limit = 1  # every request's items run with global work areas
     stats = server.run(_copy(reqs))
