@@ -860,20 +860,29 @@ def main():
         torch.distributed.init_process_group("nccl", timeout=timedelta(seconds=300),
                                              device_id=torch.device("cuda", local))
     device = torch.device("cuda", local)
-    out = run_ours(args, rank, world, device)
+    t_start = time.perf_counter()
+
+    def section(name, fn):
+        t0 = time.perf_counter()
+        res = fn()
+        print(f"[bench] {name}: {time.perf_counter() - t0:.1f} s (total {time.perf_counter() - t_start:.1f} s)",
+              file=sys.stderr, flush=True)
+        return res
+
+    out = section("main iteration", lambda: run_ours(args, rank, world, device))
     if world == 1 and not args.no_uneven:
-        out["uneven"] = run_uneven(args, device)
+        out["uneven"] = section("uneven batch", lambda: run_uneven(args, device))
     if world == 1 and not args.no_serving:
-        out["serving"] = run_serving(args, device)
+        out["serving"] = section("serving", lambda: run_serving(args, device))
     if world == 1 and not args.no_network:
-        out["network"] = run_network(args, device)
+        out["network"] = section("network", lambda: run_network(args, device))
     if world == 1 and not args.no_lm:
-        out["lm_network"] = [run_lm(args, device, n) for n in (1024, 2048)]
+        out["lm_network"] = section("lm networks", lambda: [run_lm(args, device, n) for n in (1024, 2048)])
     if world == 1 and not args.no_fp32_error:
-        out["fp32_error"] = fp32_errors(device)
+        out["fp32_error"] = section("fp32 errors", lambda: fp32_errors(device))
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
-            ref = reference_baseline(args.cpu_batch, args.cpu_tsteps)
+            ref = section("cpu baseline", lambda: reference_baseline(args.cpu_batch, args.cpu_tsteps))
             if ref is not None:
                 out["cpu_baseline"] = ref
             else:

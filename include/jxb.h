@@ -251,9 +251,14 @@ typedef struct JxbSimArgs_ {
    * not finite ORs JXB_NONFINITE into it. The host reads and clears it between
    * launches; the kernels never stop or fault on a non-finite value. */
   int32_t* status;
+  /* Step scheme of the voltage (modules/base.py:3327-3365): JXB_SCHEME_BWD_EULER, or
+   * JXB_SCHEME_CN (Crank-Nicolson: the implicit system of half a step, then
+   * v' = 2 v_half - v; the channels step by the whole dt in both). */
+  int32_t scheme, pad7;
 } JxbSimArgs;
 
 enum { JXB_NONFINITE = 1 };
+enum { JXB_SCHEME_BWD_EULER = 0, JXB_SCHEME_CN = 1 };
 
 int jxb_sim_forward(const JxbSimArgs* args, void* stream);
 int jxb_sim_backward(const JxbSimArgs* args, void* stream);

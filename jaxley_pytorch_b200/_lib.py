@@ -16,6 +16,7 @@ LIB_PATH = os.path.join(_HERE, "_build", "libjxb.so")
 JXB_OK = 0
 JXB_NONFINITE = 1  # bit of JxbSimArgs.status: a launch produced a value that is not finite
 F32, F64 = 0, 1
+SCHEME_BWD_EULER, SCHEME_CN = 0, 1  # JxbSimArgs.scheme
 
 _p = C.c_void_p
 _i32p = C.c_void_p
@@ -78,7 +79,7 @@ class JxbSimArgs(C.Structure):
         ("syn_ptr", _p), ("syn_off", _p), ("syn_rs", _p), ("g_syn_lin", _p), ("g_syn_const", _p),
         ("clamp_ptr", _p), ("clamp_slot", _p), ("clamp_col", _p), ("clamp", _p),
         ("n_clamp", C.c_int32), ("clamp_steps", C.c_int32), ("clamp_rows", C.c_int32), ("pad6", C.c_int32),
-        ("status", _p),
+        ("status", _p), ("scheme", C.c_int32), ("pad7", C.c_int32),
     ]
 
 

@@ -53,6 +53,14 @@ struct SimSmem {
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
 
+// Step of the implicit voltage system: dt for backward Euler, dt / 2 for
+// Crank-Nicolson (modules/base.py:3327-3330), whose voltage then moves by twice the
+// increment (v' = 2 v_half - v, :3362-3365); the channels always step by dt.
+template <typename T>
+__host__ __device__ __forceinline__ T solve_dt(const JxbSimArgs& a, T dt) {
+  return a.scheme == JXB_SCHEME_CN ? dt * T(0.5) : dt;
+}
+
 template <typename T>
 __host__ __device__ inline size_t sim_smem_layout(const JxbSimArgs& a, bool backward, SimSmem<T>* o,
                                                   char* base) {
@@ -113,6 +121,7 @@ __device__ __forceinline__ void stage_item(const JxbSimArgs& a, const JxbBlock& 
   const T* gu = (const T*)a.a_up;
   const T* gs = (const T*)a.gsum;
   const T* cmv = (const T*)a.cm;
+  dt = solve_dt<T>(a, dt);  // the voltage system's step (half of it for Crank-Nicolson)
   for (int j = tid; j < nn; j += NT) {
     const int i = node0 + j;
     const int cls = a.node_class[i];
@@ -313,7 +322,7 @@ __device__ __forceinline__ void chain_eliminate(const SimSmem<T>& sm, int c, T* 
 template <typename T>
 __device__ __forceinline__ void chain_backsub(const SimSmem<T>& sm, int c, const T* __restrict__ Dr,
                                               T* __restrict__ Sr, const T* __restrict__ al,
-                                              T* __restrict__ Vr) {
+                                              T* __restrict__ Vr, T vscale = T(1)) {
   const int4 dsc = sm.cdesc[c];
   const int top = dsc.x;
   const int bot = dsc.y & ~kManyKids;
@@ -341,7 +350,7 @@ __device__ __forceinline__ void chain_backsub(const SimSmem<T>& sm, int c, const
   for (int q = 0; q < kB; ++q)
     if (q < n0) {
       Sr[top + q] = sb[q];
-      if (Vr) Vr[top + q] += sb[q];
+      if (Vr) Vr[top + q] += vscale * sb[q];
     }
   for (int l0 = top + kB; l0 <= bot; l0 += kSeg) {
     const int n = min(kSeg, bot - l0 + 1);
@@ -364,7 +373,7 @@ __device__ __forceinline__ void chain_backsub(const SimSmem<T>& sm, int c, const
     for (int q = 0; q < kSeg; ++q)
       if (q < n) {
         Sr[l0 + q] = ss[q];
-        if (Vr) Vr[l0 + q] += ss[q];
+        if (Vr) Vr[l0 + q] += vscale * ss[q];
       }
   }
 }
@@ -374,7 +383,7 @@ __device__ __forceinline__ void chain_backsub(const SimSmem<T>& sm, int c, const
 // solution (and `V`, when given, has it added).
 template <typename T>
 __device__ __forceinline__ void block_solve(const JxbBlock& blk, const SimSmem<T>& sm, int rows,
-                                            const T* al, const T* au, T* V = nullptr) {
+                                            const T* al, const T* au, T* V = nullptr, T vscale = T(1)) {
   const int tid = threadIdx.x, NT = blockDim.x;
   const int nn = blk.n_nodes;
   const int nlev = blk.n_levels;
@@ -402,7 +411,7 @@ __device__ __forceinline__ void block_solve(const JxbBlock& blk, const SimSmem<T
     for (int w = tid; w < nch * rows; w += NT) {
       const int r = rows == 1 ? 0 : w / nch;
       chain_backsub<T>(sm, c0 + (w - r * nch), sm.D + (size_t)r * nn, sm.S + (size_t)r * nn, al,
-                       V ? V + (size_t)r * nn : nullptr);
+                       V ? V + (size_t)r * nn : nullptr, vscale);
     }
     __syncthreads();
   }
@@ -573,6 +582,8 @@ __device__ __forceinline__ void run_steps(const JxbSimArgs& a, const JxbBlock& b
                                           bool traj_final = false) {
   const int nn = blk.n_nodes, ns = blk.n_slots, np = blk.n_pslots;
   const NodeWalk walk(a, blk, rows, item_block);  // the same visits every step
+  const T dts = solve_dt<T>(a, dt);               // step of the voltage system
+  const T vscale = a.scheme == JXB_SCHEME_CN ? T(2) : T(1);  // v' = v + vscale * increment
   // Whether any node of the block has a voltage clamp (uniform over the CTA).
   int mine = 0;
   if (a.clamp_ptr)
@@ -637,7 +648,7 @@ __device__ __forceinline__ void run_steps(const JxbSimArgs& a, const JxbBlock& b
       // Delta form of the implicit step: A (v' - v) = rhs - A v, with
       // (A v)_j = d_j v_j + sum over neighbours of the off-diagonals times their v,
       // written with voltage differences (exact algebra, small increments).
-      const T lin_t = dt * fdiv(lin, cmv);
+      const T lin_t = dts * fdiv(lin, cmv);
       T axv = T(0);
       const int pj = sm.par[j];
       if (pj >= 0) axv += sm.al[j] * (Vr[pj] - v);
@@ -645,13 +656,13 @@ __device__ __forceinline__ void run_steps(const JxbSimArgs& a, const JxbBlock& b
         const int c = sm.kids[k];
         axv += sm.au[c] * (Vr[c] - v);
       }
-      const T dgj = sm.dg ? sm.dg[j] : ((f & FLAG_COMP) ? T(1) : T(0)) + dt * ((const T*)a.gsum)[i];
+      const T dgj = sm.dg ? sm.dg[j] : ((f & FLAG_COMP) ? T(1) : T(0)) + dts * ((const T*)a.gsum)[i];
       sm.D[(size_t)r * nn + j] = dgj + lin_t;
-      sm.S[(size_t)r * nn + j] = ((f & FLAG_COMP) ? dt * fdiv(cst, cmv) - lin_t * v : T(0)) - axv;
+      sm.S[(size_t)r * nn + j] = ((f & FLAG_COMP) ? dts * fdiv(cst, cmv) - lin_t * v : T(0)) - axv;
     }
     if (step == nsteps) break;
     __syncthreads();
-    block_solve<T>(blk, sm, rows, sm.al, sm.au, sm.V);
+    block_solve<T>(blk, sm, rows, sm.al, sm.au, sm.V, vscale);
     if (vclamps) {
       clamp_voltages<T>(a, blk, sm, row0, rows, t);
       __syncthreads();
@@ -931,6 +942,8 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
   const int tid = threadIdx.x, nthr = blockDim.x;
   const int nn = blk.n_nodes, ns = blk.n_slots, np = blk.n_pslots;
   const T dt = T(a.dt);
+  const T dts = solve_dt<T>(a, dt);  // step of the voltage system
+  const bool cn = a.scheme == JXB_SCHEME_CN;
   const int K = a.n_steps;
   T* traj = (T*)a.traj;
   stage_item<T>(a, blk, row0, rows, sm, dt, (const T*)a.ckpt, (const T*)a.adj, gslots);
@@ -985,7 +998,7 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
       }
       if constexpr (GM) sm.D[(size_t)r * nn + j] = piv[((size_t)step * a.batch + b) * a.n_nodes + i];
       // a clamped voltage after the step does not depend on the solve
-      sm.S[(size_t)r * nn + j] = (f & FLAG_VCLAMP) ? T(0) : lam[0];
+      sm.S[(size_t)r * nn + j] = (f & FLAG_VCLAMP) ? T(0) : (cn ? T(2) * lam[0] : lam[0]);
     }
     __syncthreads();
     // lambda_r = A^{-T} lambda_v'  (solver_voltage.py:168-187), with the pivots of
@@ -1010,18 +1023,21 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
       }
       (void)nslot;
       const T lr = sm.S[(size_t)r * nn + j];
-      const T xnew = sm.X1[(size_t)r * nn + j];
+      // the solve's output: v' (backward Euler) or v_half = (v' + v) / 2 (Crank-Nicolson)
+      const T xnew = cn ? T(0.5) * (sm.X1[(size_t)r * nn + j] + x[0]) : sm.X1[(size_t)r * nn + j];
       const bool comp = (sm.flags[j] & FLAG_COMP) != 0;
       // d = dg + dt * lin / cm,  rhs = v + dt * cst / cm (compartments only; the
-      // branchpoints have no channels).
-      const T lrs = fdiv(T(1000.0) * dt * lr, sm.cm[j]);
+      // branchpoints have no channels); dt is the system's step.
+      const T lrs = fdiv(T(1000.0) * dts * lr, sm.cm[j]);
       T lv = comp ? lr : T(0);
+      // Crank-Nicolson's v' = 2 v_half - v: the adjoint of v' also reaches v directly
+      if (cn && !(sm.flags[j] & FLAG_VCLAMP)) lv -= lam[0];
       if (a.g_syn_lin && a.syn_ptr) {
         // d loss / d (synaptic slope, offset) of node j: the slope enters the
         // diagonal (and, on compartments, the right-hand side as -lin * v), the
         // offset the right-hand side with a minus sign.
         const int i = blk.node0 + j;
-        const T f = fdiv(lr * dt, sm.cm[j]);
+        const T f = fdiv(lr * dts, sm.cm[j]);
         const T gl = comp ? -f * xnew : -f * (xnew - x[0]);
         const T gc = comp ? -f : T(0);
         for (int q = a.syn_ptr[i]; q < a.syn_ptr[i + 1]; ++q) {

@@ -13,7 +13,9 @@ kernel (channel parameters; geometry has no gradient here).
 
 The simulation runs on the CUDA device of the inputs, or on the current CUDA device
 when the inputs are on the CPU (there is no CPU path); the recordings are returned on
-the inputs' device, in the inputs' dtype (float32 or float64). `voltage_solver`
+the inputs' device, in the inputs' dtype (float32 or float64). `solver` is
+`bwd_euler` or `crank_nicolson` (`fwd_euler` and `exp_euler` are not covered).
+`voltage_solver`
 accepts the reference's names: every one of them solves the same tree system, here
 with the chain-ordered DHS solve. `checkpoint_lengths` sets the adjoint's segment
 length (its innermost entry), `compile` is accepted and has no effect (the kernels
@@ -91,8 +93,8 @@ def integrate(module, params: list = [], *, param_state: Optional[list] = None, 
               checkpoint_lengths: Optional[List[int]] = None, all_states: Optional[dict] = None,
               return_states: bool = False, compile: bool = False):
     """Simulates `module` with the fused CUDA kernels (see the module docstring)."""
-    if solver != "bwd_euler":
-        raise NotImplementedError(f"solver={solver!r}: the CUDA step is the backward-Euler step")
+    if solver not in ("bwd_euler", "crank_nicolson"):
+        raise NotImplementedError(f"solver={solver!r}: the CUDA step covers bwd_euler and crank_nicolson")
     if voltage_solver not in VOLTAGE_SOLVERS:
         raise ValueError(f"Unknown voltage_solver: {voltage_solver}.")
     assert module.initialized, "Module is not initialized, run `._initialize()`."
@@ -112,7 +114,8 @@ def integrate(module, params: list = [], *, param_state: Optional[list] = None, 
         raise RuntimeError("jaxley_pytorch_b200.integrate runs on a CUDA device; none is available")
 
     prob = problem_from_module(module, params=params, param_state=param_state, data_stimuli=data_stimuli,
-                               t_max=t_max, delta_t=delta_t, data_clamps=data_clamps, all_states=all_states)
+                               t_max=t_max, delta_t=delta_t, data_clamps=data_clamps, all_states=all_states,
+                               solver=solver)
     if prob.synapses:
         raise NotImplementedError("networks with synapses: use jaxley_pytorch_b200.network.NetworkSimulation "
                                   "or the reference's integrate with the drop-in kernels installed")

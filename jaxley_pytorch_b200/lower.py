@@ -128,6 +128,7 @@ class Lowered:
     n_steps: int
     max_levels: int = 0
     tree_ptr: np.ndarray = field(default_factory=lambda: np.zeros(1, np.int64))
+    scheme: int = 0  # JxbSimArgs.scheme: 0 backward Euler, 1 Crank-Nicolson
 
     @property
     def n_slots(self) -> int:
@@ -867,6 +868,7 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
         state0=state0,
         slot_names=_SlotNames(grp_names, grp_int),
         dt=float(p.dt),
+        scheme=1 if getattr(p, "solver", "bwd_euler") == "crank_nicolson" else 0,
         n_steps=int(p.n_steps),
         max_levels=max_levels,
         tree_ptr=tree_ptr,

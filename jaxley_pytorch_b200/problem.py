@@ -80,6 +80,8 @@ class Problem:
     # (`modules/base.py:3305-3308, 3396-3398`). For a node clamped twice the later
     # entry wins.
     clamps: List[Tuple[str, np.ndarray, np.ndarray]] = field(default_factory=list)
+    # Step scheme of the voltage: "bwd_euler" or "crank_nicolson" (modules/base.py:3327-3365).
+    solver: str = "bwd_euler"
 
     def solve_order_system(self):
         """Per solve position `j`: parent, `g_low[j]` (coupling of row `j` to its
@@ -164,6 +166,7 @@ def problem_from_module(
     delta_t: float = 0.025,
     data_clamps=None,
     all_states: Optional[dict] = None,
+    solver: str = "bwd_euler",
 ) -> Problem:
     """Lower a reference `jx.Module` (jaxley-pytorch) into a `Problem`.
 
@@ -175,9 +178,11 @@ def problem_from_module(
     final states). Every group of the trainable `params` (one per row of
     `module.indices_set_by_trainables`) that sets a channel parameter of nodes
     becomes a `Problem.trainable` group; `problem.trainable_source[q] = (entry, group)`
-    names where group q came from. Only the `bwd_euler` step with the DHS solve is
-    covered, with at most one leading batch dimension.
+    names where group q came from. `solver` is the step scheme, `bwd_euler` or
+    `crank_nicolson`, both with the DHS solve.
     """
+    if solver not in ("bwd_euler", "crank_nicolson"):
+        raise NotImplementedError(f"solver={solver!r}: the CUDA step covers bwd_euler and crank_nicolson")
     import torch
 
     from jaxley_pytorch.integrate import _batch_shape, _expand_states  # noqa: F401
@@ -363,6 +368,7 @@ def problem_from_module(
         current_names=list(base.membrane_current_names),
         trainable=trainable,
         clamps=clamps,
+        solver=solver,
     )
     prob.trainable_source = source
     prob.batch_shape = batch_shape
@@ -429,6 +435,7 @@ def save_problem(problem: Problem, path: str, **extra) -> None:
         "params": list(problem.params), "states": list(problem.states),
         "channels": [], "synapses": [],
         "trainable": [name for name, _ in problem.trainable],
+        "solver": problem.solver,
     }
     for q, (_, nodes) in enumerate(problem.trainable):
         arrays[f"trainable/{q}"] = np.asarray(nodes, dtype=np.int64)
@@ -499,6 +506,7 @@ def load_problem(path: str):
         batch=meta["batch"], current_names=meta["current_names"],
         trainable=[(n, z[f"trainable/{q}"]) for q, n in enumerate(meta.get("trainable", []))],
         clamps=[(n, z[f"clamp/{q}/nodes"], z[f"clamp/{q}/values"]) for q, n in enumerate(meta.get("clamps", []))],
+        solver=meta.get("solver", "bwd_euler"),
     )
     extra = {k[len("extra/"):]: z[k] for k in z.files if k.startswith("extra/")}
     return prob, extra

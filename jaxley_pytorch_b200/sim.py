@@ -299,6 +299,7 @@ class DeviceModel:
         a.pgrad = _ptr(pgrad)
         a.mode = mode
         a.status = self.status.data_ptr()
+        a.scheme = int(getattr(low, "scheme", 0))
         if self.sched_warps:
             a.sched_ptr = t["sched_ptr"].data_ptr()
             a.sched = t["sched"].data_ptr()

@@ -627,7 +627,11 @@ class _Stepper:
         # Assemble (modules/base.py:3257-3264) and solve (solver_voltage.py:250-359).
         lin_t = (lin + syn_lin) / self.cm
         const_t = (const + i_ext + syn_const) / self.cm
-        st["v"] = self._solve(v, lin_t, const_t)
+        if getattr(p, "solver", "bwd_euler") == "crank_nicolson":
+            # half a step of the implicit system, then v' = 2 v_half - v (base.py:3327-3365)
+            st["v"] = 2.0 * self._solve(v, lin_t, const_t, dt=p.dt / 2) - v
+        else:
+            st["v"] = self._solve(v, lin_t, const_t)
         # Voltage clamps after the solve (modules/base.py:3396-3398).
         for name, nodes, vals in getattr(p, "clamps", []) or []:
             if name == "v":
@@ -643,8 +647,9 @@ class _Stepper:
             out[:, node] = vt[:, q]
         return out
 
-    def _solve(self, v, lin, const):
-        p, B, n, dt = self.p, self.B, self.n, self.p.dt
+    def _solve(self, v, lin, const, dt=None):
+        p, B, n = self.p, self.B, self.n
+        dt = p.dt if dt is None else dt
         ax = dt * self.axial
         diags = dt * lin
         diags[:, self.comp] += 1.0

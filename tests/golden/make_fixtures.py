@@ -91,7 +91,8 @@ def save_with_grads(name, module, params, seed, extra=None, **kw):
     ref, grads = reference_grads(module, tensors, w, params=params, **kw)
     prob = problem_from_module(module, params=params, param_state=kw.get("param_state"),
                                t_max=kw.get("t_max"), delta_t=kw.get("delta_t", 0.025),
-                               data_clamps=kw.get("data_clamps"), data_stimuli=kw.get("data_stimuli"))
+                               data_clamps=kw.get("data_clamps"), data_stimuli=kw.get("data_stimuli"),
+                               solver=kw.get("solver", "bwd_euler"))
     extra["loss_w"] = w
     extra["trainable_source"] = np.asarray(prob.trainable_source, dtype=np.int64).reshape(-1, 2)
     for q, g in enumerate(grads):
@@ -374,6 +375,28 @@ def pospischil_cell():
     save_with_grads("pospischil_7x3", cell, cell.get_parameters(), seed=81, delta_t=0.025)
 
 
+def crank_nicolson():
+    """A branched HH cell with a voltage clamp, stepped with Crank-Nicolson
+    (`solver="crank_nicolson"`, modules/base.py:3327-3365), with the reference's
+    gradients."""
+    cell = jx.Cell([jx.Branch(jx.Compartment(), 3)] * 7, parents=binary_parents(7))
+    cell.insert(HH())
+    rng = np.random.default_rng(23)
+    for b in range(7):
+        cell.branch(b).set("radius", float(rng.uniform(0.5, 2.0)))
+        cell.branch(b).set("length", float(rng.uniform(5.0, 40.0)))
+    T = 321
+    t = np.arange(T) * 0.025
+    cell.branch(4).comp(1).clamp("v", np.where((t >= 2.0) & (t < 5.0), -30.0, -70.0), verbose=False)
+    cell.branch(0).comp(0).record(verbose=False)
+    cell.branch(4).comp(2).record(verbose=False)
+    cell.branch(6).comp(2).record("HH_n", verbose=False)
+    cell.branch(0).comp(0).stimulate(jx.step_current(1.0, 2.0, 0.3, 0.025, 8.0), verbose=False)
+    cell.make_trainable("HH_gNa", verbose=False)
+    cell.branch("all").make_trainable("HH_gK", verbose=False)
+    save_with_grads("cn_hh_7x3", cell, cell.get_parameters(), seed=91, delta_t=0.025, solver="crank_nicolson")
+
+
 def reference_l5pc_cell(parents, ncomp, radius, lengths):
     from jaxley_pytorch_b200 import synth
 
@@ -518,10 +541,10 @@ def c4_sample():
 
 if __name__ == "__main__":
     which = [w for w in sys.argv[1:] if w != "synth"] if sys.argv[1:] else [
-        "golden", "small", "tree", "l5pc", "forest", "synapse", "clamp", "pospischil", "c2", "c3", "c4",
+        "golden", "small", "tree", "l5pc", "forest", "synapse", "clamp", "pospischil", "cn", "c2", "c3", "c4",
         "synth"]
     fns = {"golden": golden_cases, "small": config_small, "tree": hh_tree, "l5pc": l5pc_cell,
-           "forest": hh_forest, "synapse": synapse_net, "clamp": clamp_cell, "pospischil": pospischil_cell,
+           "forest": hh_forest, "synapse": synapse_net, "clamp": clamp_cell, "pospischil": pospischil_cell, "cn": crank_nicolson,
            "c2": c2_sample,
            "c3": c3_sample, "c4": c4_sample}
     for w in which:

@@ -44,7 +44,7 @@ def _pgrad(prob, extra, dtype=torch.float64, device="cuda"):
     return low, ps.grad.double().cpu().numpy(), rec.detach().double().cpu().numpy()
 
 
-@pytest.mark.parametrize("name", ["l5pc_7x4_batch3", "hh_clamp_7x3", "pospischil_7x3"])
+@pytest.mark.parametrize("name", ["l5pc_7x4_batch3", "hh_clamp_7x3", "pospischil_7x3", "cn_hh_7x3"])
 def test_make_trainable_groups(cuda_device, name):
     """Every group of every trainable (one per row of indices_set_by_trainables)."""
     prob, extra = load_fixture(name)
