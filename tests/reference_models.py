@@ -120,3 +120,30 @@ def synapse_net(jx):
         net.cell(c).branch(0).comp(1).stimulate(jx.step_current(1.0, 3.0, 0.3, 0.025, 8.0), verbose=False)
     net.make_trainable("HH_gNa", verbose=False)
     return net, {"delta_t": 0.025}
+
+
+def hh_tree_cn(jx):
+    """`hh_tree` stepped with Crank-Nicolson (modules/base.py:3327-3365)."""
+    cell, kw = hh_tree(jx)
+    return cell, dict(kw, solver="crank_nicolson")
+
+
+def pospischil_cell(jx):
+    """A branched cell with the Pospischil channels (Na, K, Km, CaT, Leak) and
+    trainable conductances, threshold vt and CaT's vx."""
+    from jaxley_pytorch.channels.pospischil import CaT, K, Km, Leak, Na
+
+    cell = jx.Cell([jx.Branch(jx.Compartment(), 2)] * 5, parents=[-1, 0, 0, 1, 1])
+    for ch in (Na(), K(), Leak()):
+        cell.insert(ch)
+    cell.branch([0, 1]).insert(Km())
+    cell.branch([0, 3]).insert(CaT())
+    cell.set("v", -70.0)
+    cell.init_states()
+    cell.branch(0).comp(0).record(verbose=False)
+    cell.branch(4).comp(1).record(verbose=False)
+    cell.branch(0).comp(0).stimulate(jx.step_current(1.0, 3.0, 0.1, 0.025, 8.0), verbose=False)
+    cell.make_trainable("Na_gNa", verbose=False)
+    cell.make_trainable("vt", verbose=False)
+    cell.make_trainable("CaT_vx", verbose=False)
+    return cell, {"delta_t": 0.025}

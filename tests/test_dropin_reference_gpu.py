@@ -25,7 +25,7 @@ from conftest import import_reference
 
 pytestmark = pytest.mark.gpu
 
-CELLS = ["hh_tree", "l5pc_cell", "clamped_cell"]
+CELLS = ["hh_tree", "l5pc_cell", "clamped_cell", "hh_tree_cn", "pospischil_cell"]
 
 
 def _build(jx, name):
