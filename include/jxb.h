@@ -277,6 +277,19 @@ int jxb_sim_backward(const JxbSimArgs* args, void* stream);
  * in the array needs to start at zero: every slot a segment reads was written earlier
  * in the same launch. It calls no cudaMalloc, cudaFree or allocating library routine. */
 int jxb_sim_backward_noalloc(const JxbSimArgs* args, void* stream);
+
+/* Forward-mode derivatives: a forward launch (mode 0, 1 or 2) in dual numbers. Every
+ * floating-point array of `args` (a_low, a_up, gsum, cm, pbase, pscale, area, stim,
+ * clamp, state, rec_out, ckpt) holds (value, tangent) pairs of the element type
+ * `dtype`, interleaved and aligned to the pair size (8 or 16 bytes); the launch
+ * advances both, so that the tangents of the states and recordings are the
+ * directional derivatives along the inputs' tangents. Replaces the reference's
+ * forward-mode rule of the tree solve inside a forward-AD level (_DHSSolveForwardAD,
+ * solver_voltage.py:190-224; dhs_solve, :235-236) for the fused step. Trajectory
+ * stores, synapse inputs and multi-request launches are not taken (traj, traj_piv,
+ * syn_lin, syn_const and multi must be null). Up to 512 threads. */
+int jxb_sim_tangent(const JxbSimArgs* args, void* stream);
+int64_t jxb_sim_tangent_smem_bytes(const JxbSimArgs* args);
 int64_t jxb_sim_smem_bytes(const JxbSimArgs* args, int backward);
 
 /* Continuous batching of requests (no counterpart in the reference, whose

@@ -105,6 +105,8 @@ EXPORTED = [
     "jxb_sim_backward",
     "jxb_sim_backward_noalloc",
     "jxb_sim_smem_bytes",
+    "jxb_sim_tangent",
+    "jxb_sim_tangent_smem_bytes",
     "jxb_sim_forward_multi",
     "jxb_sim_backward_multi",
     "jxb_sim_multi_scratch_bytes",
@@ -131,7 +133,9 @@ def load(path: str = LIB_PATH) -> C.CDLL:
     lib.jxb_version.restype = C.c_int
     lib.jxb_sim_smem_bytes.restype = C.c_int64
     lib.jxb_sim_smem_bytes.argtypes = [C.POINTER(JxbSimArgs), C.c_int]
-    for name in ["jxb_sim_forward", "jxb_sim_backward", "jxb_sim_backward_noalloc"]:
+    lib.jxb_sim_tangent_smem_bytes.restype = C.c_int64
+    lib.jxb_sim_tangent_smem_bytes.argtypes = [C.POINTER(JxbSimArgs)]
+    for name in ["jxb_sim_forward", "jxb_sim_backward", "jxb_sim_backward_noalloc", "jxb_sim_tangent"]:
         fn = getattr(lib, name)
         fn.restype = C.c_int
         fn.argtypes = [C.POINTER(JxbSimArgs), C.c_void_p]

@@ -45,10 +45,20 @@ __device__ __forceinline__ double rcp(double b) { return 1.0 / b; }
 template <typename T>
 struct Dual {
   T v, d;
-  __device__ __forceinline__ Dual() {}
-  __device__ __forceinline__ Dual(T a) : v(a), d(T(0)) {}
-  __device__ __forceinline__ Dual(T a, T b) : v(a), d(b) {}
+  __host__ __device__ __forceinline__ Dual() {}
+  __host__ __device__ __forceinline__ Dual(T a) : v(a), d(T(0)) {}
+  __host__ __device__ __forceinline__ Dual(T a, T b) : v(a), d(b) {}
+  __device__ __forceinline__ Dual& operator+=(Dual b) { v += b.v; d += b.d; return *this; }
+  __device__ __forceinline__ Dual& operator-=(Dual b) { v -= b.v; d -= b.d; return *this; }
+  __device__ __forceinline__ Dual& operator*=(Dual b) { d = d * b.v + v * b.d; v *= b.v; return *this; }
 };
+// Comparisons look at the value (a branch of the function, not of its derivative).
+template <typename T> __device__ __forceinline__ bool operator<(Dual<T> a, Dual<T> b) { return a.v < b.v; }
+template <typename T> __device__ __forceinline__ bool operator>(Dual<T> a, Dual<T> b) { return a.v > b.v; }
+template <typename T> __device__ __forceinline__ bool operator!=(Dual<T> a, Dual<T> b) { return a.v != b.v || a.d != b.d; }
+__device__ __forceinline__ bool is_finite(float x) { return ::isfinite(x); }
+__device__ __forceinline__ bool is_finite(double x) { return ::isfinite(x); }
+template <typename T> __device__ __forceinline__ bool is_finite(Dual<T> a) { return is_finite(a.v) && is_finite(a.d); }
 template <typename T> __device__ __forceinline__ Dual<T> operator+(Dual<T> a, Dual<T> b) { return Dual<T>(a.v + b.v, a.d + b.d); }
 template <typename T> __device__ __forceinline__ Dual<T> operator-(Dual<T> a, Dual<T> b) { return Dual<T>(a.v - b.v, a.d - b.d); }
 template <typename T> __device__ __forceinline__ Dual<T> operator-(Dual<T> a) { return Dual<T>(-a.v, -a.d); }

@@ -189,6 +189,8 @@ static int check_sim_args(const JxbSimArgs* a, bool backward) {
   return JXB_OK;
 }
 
+int check_sim_args_public(const JxbSimArgs* a, bool backward) { return check_sim_args(a, backward); }
+
 }  // namespace jxb
 
 using namespace jxb;

@@ -715,7 +715,7 @@ __device__ __forceinline__ void sim_forward_body(const JxbSimArgs& a, const JxbS
     for (int q = threadIdx.x; q < ns; q += blockDim.x) {
       const T val = s[q];
       g[q] = val;
-      bad |= !isfinite(val);
+      bad |= !is_finite(val);
     }
   }
   report_nonfinite(a, bad);
@@ -906,6 +906,7 @@ __device__ __forceinline__ void block_solve_pivots(const JxbBlock& blk, const Si
 template <typename T>
 __device__ __forceinline__ void cp_async_elem(T* smem_dst, const T* gsrc) {
   const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  static_assert(sizeof(T) == 4 || sizeof(T) == 8, "element copies of 4 or 8 bytes");
   if constexpr (sizeof(T) == 4)
     asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(s), "l"(gsrc) : "memory");
   else
@@ -1099,7 +1100,7 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
     for (int k = 0; k < npar; ++k) {
       const int q = sm.gk[po + k];
       if (q >= 0 && ga[q] != T(0)) {
-        bad |= !isfinite(ga[q]);
+        bad |= !is_finite(ga[q]);
         atomicAdd(pg + sm.pc[po + k], (double)ga[q]);
       }
     }
@@ -1111,7 +1112,7 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
     for (int q = tid; q < ns; q += nthr) {
       const T val = sa[q];
       ga[q] = val;
-      bad |= !isfinite(val);
+      bad |= !is_finite(val);
     }
   }
   report_nonfinite(a, bad);

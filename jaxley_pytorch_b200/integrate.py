@@ -29,7 +29,7 @@ import numpy as np
 import torch
 
 from .lower import lower
-from .problem import problem_from_module
+from .problem import differentiable, host_mode, problem_from_module
 from .sim import Simulation
 
 VOLTAGE_SOLVERS = ("jaxley.dhs", "jaxley.dhs.cpu", "jaxley.dhs.gpu", "jaxley.stone",
@@ -51,6 +51,15 @@ def _first_float_tensor(*trees):
             elif isinstance(x, (list, tuple)):
                 stack.extend(x)
     return None
+
+
+def _has_tangent(x) -> bool:
+    """Whether a tensor carries a forward-mode tangent."""
+    import torch.autograd.forward_ad as fwAD
+
+    if torch._C._functorch.is_functorch_wrapped_tensor(x):
+        return True
+    return fwAD._current_level >= 0 and fwAD.unpack_dual(x).tangent is not None
 
 
 def _group_values(t: torch.Tensor, g: int, batch_shape, device, dtype) -> torch.Tensor:
@@ -113,26 +122,32 @@ def integrate(module, params: list = [], *, param_state: Optional[list] = None, 
     else:
         raise RuntimeError("jaxley_pytorch_b200.integrate runs on a CUDA device; none is available")
 
-    prob = problem_from_module(module, params=params, param_state=param_state, data_stimuli=data_stimuli,
-                               t_max=t_max, delta_t=delta_t, data_clamps=data_clamps, all_states=all_states,
-                               solver=solver)
-    if prob.synapses:
-        raise NotImplementedError("networks with synapses: use jaxley_pytorch_b200.network.NetworkSimulation "
-                                  "or the reference's integrate with the drop-in kernels installed")
-    K = int(checkpoint_lengths[-1]) if checkpoint_lengths else 100
-    low = lower(prob)
-    sim = Simulation(prob, low=low, dtype=dtype, device=sim_device, checkpoint=K)
+    with host_mode():  # the host-side assembly reads tensors, also under torch.func transforms
+        prob = problem_from_module(module, params=params, param_state=param_state, data_stimuli=data_stimuli,
+                                   t_max=t_max, delta_t=delta_t, data_clamps=data_clamps,
+                                   all_states=all_states, solver=solver)
+        if prob.synapses:
+            raise NotImplementedError("networks with synapses: use jaxley_pytorch_b200.network.NetworkSimulation "
+                                      "or the reference's integrate with the drop-in kernels installed")
+        K = int(checkpoint_lengths[-1]) if checkpoint_lengths else 100
+        low = lower(prob)
+        sim = Simulation(prob, low=low, dtype=dtype, device=sim_device, checkpoint=K)
     pscale = sim.model.pscale
     sources = [list(e.values())[0] for e in params] + [e["val"] for e in (param_state or [])]
-    wants_grad = torch.is_grad_enabled() and any(
-        isinstance(t, torch.Tensor) and t.requires_grad for t in sources)
-    if wants_grad and prob.trainable:
+    for tree in (data_stimuli[1] if data_stimuli is not None else [],
+                 data_clamps[1] if data_clamps is not None else [], list((all_states or {}).values())):
+        if any(isinstance(x, torch.Tensor) and _has_tangent(x) for x in tree):
+            raise NotImplementedError("forward-mode derivatives with respect to stimuli, clamps or states "
+                                      "are not covered")
+    wants = any(differentiable(t) for t in sources) and (
+        torch.is_grad_enabled() or torch.autograd.forward_ad._current_level >= 0)
+    if wants and prob.trainable:
         cols, base = low.group_scale()
         columns = list(pscale.unbind(1))
         B = pscale.shape[0]
         for q, (src, g) in enumerate(prob.trainable_source):
             t = sources[src]
-            if not (isinstance(t, torch.Tensor) and t.requires_grad):
+            if not differentiable(t):
                 continue
             if cols[q] <= 0:
                 raise NotImplementedError(f"trainable {prob.trainable[q][0]}: its nodes do not share one value")
@@ -144,7 +159,8 @@ def integrate(module, params: list = [], *, param_state: Optional[list] = None, 
     rec = rec.reshape(shape).to(out_device)
     if not return_states:
         return rec
-    states = named_states(sim, prob, sim.last_state)
-    n = prob.n_nodes
-    states = {k: v.reshape(tuple(prob.batch_shape) + (n,)).to(out_device) for k, v in states.items()}
+    with host_mode():
+        states = named_states(sim, prob, sim.last_state)
+        n = prob.n_nodes
+        states = {k: v.reshape(tuple(prob.batch_shape) + (n,)).to(out_device) for k, v in states.items()}
     return rec, states

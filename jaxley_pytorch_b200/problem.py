@@ -136,10 +136,44 @@ def _flatten_to(a: np.ndarray, batch_shape: tuple, core: int = 1) -> np.ndarray:
     return np.broadcast_to(a, tuple(batch_shape) + tail).reshape((-1,) + tail)
 
 
+def unwrap(x):
+    """The plain tensor under the wrappers of `torch.func` transforms (`jvp`, `grad`),
+    whose data cannot be read directly (other values unchanged)."""
+    import torch
+
+    ft = torch._C._functorch
+    while isinstance(x, torch.Tensor) and ft.is_functorch_wrapped_tensor(x):
+        x = ft.get_unwrapped(x)
+    return x
+
+
+def host_mode():
+    """A context in which tensors can be read on the host (`.numpy()`, `data_ptr()`)
+    also inside `torch.func` transforms: their functorch layers are switched off, and
+    tensors made inside are plain."""
+    import torch
+
+    return torch._C._DisableFuncTorch()
+
+
+def differentiable(x) -> bool:
+    """Whether a tensor asks for derivatives: it requires grad (reverse mode) or
+    carries a forward-mode tangent (`torch.autograd.forward_ad`, `torch.func.jvp`)."""
+    import torch
+    import torch.autograd.forward_ad as fwAD
+
+    if not isinstance(x, torch.Tensor):
+        return False
+    if x.requires_grad or torch._C._functorch.is_functorch_wrapped_tensor(x):
+        return True
+    return fwAD._current_level >= 0 and fwAD.unpack_dual(x).tangent is not None
+
+
 def _cpu64(x):
     """A detached CPU float64 copy of a tensor (other values unchanged)."""
     import torch
 
+    x = unwrap(x)
     if isinstance(x, torch.Tensor):
         return x.detach().to(device="cpu", dtype=torch.float64)
     return x
@@ -149,6 +183,7 @@ def _broadcast_last(x) -> bool:
     """Whether the last dimension of a tensor is a broadcast (stride 0) of one value."""
     import torch
 
+    x = unwrap(x)
     return isinstance(x, torch.Tensor) and x.dim() > 0 and x.shape[-1] > 1 and x.stride(-1) == 0
 
 
@@ -195,7 +230,7 @@ def problem_from_module(
     module.to_torch(device=device, dtype=dtype)
     # Inputs may live on any device and dtype: the problem is assembled from detached
     # float64 copies on the CPU (which entries ask for gradients is noted first).
-    ps_grad = [(isinstance(e["val"], torch.Tensor) and e["val"].requires_grad, _broadcast_last(e["val"]))
+    ps_grad = [(differentiable(e["val"]), _broadcast_last(e["val"]))
                for e in (param_state or [])]
     params = [{k: _cpu64(v) for k, v in e.items()} for e in params]
     if param_state is not None:

@@ -17,7 +17,7 @@ import torch
 
 from . import _lib
 from .lower import Lowered, lower
-from .problem import Problem
+from .problem import Problem, host_mode, unwrap
 
 
 def _dtype_code(dtype: torch.dtype) -> int:
@@ -90,16 +90,24 @@ class DeviceModel:
     def __init__(self, low: Lowered, dtype: torch.dtype = torch.float32, device="cuda",
                  rows_per_item: int = 1, threads: int = 256, programs: bool = True,
                  smem_limit: Optional[int] = None, schedule: bool = True,
-                 forward_threads: Optional[int] = None, forward_wide: bool = False):
+                 forward_threads: Optional[int] = None, forward_wide: bool = False,
+                 tangent: bool = False):
         self.low = low
         self.dtype = dtype
         self.device = torch.device(device)
         self.code = _dtype_code(dtype)
-        self.itemsize = torch.empty((), dtype=dtype).element_size()
+        # With `tangent`, every floating-point array holds (value, tangent) pairs in a
+        # trailing dimension of 2 (tangents zero) and only forward launches are taken
+        # (`jxb_sim_tangent`, the forward kernel in dual numbers).
+        self.tangent = bool(tangent)
+        self.itemsize = torch.empty((), dtype=dtype).element_size() * (2 if tangent else 1)
         dev = self.device
 
         def f(x):
-            return torch.as_tensor(np.asarray(x, dtype=np.float64), dtype=dtype, device=dev).contiguous()
+            x = torch.as_tensor(np.asarray(x, dtype=np.float64), dtype=dtype, device=dev)
+            if tangent:
+                x = torch.stack([x, torch.zeros_like(x)], -1)
+            return x.contiguous()
 
         def i(x):
             return torch.as_tensor(np.asarray(x, dtype=np.int32), device=dev).contiguous()
@@ -148,7 +156,9 @@ class DeviceModel:
         # Threads per CTA of each launch kind (the forward may use fewer, with the wide
         # register budget of JxbSimArgs.wide) and a node schedule for each warp count.
         self.kind_threads = {"forward": int(forward_threads or threads), "backward": int(threads)}
-        self.forward_wide = bool(forward_wide)
+        if tangent:
+            self.kind_threads["forward"] = min(self.kind_threads["forward"], 512)
+        self.forward_wide = bool(forward_wide) and not tangent
         self.sched_warps = 0
         self.kind_sched: Dict[str, tuple] = {}
         if schedule:
@@ -194,6 +204,8 @@ class DeviceModel:
             setattr(a, k, v)
         a.n_entries = int(self.low.entries.shape[0])
         a.n_classes = len(self.low.cls_comp)
+        if self.tangent and not backward:
+            return int(_lib.load().jxb_sim_tangent_smem_bytes(C.byref(a)))
         return int(_lib.load().jxb_sim_smem_bytes(C.byref(a), int(backward)))
 
     def set_rows_per_item(self, rows: int) -> None:
@@ -284,7 +296,7 @@ class DeviceModel:
             a.clamp_slot = t["clamp_slot"].data_ptr()
             a.clamp_col = t["clamp_col"].data_ptr()
             a.clamp = self.clamp.data_ptr()
-            a.clamp_steps, a.clamp_rows, a.n_clamp = self.clamp.shape
+            a.clamp_steps, a.clamp_rows, a.n_clamp = self.clamp.shape[:3]
         a.syn_lin = _ptr(syn_lin)
         a.syn_const = _ptr(syn_const)
         a.rec_out = _ptr(rec_out)
@@ -388,16 +400,22 @@ class DeviceModel:
             raise FloatingPointError(f"the {what} produced values that are not finite (NaN or inf)")
 
     def launch_forward(self, args: _lib.JxbSimArgs, stream=None) -> None:
-        self._launch("forward", _lib.load().jxb_sim_forward, args, stream)
+        lib = _lib.load()
+        self._launch("forward", lib.jxb_sim_tangent if self.tangent else lib.jxb_sim_forward, args, stream)
 
     def launch_backward(self, args: _lib.JxbSimArgs, stream=None) -> None:
+        if self.tangent:
+            raise RuntimeError("a tangent model runs forward launches only")
         self._launch("backward", _lib.load().jxb_sim_backward, args, stream)
 
     def initial_state(self) -> torch.Tensor:
-        """A fresh copy of the initial state (uploaded once, copied on the device)."""
+        """A fresh copy of the initial state (uploaded once, copied on the device);
+        (value, zero tangent) pairs for a tangent model."""
         if getattr(self, "_state0", None) is None:
-            self._state0 = torch.as_tensor(self.low.state0, dtype=self.dtype,
-                                           device=self.device).contiguous()
+            s0 = torch.as_tensor(self.low.state0, dtype=self.dtype, device=self.device)
+            if self.tangent:
+                s0 = torch.stack([s0, torch.zeros_like(s0)], -1)
+            self._state0 = s0.contiguous()
         return self._state0.clone()
 
 
@@ -537,6 +555,48 @@ class Simulation:
             m.launch_backward(a)
         return pgrad
 
+    def tangent_model(self) -> DeviceModel:
+        """The model's arrays as (value, tangent) pairs, for `jvp` (built once)."""
+        if getattr(self, "_tangent", None) is None:
+            m = self.model
+            self._tangent = DeviceModel(self.low, m.dtype, m.device, m.rows_per_item, threads=m.threads,
+                                        schedule=bool(m.kind_sched), tangent=True)
+        return self._tangent
+
+    def jvp(self, pscale: torch.Tensor, pscale_tangent: torch.Tensor, n_steps: Optional[int] = None,
+            state_tangent: Optional[torch.Tensor] = None):
+        """Forward-mode derivative: returns the recordings `(B, n_rec, T + 1)` and their
+        directional derivative along `pscale_tangent` (the tangent of the per-row
+        parameter scales `(B, n_cols)`) and `state_tangent` (that of the initial state
+        `(B, n_slots)`, default zero), as `torch.func.jvp` through the reference's
+        `integrate` gives them (its tree solve's forward-mode rule,
+        `solver_voltage.py:190-224`). One launch sequence of the forward kernel in dual
+        numbers; the steps are the same launches as `run`'s."""
+        if self.problem.synapses:
+            raise NotImplementedError("forward-mode derivatives cover cells without synapses")
+        tm = self.tangent_model()
+        low = self.low
+        T = self.n_steps(n_steps)
+        dt = tm.dtype
+        ps = torch.stack([pscale.detach().to(device=tm.device, dtype=dt),
+                          pscale_tangent.detach().to(device=tm.device, dtype=dt)], -1).contiguous()
+        state = tm.initial_state()
+        if state_tangent is not None:
+            state[..., 1] = state_tangent.to(device=tm.device, dtype=dt)
+        rec = torch.zeros((T + 1, low.batch, low.n_rec, 2), dtype=dt, device=tm.device)
+        tm.launch_forward(tm.args(state, 0, 0, rec, mode=2 if self.init_steady else 1, pscale=ps))
+        seg = T if not self.segment else int(self.segment)
+        t = 0
+        while t < T:
+            k = min(seg, T - t)
+            tm.launch_forward(tm.args(state, k, t, rec, pscale=ps))
+            t += k
+        if self.check_finite:
+            tm.check_finite("forward-mode derivative")
+        out = rec.permute(1, 2, 0, 3)
+        self.last_state_tangent = state  # (B, n_slots, 2)
+        return out[..., 0], out[..., 1]
+
     def run(self, n_steps: Optional[int] = None, pscale: Optional[torch.Tensor] = None,
             return_state: bool = False):
         """Recordings `(B, n_rec, T + 1)`; differentiable with respect to `pscale`
@@ -544,9 +604,9 @@ class Simulation:
         T = self.n_steps(n_steps)
         if pscale is None:
             pscale = self.model.pscale
-        if pscale.requires_grad and torch.is_grad_enabled():
-            out = _IntegrateFn.apply(pscale, self, T)
-            return out
+        reverse = pscale.requires_grad and torch.is_grad_enabled()
+        if reverse or torch.autograd.forward_ad._current_level >= 0:
+            return _IntegrateFn.apply(pscale, self, T, _Stash(reverse))
         rec, state = self.forward_raw(pscale.detach().contiguous(), T)
         if self.check_finite:
             self.model.check_finite("simulation")
@@ -554,46 +614,80 @@ class Simulation:
         return (out, state) if return_state else out
 
 
+class _Stash:
+    """Hands `_IntegrateFn.forward`'s saved tensors to its `setup_context` (an object,
+    so that `torch.func` passes it through unchanged)."""
+
+    def __init__(self, reverse: bool):
+        self.reverse = reverse
+        self.saved = None
+
+
 class _IntegrateFn(torch.autograd.Function):
     """Forward: the fused step kernels, storing the trajectory (states and pivots of
     every step) or a checkpoint every `sim.checkpoint` steps. Backward: the adjoint
     kernel per segment of `sim.checkpoint` steps, in reverse order (reverse sweep over
     the stored trajectory, or recompute + reverse sweep), instead of autograd through
-    every operation of every step."""
+    every operation of every step. Forward-mode rule (`torch.autograd.forward_ad`,
+    `torch.func.jvp`): the steps once more in dual numbers (`Simulation.jvp`).
+
+    With `stash.reverse` false (forward mode only) the forward stores no trajectory.
+    Under `torch.func.jvp` / `torch.func.grad` the rules unwrap their operands and run
+    the kernels with the functorch layers off (`host_mode`)."""
 
     @staticmethod
-    def forward(ctx, pscale, sim, T):
+    def forward(pscale, sim, T, stash):
         low = sim.low
         K = sim.checkpoint
         nseg = (T + K - 1) // K
         ps = pscale.detach().to(sim.model.dtype).contiguous()
         dev, dt = sim.model.device, sim.model.dtype
-        ctx.stored = sim.stores_trajectory(T)
-        if ctx.stored:
+        stored = stash.reverse and sim.stores_trajectory(T)
+        if not stash.reverse:
+            rec, _ = sim.forward_raw(ps, T)
+            stash.saved = (False, ps)
+        elif stored:
             traj = torch.empty((T + 1, low.batch, low.n_slots), dtype=dt, device=dev)
             piv = torch.empty((T, low.batch, low.n_nodes), dtype=dt, device=dev)
             rec, _ = sim.forward_raw(ps, T, traj=traj, piv=piv)
-            ctx.save_for_backward(ps, traj, piv)
+            stash.saved = (True, ps, traj, piv)
         else:
             ckpt = torch.empty((nseg, low.batch, low.n_slots), dtype=dt, device=dev)
             rec, _ = sim.forward_raw(ps, T, ckpt=ckpt)
-            ctx.save_for_backward(ps, ckpt)
-        ctx.sim, ctx.T = sim, T
-        ctx.in_dtype = pscale.dtype
+            stash.saved = (False, ps, ckpt)
         if sim.check_finite:
             sim.model.check_finite("simulation")
         return rec.permute(1, 2, 0)
 
     @staticmethod
+    def setup_context(ctx, inputs, output):
+        pscale, sim, T, stash = inputs
+        ctx.sim, ctx.T = sim, T
+        ctx.in_dtype = pscale.dtype
+        ctx.saved, stash.saved = stash.saved, None
+
+    @staticmethod
     def backward(ctx, grad_out):
         sim = ctx.sim
-        rec_grad = grad_out.to(sim.model.dtype).permute(2, 0, 1).contiguous()
-        if ctx.stored:
-            ps, traj, piv = ctx.saved_tensors
-            pgrad = sim.backward_stored(ps, ctx.T, traj, piv, rec_grad)
-        else:
-            ps, ckpt = ctx.saved_tensors
-            pgrad = sim.backward_raw(ps, ctx.T, ckpt, rec_grad)
-        if sim.check_finite:
-            sim.model.check_finite("adjoint")
-        return pgrad.to(ctx.in_dtype), None, None
+        if len(ctx.saved) < 3:
+            raise RuntimeError("the simulation ran for forward-mode derivatives only (no trajectory stored)")
+        with host_mode():
+            rec_grad = unwrap(grad_out).detach().to(sim.model.dtype).permute(2, 0, 1).contiguous()
+            if ctx.saved[0]:
+                _, ps, traj, piv = ctx.saved
+                pgrad = sim.backward_stored(ps, ctx.T, traj, piv, rec_grad)
+            else:
+                _, ps, ckpt = ctx.saved
+                pgrad = sim.backward_raw(ps, ctx.T, ckpt, rec_grad)
+            if sim.check_finite:
+                sim.model.check_finite("adjoint")
+            pgrad = pgrad.to(ctx.in_dtype)
+        return pgrad, None, None, None
+
+    @staticmethod
+    def jvp(ctx, t_pscale, _sim, _T, _stash):
+        sim = ctx.sim
+        with host_mode():
+            _, rec_t = sim.jvp(ctx.saved[1], unwrap(t_pscale).detach(), ctx.T)
+            rec_t = rec_t.to(ctx.in_dtype)
+        return rec_t

@@ -81,12 +81,35 @@ def reference_grads(module, tensors, loss_w, **kw):
     return rec.detach().numpy(), [t.grad.detach().numpy().copy() for t in tensors]
 
 
-def save_with_grads(name, module, params, seed, extra=None, **kw):
+def reference_jvp(module, params, seed, **kw):
+    """`(directions, tangent)`: seeded directions for the trainable `params` and the
+    reference's forward-mode derivative of its `jx.integrate` recordings along them
+    (`torch.func.jvp`, through `_DHSSolveForwardAD`, solver_voltage.py:190-224)."""
+    keys = [list(p.keys())[0] for p in params]
+    vals = tuple(list(p.values())[0].detach().clone() for p in params)
+    rng = np.random.default_rng(seed)
+    dirs = tuple(torch.as_tensor(rng.normal(size=v.shape)) * v.abs().clamp_min(1e-3) for v in vals)
+
+    def run(*xs):
+        return jx.integrate(module, params=[{k: x} for k, x in zip(keys, xs)], **kw)
+
+    _, tangent = torch.func.jvp(run, vals, dirs)
+    return [d.numpy() for d in dirs], tangent.detach().numpy()
+
+
+def save_with_grads(name, module, params, seed, extra=None, jvp=False, **kw):
     """A fixture of `module` with the reference's gradients with respect to the
-    trainable `params` (entry q, group g -> `extra/grad_q`) of a linear loss."""
+    trainable `params` (entry q, group g -> `extra/grad_q`) of a linear loss, and with
+    `jvp` its forward-mode derivative along seeded directions (`extra/jvp_dir_q`,
+    `extra/jvp`)."""
     extra = dict(extra or {})
     probe = jx.integrate(module, params=params, **kw).detach().numpy()
     w = loss_weights(probe.shape, seed)
+    if jvp:
+        dirs, tangent = reference_jvp(module, params, seed + 1, **kw)
+        for q, d in enumerate(dirs):
+            extra[f"jvp_dir_{q}"] = d
+        extra["jvp"] = tangent
     tensors = [list(p.values())[0] for p in params]
     ref, grads = reference_grads(module, tensors, w, params=params, **kw)
     prob = problem_from_module(module, params=params, param_state=kw.get("param_state"),
@@ -324,7 +347,7 @@ def clamp_cell():
     cell.make_trainable("HH_gNa", verbose=False)
     cell.branch(3).make_trainable("HH_gK", verbose=False)
     cell.branch("all").make_trainable("HH_gLeak", verbose=False)
-    save_with_grads("hh_clamp_7x3", cell, cell.get_parameters(), seed=41, delta_t=0.025)
+    save_with_grads("hh_clamp_7x3", cell, cell.get_parameters(), seed=41, delta_t=0.025, jvp=True)
 
 
 def pospischil_cell():
@@ -372,7 +395,7 @@ def pospischil_cell():
     cell.make_trainable("CaT_vx", verbose=False)
     cell.make_trainable("CaT_gCaT", verbose=False)
     cell.make_trainable("CaL_gCaL", verbose=False)
-    save_with_grads("pospischil_7x3", cell, cell.get_parameters(), seed=81, delta_t=0.025)
+    save_with_grads("pospischil_7x3", cell, cell.get_parameters(), seed=81, delta_t=0.025, jvp=True)
 
 
 def crank_nicolson():
@@ -394,7 +417,8 @@ def crank_nicolson():
     cell.branch(0).comp(0).stimulate(jx.step_current(1.0, 2.0, 0.3, 0.025, 8.0), verbose=False)
     cell.make_trainable("HH_gNa", verbose=False)
     cell.branch("all").make_trainable("HH_gK", verbose=False)
-    save_with_grads("cn_hh_7x3", cell, cell.get_parameters(), seed=91, delta_t=0.025, solver="crank_nicolson")
+    save_with_grads("cn_hh_7x3", cell, cell.get_parameters(), seed=91, delta_t=0.025, jvp=True,
+                    solver="crank_nicolson")
 
 
 def reference_l5pc_cell(parents, ncomp, radius, lengths):

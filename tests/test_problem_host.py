@@ -68,3 +68,34 @@ def test_short_clamp_is_refused():
     cell, kw = rm.clamped_cell(jx, torch)
     with pytest.raises(NotImplementedError):
         problem_from_module(cell, data_clamps=kw["data_clamps"], t_max=20.0, delta_t=0.025)
+
+
+def test_differentiable_and_unwrap():
+    """Inputs that ask for derivatives are recognised in reverse mode, inside a
+    forward-AD level and under `torch.func.jvp`, whose wrapped tensors are read
+    through `unwrap` in `host_mode`."""
+    import torch
+    import torch.autograd.forward_ad as fwAD
+
+    from jaxley_pytorch_b200.problem import _cpu64, differentiable, host_mode, unwrap
+
+    x = torch.tensor([1.0, 2.0], dtype=torch.float64)
+    assert not differentiable(x) and not differentiable(3.0)
+    assert differentiable(x.clone().requires_grad_(True))
+    with fwAD.dual_level():
+        d = fwAD.make_dual(x, torch.ones_like(x))
+        assert differentiable(d)
+        assert not differentiable(x)
+        assert torch.equal(_cpu64(d), x)
+    seen = {}
+
+    def f(y):
+        seen["diff"] = differentiable(y)
+        with host_mode():
+            seen["val"] = _cpu64(y).numpy().copy()
+        seen["plain"] = unwrap(y) is not y
+        return y * 2
+
+    torch.func.jvp(f, (x,), (torch.ones_like(x),))
+    assert seen["diff"] and seen["plain"]
+    np.testing.assert_array_equal(seen["val"], [1.0, 2.0])
