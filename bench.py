@@ -83,6 +83,8 @@ def parse():
     ap.add_argument("--lm-tokens", type=int, default=10, help="tokens of 200 solver steps per training step")
     ap.add_argument("--no-fp32-error", action="store_true",
                     help="skip the float32-against-float64 error of the sampled configurations")
+    ap.add_argument("--no-kernel-compare", action="store_true",
+                    help="skip the standalone drop-in ops against the reference's Triton kernels")
     ap.add_argument("--serve-requests", type=int, default=240)
     ap.add_argument("--serve-capacity-requests", type=int, default=160)
     return ap.parse_args()
@@ -785,6 +787,143 @@ def run_lm(args, device, n_cells: int):
             "value": n_cells * 32 * T / (ms / 1e3), "unit": UNIT, "loss": float(it.loss)}
 
 
+def _device_us(fn, reps: int) -> float:
+    """Mean device time of `fn` in microseconds (CUDA events on the current stream,
+    after one untimed call)."""
+    import torch
+
+    fn()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(reps):
+        fn()
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) * 1e3 / reps
+
+
+def run_kernel_compare(device, reps: int = 200):
+    """The standalone drop-in ops against the reference's Triton kernels, both on this
+    GPU with the same inputs: the tree solve (`kernels/tree_solve.py`, registers and
+    levels variants) on the 300 x 4 L5PC tree with 256 rows and on a forest of 512
+    small trees with 32 rows, and the synapse step (`kernels/synapse_step.py`,
+    KineticSynapse forward and backward with the gS gradient) at the language-model
+    shapes (1024 and 2048 targets x 100 inputs, 32 rows), float32. Inputs stay in L2
+    between calls, as in the reference's step loop. `fraction_of_hbm` counts one read
+    of the operands and one write of the results."""
+    import torch
+
+    jx = import_reference()
+    if jx is None:
+        return {"unavailable": "the reference is not installed under baseline/_ref"}
+    try:
+        import triton  # noqa: F401
+        from jaxley_pytorch.kernels import synapse_step as rss
+        from jaxley_pytorch.kernels import tree_solve as rts
+    except Exception as e:  # noqa: BLE001
+        return {"unavailable": f"the reference's Triton kernels do not import: {e!r}"[:300]}
+    if not (rts.HAS_TRITON and rss.HAS_TRITON):
+        return {"unavailable": "triton is not importable for the reference's kernels"}
+    from jaxley_pytorch.synapses import KineticSynapse
+
+    from jaxley_pytorch_b200 import synth
+    from jaxley_pytorch_b200.kernels import synapse_step as ss
+    from jaxley_pytorch_b200.kernels import tree_solve as ts
+    from jaxley_pytorch_b200.lower import lower
+
+    peak = measured_peak_hbm()[0]
+    gen = torch.Generator(device=device).manual_seed(3)
+    out = {"tree_solve": [], "synapse_step": []}
+
+    def systems(parent, B):
+        n = len(parent)
+        par = torch.as_tensor(parent, device=device)
+        l = -0.05 - 0.35 * torch.rand(B, n, generator=gen, device=device)
+        u = -0.05 - 0.35 * torch.rand(B, n, generator=gen, device=device)
+        root = par < 0
+        l[:, root] = 0
+        u[:, root] = 0
+        d = 1.5 + torch.rand(B, n, generator=gen, device=device) + l.abs()
+        d.index_add_(1, par.clamp_min(0)[~root], u[:, ~root].abs())
+        s = torch.randn(B, n, generator=gen, device=device)
+        return d, l, u, s
+
+    c2 = lower(synth.config_l5pc_tree(batch=1, n_steps=1, seed=0))
+    rng = np.random.default_rng(5)
+    small = []
+    for _ in range(512):
+        b = len(small)
+        small += [-1] + [b + int(rng.integers(0, j)) for j in range(1, 40)]
+    for name, parent, B in (("l5pc_tree_300x4", np.asarray(c2.parent), 256),
+                            ("forest_512x40", np.asarray(small), 32)):
+        d, l, u, s = systems(parent, B)
+        n = len(parent)
+        for mode in ("registers", "levels"):
+            rk = rts.make_tree_solve_kernel(parent, device, mode=mode)
+            ok = ts.make_tree_solve_kernel(parent, device, mode=mode)
+            if rk is None or ok is None:
+                continue
+            err = float(((ok.solve(d, l, u, s) - rk.solve(d, l, u, s)).abs().max()
+                         / rk.solve(d, l, u, s).abs().max()).item())
+            t_ref = _device_us(lambda: rk.solve(d, l, u, s), reps)
+            t_ours = _device_us(lambda: ok.solve(d, l, u, s), reps)
+            nbytes = 5 * n * B * 4
+            out["tree_solve"].append({
+                "shape": f"{name}_b{B}", "nodes": n, "rows": B, "variant": mode,
+                "us_reference_triton": t_ref, "us_ours": t_ours, "speedup": t_ref / t_ours,
+                "fraction_of_hbm_ours": nbytes / (t_ours * 1e-6) / 1e9 / peak,
+                "max_rel_diff": err})
+
+    syn = KineticSynapse()
+    names = list(syn.synapse_params)
+    B, k = 32, 100
+    for T in (1024, 2048):
+        E = T * k
+        n = T
+        pre = np.concatenate([rng.choice(np.delete(np.arange(n), t), size=k, replace=False) for t in range(T)])
+        targets = np.arange(T)
+        v = -70.0 + 20.0 * torch.rand(B, n, generator=gen, device=device)
+        st = torch.rand(B, E, generator=gen, device=device)
+        params = []
+        for q, nm in enumerate(names):
+            base = float(syn.synapse_params[nm])
+            p = torch.full((E,), base, device=device)
+            if q == 0:
+                p = p * (0.5 + torch.rand(E, generator=gen, device=device))
+            params.append(p)
+        params += [params[0]] * (6 - len(params))
+        area = torch.full((E,), 100.0, device=device)
+        g_sn = torch.randn(B, E, generator=gen, device=device)
+        g_lin = torch.randn(B, T, generator=gen, device=device)
+        g_const = torch.randn(B, T, generator=gen, device=device)
+        none = v.new_empty(0)
+        row = {"shape": f"kinetic_{T}x{k}_b{B}", "synapses": E, "rows": B}
+        for tag, mod in (("reference_triton", rss), ("ours", ss)):
+            plan = mod.kernel_plan(syn, pre, targets, n, device)
+            if tag == "ours":
+                ss._ensure_ops()
+            sc = mod.kernel_scalars(0.025, 1e-3, torch.float32, device)
+            fargs = (v, st, plan["kernel_pre"], plan["kernel_targets"], *params, area, sc, plan["kernel_inv"],
+                     plan["kernel_pre_nodes"], k, rss.KINETIC, True, False)
+            bargs = (v, st, plan["kernel_pre"], plan["kernel_targets"], *params, area, sc, plan["kernel_inv"],
+                     plan["kernel_pre_nodes"], g_sn, none, g_lin, g_const, k, rss.KINETIC, True, True, False, 1)
+            row[f"us_forward_{tag}"] = _device_us(lambda: mod.synapse_step_op(*fargs), reps)
+            row[f"us_backward_{tag}"] = _device_us(lambda: mod.synapse_step_backward_op(*bargs), reps)
+            row[f"outputs_{tag}"] = (mod.synapse_step_op(*fargs), mod.synapse_step_backward_op(*bargs))
+        fo, bo = row.pop("outputs_ours")
+        fr, br = row.pop("outputs_reference_triton")
+        row["max_rel_diff"] = max(float(((a - b).abs().max() / b.abs().max().clamp_min(1e-30)).item())
+                                  for a, b in zip((fo[0], fo[2], fo[3], bo[0], bo[1], bo[2]),
+                                                  (fr[0], fr[2], fr[3], br[0], br[1], br[2])))
+        row["speedup_forward"] = row["us_forward_reference_triton"] / row["us_forward_ours"]
+        row["speedup_backward"] = row["us_backward_reference_triton"] / row["us_backward_ours"]
+        out["synapse_step"].append(row)
+    out["note"] = ("device time per call, mean of %d calls after one, float32, same inputs for both; "
+                   "operands resident in L2 between calls" % reps)
+    return out
+
+
 def cpu_sample(batch: int, tsteps: int, reps: int = 1):
     """Times the torch CPU restatement of the reference path (forward + autograd
     backward) on `batch` rows x `tsteps` steps of the workload."""
@@ -870,6 +1009,9 @@ def main():
         return res
 
     out = section("main iteration", lambda: run_ours(args, rank, world, device))
+    if world == 1 and not args.no_kernel_compare:
+        out["dropin_vs_triton"] = section("drop-in ops vs the reference's Triton kernels",
+                                          lambda: run_kernel_compare(device))
     if world == 1 and not args.no_uneven:
         out["uneven"] = section("uneven batch", lambda: run_uneven(args, device))
     if world == 1 and not args.no_serving:

@@ -19,8 +19,9 @@ same process) as `jaxley_pytorch_b200::tree_solve[_levels]`.
 from __future__ import annotations
 
 import ctypes as C
-import math
 import os
+import weakref
+from collections import OrderedDict
 from typing import Dict, Optional
 
 import numpy as np
@@ -272,7 +273,14 @@ def make_tree_solve_kernel(parent: np.ndarray, device, mode: Optional[str] = Non
 # ----------------------------------------------------------------------------------
 # Custom ops (registered on first use; the registry maps schedule tensors to kernels)
 # ----------------------------------------------------------------------------------
-_KERNELS: Dict[int, object] = {}
+# Kernels whose `fused` was called, by the address of their block_info tensor; held
+# weakly, so that an entry goes with its kernel (the solver that built it).
+_KERNELS: "weakref.WeakValueDictionary[int, object]" = weakref.WeakValueDictionary()
+# Kernels built for schedule tensors that reached an op without their kernel object
+# (a caller that calls the op with tensors of its own): the last few, by the addresses
+# of block_info and parent_safe and the node count.
+_ADOPTED: "OrderedDict[tuple, object]" = OrderedDict()
+_ADOPTED_MAX = 8
 _NS = None
 tree_solve_op = None
 tree_solve_levels_op = None
@@ -284,10 +292,23 @@ def _register(kernel) -> None:
         _define_ops()
 
 
-def _kernel_for(block_info: torch.Tensor):
+def _kernel_for(block_info: torch.Tensor, parent_safe: torch.Tensor, has_parent: torch.Tensor,
+                mode: str):
+    """The kernel of an op call: the one whose schedule tensors these are, else one
+    built from the tree the op's `parent_safe` / `has_parent` describe."""
     k = _KERNELS.get(block_info.data_ptr())
+    if k is not None and k.parent_safe.data_ptr() == parent_safe.data_ptr():
+        return k
+    key = (block_info.data_ptr(), parent_safe.data_ptr(), int(parent_safe.shape[-1]), mode)
+    k = _ADOPTED.get(key)
     if k is None:
-        raise RuntimeError("tree_solve: unknown schedule (build it with make_tree_solve_kernel)")
+        parent = np.where(has_parent.cpu().numpy(), parent_safe.cpu().numpy(), -1)
+        k = make_tree_solve_kernel(parent, parent_safe.device, mode=mode)
+        _ADOPTED[key] = k
+        while len(_ADOPTED) > _ADOPTED_MAX:
+            _ADOPTED.popitem(last=False)
+    else:
+        _ADOPTED.move_to_end(key)
     return k
 
 
@@ -322,7 +343,7 @@ def _define_in(ns: str):
                     parent_safe: torch.Tensor, has_parent: torch.Tensor, block_size: int,
                     num_slots: int, num_warps: int) -> torch.Tensor:
         """Registers-variant tree solve (reference `tree_solve.py:518-563`)."""
-        return _kernel_for(block_info).solve(diags, lowers, uppers, solves)
+        return _kernel_for(block_info, parent_safe, has_parent, "registers").solve(diags, lowers, uppers, solves)
 
     @_tree_solve.register_fake
     def _(diags, lowers, uppers, solves, *args):
@@ -346,7 +367,7 @@ def _define_in(ns: str):
                            parent_safe: torch.Tensor, has_parent: torch.Tensor, num_slots: int,
                            w: int) -> torch.Tensor:
         """Levels-variant tree solve (reference `tree_solve.py:589-609`)."""
-        return _kernel_for(block_info).solve(diags, lowers, uppers, solves)
+        return _kernel_for(block_info, parent_safe, has_parent, "levels").solve(diags, lowers, uppers, solves)
 
     @_tree_solve_levels.register_fake
     def _(diags, lowers, uppers, solves, *args):

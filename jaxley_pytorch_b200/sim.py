@@ -657,14 +657,15 @@ class _IntegrateFn(torch.autograd.Function):
             stash.saved = (False, ps, ckpt)
         if sim.check_finite:
             sim.model.check_finite("simulation")
-        return rec.permute(1, 2, 0)
+        # Contiguous, so that a forward-mode tangent can have the output's layout.
+        return rec.permute(1, 2, 0).contiguous()
 
     @staticmethod
     def setup_context(ctx, inputs, output):
         pscale, sim, T, stash = inputs
         ctx.sim, ctx.T = sim, T
         ctx.in_dtype = pscale.dtype
-        ctx.saved, stash.saved = stash.saved, None
+        ctx.saved = stash.saved  # (functorch may call this more than once per forward)
 
     @staticmethod
     def backward(ctx, grad_out):
@@ -689,5 +690,5 @@ class _IntegrateFn(torch.autograd.Function):
         sim = ctx.sim
         with host_mode():
             _, rec_t = sim.jvp(ctx.saved[1], unwrap(t_pscale).detach(), ctx.T)
-            rec_t = rec_t.to(ctx.in_dtype)
+            rec_t = rec_t.to(ctx.in_dtype).contiguous()
         return rec_t

@@ -49,9 +49,10 @@ def test_tangent_matches_reference_jvp(cuda_device, name):
     assert _rel(rec.cpu().numpy(), ref) <= 1e-9
     err = _rel(tan.cpu().numpy(), extra["jvp"].reshape(tan.shape))
     assert err <= 1e-7, err
-    # The values of the dual launch are the plain forward's.
+    # The values of the dual launch are the plain forward's (to round-off: the dual
+    # arithmetic contracts some products differently).
     plain = sim.run(pscale=sim.model.pscale)
-    assert torch.equal(plain, rec)
+    assert _rel(rec.cpu(), plain.cpu()) <= 1e-12
 
 
 @pytest.mark.parametrize("name", ["hh_clamp_7x3", "cn_hh_7x3"])
@@ -80,7 +81,7 @@ def test_tangent_linear_and_adjoint_consistent(cuda_device):
     _, t1 = sim.jvp(sim.model.pscale, q1)
     _, t2 = sim.jvp(sim.model.pscale, q2)
     _, t12 = sim.jvp(sim.model.pscale, 2.0 * q1 - 0.5 * q2)
-    assert _rel((t12 - (2.0 * t1 - 0.5 * t2)).cpu(), t12.cpu()) <= 1e-6
+    assert _rel((2.0 * t1 - 0.5 * t2).cpu(), t12.cpu()) <= 1e-6
     ps = sim.model.pscale.clone().requires_grad_(True)
     rec = sim.run(pscale=ps)
     w = torch.randn(rec.shape, generator=gen, dtype=torch.float64).to(cuda_device)

@@ -129,3 +129,41 @@ def test_env_var_selects_variant(cuda_device, monkeypatch):
     monkeypatch.setenv("JAXLEY_PYTORCH_TREE_KERNEL", "auto")
     deep = np.asarray(forests()["deep_600"])
     assert isinstance(ts.make_tree_solve_kernel(deep, cuda_device), ts.LevelTreeSolveKernel)
+
+
+def test_op_registry_holds_kernels_weakly():
+    """A kernel registered by `fused` leaves the op registry with its last owner."""
+    import gc
+
+    parent = np.asarray(forests()["random_40"])
+    kern = ts.TreeSolveKernel(ts.build_forest_schedule(parent), "cpu")
+    ts._register(kern)
+    key = kern.t["block_info"].data_ptr()
+    assert ts._KERNELS.get(key) is kern
+    del kern
+    gc.collect()
+    assert key not in ts._KERNELS
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("mode", ["registers", "levels"])
+def test_op_with_callers_schedule_tensors(cuda_device, mode):
+    """The custom op called with schedule tensors of the caller's own (no kernel object
+    registered for them) solves the tree its parent_safe / has_parent describe."""
+    parent = np.asarray(forests()["forest_mixed"])
+    kern = ts.make_tree_solve_kernel(parent, cuda_device, mode=mode)
+    d, l, u, s = (torch.as_tensor(a, device=cuda_device) for a in system(parent, 3, np.float64, seed=7))
+    ref = kern.solve(d, l, u, s)
+    ts._register(kern)
+    # Copies of every schedule tensor: addresses the registry has never seen.
+    if mode == "registers":
+        t = {k: v.clone() for k, v in kern.t.items()}
+        x = ts.tree_solve_op(d, l, u, s, t["block_info"], t["rel_parent"], t["rel_height"],
+                             t["rel_children"], kern.parent_safe.clone(), kern.has_parent.clone(),
+                             kern.block_size, kern.num_slots, kern.num_warps)
+    else:
+        t = {k: v.clone() for k, v in kern.t.items()}
+        x = ts.tree_solve_levels_op(d, l, u, s, t["block_info"], t["level_ptr"], t["perm"],
+                                    t["chain_ptop"], t["chain_child"], kern.parent_safe.clone(),
+                                    kern.has_parent.clone(), kern.num_slots, 0)
+    torch.testing.assert_close(x, ref, rtol=1e-12, atol=1e-12)
