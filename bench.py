@@ -85,6 +85,9 @@ def parse():
                     help="skip the float32-against-float64 error of the sampled configurations")
     ap.add_argument("--no-kernel-compare", action="store_true",
                     help="skip the standalone drop-in ops against the reference's Triton kernels")
+    ap.add_argument("--kernel-compare-only", action="store_true",
+                    help="print only the drop-in comparison as JSON (run as a child of the bench)")
+    ap.add_argument("--local-device", type=int, default=0, help=argparse.SUPPRESS)
     ap.add_argument("--serve-requests", type=int, default=240)
     ap.add_argument("--serve-capacity-requests", type=int, default=160)
     return ap.parse_args()
@@ -924,6 +927,22 @@ def run_kernel_compare(device, reps: int = 200):
     return out
 
 
+def kernel_compare_child(local: int, timeout_s: int = 600):
+    """`run_kernel_compare` in a child process (the reference's Triton kernels are
+    compiled and run there), so that a failure of that path leaves the rest of the
+    line intact; its stderr tail is kept when it fails."""
+    cmd = [sys.executable, "-X", "faulthandler", os.path.abspath(__file__), "--kernel-compare-only",
+           "--local-device", str(local)]
+    try:
+        r = subprocess.run(cmd, capture_output=True, text=True, timeout=timeout_s)
+    except subprocess.TimeoutExpired:
+        return {"unavailable": f"the comparison did not finish within {timeout_s} s"}
+    if r.returncode == 0 and r.stdout.strip():
+        return json.loads(r.stdout.strip().splitlines()[-1])
+    return {"unavailable": f"the comparison process ended with status {r.returncode}",
+            "stderr_tail": r.stderr[-1500:]}
+
+
 def cpu_sample(batch: int, tsteps: int, reps: int = 1):
     """Times the torch CPU restatement of the reference path (forward + autograd
     backward) on `batch` rows x `tsteps` steps of the workload."""
@@ -955,6 +974,11 @@ def cpu_sample(batch: int, tsteps: int, reps: int = 1):
 
 def main():
     args = parse()
+    if args.kernel_compare_only:
+        import torch
+
+        print(json.dumps(run_kernel_compare(torch.device("cuda", args.local_device))))
+        return 0
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
@@ -1009,9 +1033,6 @@ def main():
         return res
 
     out = section("main iteration", lambda: run_ours(args, rank, world, device))
-    if world == 1 and not args.no_kernel_compare:
-        out["dropin_vs_triton"] = section("drop-in ops vs the reference's Triton kernels",
-                                          lambda: run_kernel_compare(device))
     if world == 1 and not args.no_uneven:
         out["uneven"] = section("uneven batch", lambda: run_uneven(args, device))
     if world == 1 and not args.no_serving:
@@ -1022,6 +1043,9 @@ def main():
         out["lm_network"] = section("lm networks", lambda: [run_lm(args, device, n) for n in (1024, 2048)])
     if world == 1 and not args.no_fp32_error:
         out["fp32_error"] = section("fp32 errors", lambda: fp32_errors(device))
+    if world == 1 and not args.no_kernel_compare:
+        out["dropin_vs_triton"] = section("drop-in ops vs the reference's Triton kernels",
+                                          lambda: kernel_compare_child(local))
     if rank == 0:
         if world == 1 and not args.no_cpu_baseline:
             ref = section("cpu baseline", lambda: reference_baseline(args.cpu_batch, args.cpu_tsteps))

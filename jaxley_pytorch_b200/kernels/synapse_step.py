@@ -23,6 +23,7 @@ import torch
 
 from .. import _lib
 from ..lower import presynaptic_lists
+from . import op_namespace
 
 KINETIC, SIGMOID_RATE = 0, 1
 _NAMES = {
@@ -250,13 +251,7 @@ def _define_in(ns: str):
 def _ensure_ops():
     if synapse_step_op is not None:
         return
-    for ns in ("jaxley_pytorch", "jaxley_pytorch_b200"):
-        try:
-            _define_in(ns)
-            return
-        except RuntimeError:
-            continue
-    raise RuntimeError("could not register the synapse ops")
+    _define_in(op_namespace(("synapse_step", "synapse_step_backward")))
 
 
 def _scatter_to_nodes(per_target: torch.Tensor, targets: torch.Tensor, n: int) -> torch.Tensor:

@@ -29,6 +29,7 @@ import torch
 
 from .. import _lib
 from ..lower import block_schedule, chain_table
+from . import op_namespace
 
 MAX_BLOCK = 8192  # registers variant: up to 256 nodes in one warp, larger blocks in a CTA
 LEVEL_BLOCK = 4096  # levels variant: nodes per block of trees (shared memory bound)
@@ -322,15 +323,10 @@ def _transposed_backward(kernel_op, ctx, grad_x, args_after):
 
 
 def _define_ops():
-    global _NS, tree_solve_op, tree_solve_levels_op
-    for ns in ("jaxley_pytorch", "jaxley_pytorch_b200"):
-        try:
-            _define_in(ns)
-            _NS = ns
-            return
-        except RuntimeError:
-            continue
-    raise RuntimeError("could not register the tree-solve ops")
+    global _NS
+    ns = op_namespace(("tree_solve", "tree_solve_levels"))
+    _define_in(ns)
+    _NS = ns
 
 
 def _define_in(ns: str):
