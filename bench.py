@@ -426,9 +426,15 @@ def run_uneven(args, device):
         rec = plain.run(n_steps=Tp, pscale=ps)
         torch.autograd.grad(((rec - tp) ** 2).mean(), ps)
 
-    ms_plain = timed(plain_step, 2)
+    ms_plain_eager = timed(plain_step, 1)
+    # The same per-step launches captured as one CUDA graph (no host work per launch).
+    git = GraphedIteration(plain, loss_of(tp), ps0.clone().requires_grad_(True), n_steps=Tp, warmup=1)
+    ms_plain = timed(git.replay, 2)
+    plain_launches = git.launches_per_replay
+    del git
     rate = n_comp * T / (ms / 1e3)
     rate_plain = n_comp * Tp / (ms_plain / 1e3)
+    rate_plain_eager = n_comp * Tp / (ms_plain_eager / 1e3)
     del plain
     torch.cuda.empty_cache()
     # Per size group: one eager iteration of the persistent form with an event pair
@@ -461,8 +467,12 @@ def run_uneven(args, device):
                        "adjoint": "stored trajectory (%d MB)" % (sim.trajectory_bytes(T) // 2**20) if stored
                        else "recompute from checkpoints"},
         "per_step": {"value": rate_plain, "unit": UNIT, "ms_per_iteration": ms_plain, "time_steps": Tp,
-                     "checkpoint": 1},
+                     "checkpoint": 1, "graph_launches": plain_launches,
+                     "form": "one forward launch per step and one adjoint launch per step, replayed as one "
+                             "CUDA graph",
+                     "eager": {"value": rate_plain_eager, "ms_per_iteration": ms_plain_eager}},
         "persistent_over_per_step": rate / rate_plain,
+        "persistent_over_per_step_eager": rate / rate_plain_eager,
         "per_group": per_group,
         "tuning": table,
     }
@@ -790,23 +800,37 @@ def run_lm(args, device, n_cells: int):
             "value": n_cells * 32 * T / (ms / 1e3), "unit": UNIT, "loss": float(it.loss)}
 
 
-def _device_us(fn, reps: int) -> float:
-    """Mean device time of `fn` in microseconds (CUDA events on the current stream,
-    after one untimed call)."""
+def _device_us(fn, reps: int, calls: int = 20) -> float:
+    """Device time of one call of `fn` in microseconds: `calls` calls captured in a
+    CUDA graph (so that host-side dispatch does not pace the GPU), replayed `reps`
+    times between CUDA events, after warm-up calls on a side stream."""
     import torch
 
-    fn()
+    side = torch.cuda.Stream()
+    side.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(side):
+        for _ in range(3):
+            fn()
+    torch.cuda.current_stream().wait_stream(side)
+    torch.cuda.synchronize()
+    graph = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(graph):
+        for _ in range(calls):
+            fn()
+    graph.replay()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record()
     for _ in range(reps):
-        fn()
+        graph.replay()
     e1.record()
     torch.cuda.synchronize()
-    return e0.elapsed_time(e1) * 1e3 / reps
+    us = e0.elapsed_time(e1) * 1e3 / (reps * calls)
+    del graph
+    return us
 
 
-def run_kernel_compare(device, reps: int = 200):
+def run_kernel_compare(device, reps: int = 20):
     """The standalone drop-in ops against the reference's Triton kernels, both on this
     GPU with the same inputs: the tree solve (`kernels/tree_solve.py`, registers and
     levels variants) on the 300 x 4 L5PC tree with 256 rows and on a forest of 512
@@ -916,14 +940,16 @@ def run_kernel_compare(device, reps: int = 200):
             row[f"outputs_{tag}"] = (mod.synapse_step_op(*fargs), mod.synapse_step_backward_op(*bargs))
         fo, bo = row.pop("outputs_ours")
         fr, br = row.pop("outputs_reference_triton")
-        row["max_rel_diff"] = max(float(((a - b).abs().max() / b.abs().max().clamp_min(1e-30)).item())
-                                  for a, b in zip((fo[0], fo[2], fo[3], bo[0], bo[1], bo[2]),
-                                                  (fr[0], fr[2], fr[3], br[0], br[1], br[2])))
+        names = ("s_new", "lin", "const", "g_v", "g_s", "g_gS")
+        row["max_rel_diff"] = {
+            nm: float(((a - b).abs().max() / b.abs().max().clamp_min(1e-30)).item())
+            for nm, a, b in zip(names, (fo[0], fo[2], fo[3], bo[0], bo[1], bo[2]),
+                                (fr[0], fr[2], fr[3], br[0], br[1], br[2]))}
         row["speedup_forward"] = row["us_forward_reference_triton"] / row["us_forward_ours"]
         row["speedup_backward"] = row["us_backward_reference_triton"] / row["us_backward_ours"]
         out["synapse_step"].append(row)
-    out["note"] = ("device time per call, mean of %d calls after one, float32, same inputs for both; "
-                   "operands resident in L2 between calls" % reps)
+    out["note"] = ("device time per call: 20 calls captured in a CUDA graph, replayed %d times; float32, "
+                   "same inputs for both; operands resident in L2 between calls" % reps)
     return out
 
 

@@ -658,9 +658,9 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
     if group_uses:
         tgs = np.concatenate([t for t, _ in group_uses])
         cls_ = new_of[np.concatenate([c for _, c in group_uses])]
-        for gi in np.unique(tgs):
-            cs = np.unique(cls_[tgs == gi])
-            train_cols[gi] = cs[0] if len(cs) == 1 else -2
+        pairs = np.unique(np.stack([tgs, cls_], 1), axis=0)  # sorted by group, then column
+        gids, first, counts = np.unique(pairs[:, 0], return_index=True, return_counts=True)
+        train_cols[gids] = np.where(counts == 1, pairs[first, 1], -2)
 
     # ---- initial state ----
     L = int(soff[-1])
