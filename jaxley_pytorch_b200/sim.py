@@ -91,7 +91,7 @@ class DeviceModel:
                  rows_per_item: int = 1, threads: int = 256, programs: bool = True,
                  smem_limit: Optional[int] = None, schedule: bool = True,
                  forward_threads: Optional[int] = None, forward_wide: bool = False,
-                 tangent: bool = False):
+                 tangent: bool = False, gm_threads: Optional[int] = None):
         self.low = low
         self.dtype = dtype
         self.device = torch.device(device)
@@ -159,18 +159,31 @@ class DeviceModel:
         if tangent:
             self.kind_threads["forward"] = min(self.kind_threads["forward"], 512)
         self.forward_wide = bool(forward_wide) and not tangent
+        # Threads per CTA of the groups whose work areas live in global memory (blocks
+        # too large for shared memory; they run one CTA per SM at most, so they can
+        # use more threads than the shared-memory groups).
+        self.gm_threads = int(gm_threads) if gm_threads else None
+        if tangent and self.gm_threads:
+            self.gm_threads = min(self.gm_threads, 512)
         self.sched_warps = 0
         self.kind_sched: Dict[str, tuple] = {}
+        self.gm_sched: Optional[tuple] = None
         if schedule:
             by_warps: Dict[int, tuple] = {}
-            for kind, th in self.kind_threads.items():
-                if th % 32:
-                    continue
+
+            def sched_for(th):
                 w = th // 32
                 if w not in by_warps:
                     sp, sc = node_schedule(low, w)
                     by_warps[w] = (w, i(sp), torch.as_tensor(sc, device=dev).contiguous())
-                self.kind_sched[kind] = by_warps[w]
+                return by_warps[w]
+
+            for kind, th in self.kind_threads.items():
+                if th % 32:
+                    continue
+                self.kind_sched[kind] = sched_for(th)
+            if self.gm_threads and self.gm_threads % 32 == 0:
+                self.gm_sched = sched_for(self.gm_threads)
             if "backward" in self.kind_sched:
                 w, sp_t, sc_t = self.kind_sched["backward"]
                 self.t["sched_ptr"], self.t["sched"], self.sched_warps = sp_t, sc_t, w
@@ -331,6 +344,8 @@ class DeviceModel:
             a.threads = self.kind_threads[kind]
             a.wide = int(kind == "forward" and self.forward_wide)
             ks = self.kind_sched.get(kind)
+            if group["gm"] and self.gm_threads:
+                a.threads, a.wide, ks = self.gm_threads, 0, self.gm_sched
             if ks is not None:
                 a.sched_warps, a.sched_ptr, a.sched = ks[0], ks[1].data_ptr(), ks[2].data_ptr()
         a.items = group["items"].data_ptr()
@@ -431,9 +446,10 @@ class Simulation:
     `store_fraction` of the free device memory). `threads` is the CTA size of the
     launches; `forward_threads` (default: `threads`) that of the forward launches,
     which with `forward_wide` (float32, up to 256 threads) use kernels of two CTAs per
-    SM with up to 128 registers a thread instead of 64. With `check_finite`, a run
-    whose final states or gradients hold a NaN or an infinity raises
-    `FloatingPointError` (the kernels flag it on the device).
+    SM with up to 128 registers a thread instead of 64. `gm_threads` (default: as the
+    kind's) is the CTA size of the launches of blocks whose work areas live in global
+    memory. With `check_finite`, a run whose final states or gradients hold a NaN or
+    an infinity raises `FloatingPointError` (the kernels flag it on the device).
     """
 
     def __init__(self, problem: Problem, dtype=torch.float32, device="cuda",
@@ -443,13 +459,14 @@ class Simulation:
                  keep_currents: bool = True, programs: bool = True, schedule: bool = True,
                  store_trajectory="auto", store_fraction: float = 0.5,
                  forward_threads: Optional[int] = None, forward_wide: bool = False,
-                 check_finite: bool = True):
+                 check_finite: bool = True, gm_threads: Optional[int] = None):
         self.problem = problem
         self.low = low if low is not None else lower(problem, max_block_nodes=max_block_nodes,
                                                      keep_currents=keep_currents)
         self.model = DeviceModel(self.low, dtype, device, rows_per_item, threads=threads,
                                  programs=programs, schedule=schedule,
-                                 forward_threads=forward_threads, forward_wide=forward_wide)
+                                 forward_threads=forward_threads, forward_wide=forward_wide,
+                                 gm_threads=gm_threads)
         self.segment = segment
         self.init_steady = init_steady
         self.checkpoint = int(checkpoint)
@@ -560,7 +577,7 @@ class Simulation:
         if getattr(self, "_tangent", None) is None:
             m = self.model
             self._tangent = DeviceModel(self.low, m.dtype, m.device, m.rows_per_item, threads=m.threads,
-                                        schedule=bool(m.kind_sched), tangent=True)
+                                        schedule=bool(m.kind_sched), tangent=True, gm_threads=m.gm_threads)
         return self._tangent
 
     def jvp(self, pscale: torch.Tensor, pscale_tangent: torch.Tensor, n_steps: Optional[int] = None,
