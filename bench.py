@@ -955,6 +955,22 @@ def run_kernel_compare(device, reps: int = 20):
             nm: float(((a - b).abs().max() / b.abs().max().clamp_min(1e-30)).item())
             for nm, a, b in zip(outs, (fo[0], fo[2], fo[3], bo[0], bo[1], bo[2]),
                                 (fr[0], fr[2], fr[3], br[0], br[1], br[2]))}
+        # The same calls in float64: the float32 differences in g_s and g_gS are the
+        # cancellation in the adjoint of the finite-difference slope (1e-3 mV), which
+        # both implementations evaluate in their own order.
+        d64 = []
+        for mod in (ss, rss):
+            plan = mod.kernel_plan(syn, pre, targets, n, device)
+            sc = mod.kernel_scalars(0.025, 1e-3, torch.float64, device)
+            dd = lambda x: x.double()  # noqa: E731
+            fa = (dd(v), dd(st), plan["kernel_pre"], plan["kernel_targets"], *[dd(p) for p in params], dd(area), sc,
+                  plan["kernel_inv"], plan["kernel_pre_nodes"], k, rss.KINETIC, True, False)
+            ba = fa[:14] + (dd(g_sn), none.double(), dd(g_lin), dd(g_const), k, rss.KINETIC, True, True, False, 1)
+            fo64, bo64 = mod.synapse_step_op(*fa), mod.synapse_step_backward_op(*ba)
+            d64.append((fo64[0], fo64[2], fo64[3], bo64[0], bo64[1], bo64[2]))
+        row["max_rel_diff_f64"] = {
+            nm: float(((a - b).abs().max() / b.abs().max().clamp_min(1e-300)).item())
+            for nm, a, b in zip(outs, d64[0], d64[1])}
         row["speedup_forward"] = row["us_forward_reference_triton"] / row["us_forward_ours"]
         row["speedup_backward"] = row["us_backward_reference_triton"] / row["us_backward_ours"]
         out["synapse_step"].append(row)

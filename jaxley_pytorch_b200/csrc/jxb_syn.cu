@@ -2,19 +2,24 @@
 // layout: E = T * k synapses ordered by postsynaptic target, k per target
 // (jaxley-pytorch kernels/synapse_step.py, modules/network.py:381-478).
 //
-// Both passes run one CTA per target with one thread per synapse of the target
-// (warps over chunks of 32 synapses, up to 1024 synapses per target). A thread keeps
-// its synapse's parameters, area and presynaptic index in registers and walks the
-// batch rows in blocks of kRowBlock rows, whose loads (state, presynaptic and target
-// voltages) are independent and issued together. Sums over a target's synapses (the
-// slope and offset of the forward, the target-voltage gradient of the backward) are
-// warp reductions followed by a fixed-order sum over the CTA's warps in shared
-// memory. The backward's parameter gradients are summed over the rows in the
-// synapse's own thread (no cross-CTA reduction); its presynaptic voltage gradients
-// go to an (E, batch) buffer, kRowBlock consecutive rows per thread, which a second
-// kernel sums per presynaptic node through the transposed index. No atomics,
-// deterministic. float: fast reciprocal / division / exp (jxb_math.cuh); float64
-// stays exact.
+// Lane groups: L lanes (a power of two, about 16 synapses each) serve one
+// (row, target) pair; lane c takes the target's synapses c, c + L, c + 2L, ..., so
+// that the 32 / L groups of a warp read L consecutive values of each state and
+// parameter array per instruction (whole 32-byte sectors at L = 8), sum their
+// synapses in registers and combine them with log2(L) shuffles. No shared-memory
+// reductions and no block barriers in the forward.
+//
+// forward:  warps over batch rows (4 per CTA, the same targets, so that the
+//           parameters are reused from L1), 32 / L targets per warp.
+// backward: one CTA per group of 32 / L targets with 8 warps over the batch rows
+//           (each warp up to kRowsPerWarp rows per pass). Per synapse chunk (one
+//           value of i in c + i L) the parameter gradients are summed over the
+//           warp's rows in registers and over the warps in shared memory in a fixed
+//           order, and the presynaptic voltage gradients of the chunk are staged in
+//           shared memory and written to an (E, batch) buffer row-contiguously; a
+//           second kernel sums them per presynaptic node through the transposed
+//           index. No atomics, deterministic.
+// float: fast reciprocal / division / exp (jxb_math.cuh); float64 stays exact.
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
@@ -46,209 +51,265 @@ struct SynP {
   const T* p[6];
 };
 
-constexpr int kRowBlock = 8;  // batch rows per register block
-constexpr int kMaxWarps = 32;  // up to 1024 synapses per target
-
-// Sums over the CTA's synapses of NV values per row of a block (lane sums, then the
-// warps in a fixed order); thread r (r < nr) receives the sums of row r in out[].
-// `red` holds NV x kMaxWarps x kRowBlock values.
-template <typename T, int NV>
-__device__ __forceinline__ void block_row_sums(T (&v)[NV][kRowBlock], int nr, T* red, T (&out)[NV]) {
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-#pragma unroll
-  for (int i = 0; i < NV; ++i)
-#pragma unroll
-    for (int r = 0; r < kRowBlock; ++r) v[i][r] = warp_sum(v[i][r]);
-  if (lane == 0) {
-#pragma unroll
-    for (int i = 0; i < NV; ++i)
-#pragma unroll
-      for (int r = 0; r < kRowBlock; ++r) red[(i * kMaxWarps + warp) * kRowBlock + r] = v[i][r];
-  }
-  __syncthreads();
-#pragma unroll
-  for (int i = 0; i < NV; ++i) {
-    out[i] = T(0);
-    if ((int)threadIdx.x < nr)
-      for (int w = 0; w < nw; ++w) out[i] += red[(i * kMaxWarps + w) * kRowBlock + threadIdx.x];
-  }
-  __syncthreads();
-}
+// One synapse's constants: parameters in the reference order (Kinetic: gS, e_syn,
+// alpha, beta, v_th, delta; SigmoidRate: gS, x_offset, slope), the area of its
+// target compartment and its presynaptic node.
+template <typename T>
+struct SynC {
+  T gs, ar, q1, q2, q3, q4, q5;
+  int pre;
+};
 
 template <typename T>
-__global__ void __launch_bounds__(1024) syn_forward_kernel(JxbSynArgs a, SynP<T> P) {
-  __shared__ T red[2 * kMaxWarps * kRowBlock];
-  const int tgt = blockIdx.x;
-  const int kk = threadIdx.x;
-  const bool act = kk < a.k;
+__device__ __forceinline__ SynC<T> load_syn(const JxbSynArgs& a, const SynP<T>& P, int64_t e) {
+  SynC<T> c;
+  c.pre = a.pre[e];
+  c.gs = P.p[0][e];
+  c.ar = ((const T*)a.area)[e];
+  c.q1 = P.p[1][e];
+  c.q2 = P.p[2][e];
+  c.q3 = a.model == 0 ? P.p[3][e] : T(0);
+  c.q4 = a.model == 0 ? P.p[4][e] : T(0);
+  c.q5 = a.model == 0 ? P.p[5][e] : T(1);
+  return c;
+}
+
+// Forward of one synapse and row (synapses/kinetic.py:37-63, sigmoid_rate.py:43-50,
+// the slope and offset of kernels/synapse_step.py:150-180): the new kinetic state,
+// the current i0 at vp and the slope vt / offset d0 - vt vp in uA/cm^2.
+template <typename T>
+__device__ __forceinline__ void syn_forward_one(int model, const SynC<T>& c, T s, T vpre, T vp, T dt, T diff,
+                                                T& s_new, T& i0, T& vt, T& d0) {
+  T i1;
+  if (model == 0) {
+    const T tr = sigm(qdiv<T>(vpre - c.q4, c.q5));
+    const T aa = c.q2 * tr;
+    const T rate = aa + c.q3;
+    const T s_inf = qdiv<T>(aa, rate);
+    s_new = s_inf + (s - s_inf) * ex(-dt * rate);
+    i0 = c.gs * s_new * (vp - c.q1);
+    i1 = c.gs * s_new * ((vp + diff) - c.q1);
+  } else {
+    s_new = T(0);
+    i0 = -c.gs * sigm((vpre - c.q1) * c.q2);
+    i1 = -c.gs * sigm(((vpre + diff) - c.q1) * c.q2);
+  }
+  d0 = qdiv<T>(i0, c.ar) * T(100000.0);
+  const T d1 = qdiv<T>(i1, c.ar) * T(100000.0);
+  vt = qdiv<T>(d1 - d0, diff);
+}
+
+// Adjoint of one synapse and row (kernels/synapse_step.py:256-305) given the
+// gradients of the target's slope and offset (glin, gconst), of the new state and of
+// the current: adds the parameter gradients to gp[], returns the state gradient in
+// g_s, the target-voltage gradient in g_vp and the presynaptic one in g_vpre.
+template <typename T>
+__device__ __forceinline__ void syn_backward_one(int model, const SynC<T>& c, T s, T vpre, T vp, T dt, T diff,
+                                                 T glin, T gconst, T g_sn_in, T g_cur, T (&gp)[6], T& g_s,
+                                                 T& g_vp, T& g_vpre) {
+  T i0, i1, w0 = T(0), w1 = T(0), s_new = T(0), tr = T(0), rate = T(1), s_inf = T(0), decay = T(0),
+           x = T(0), u0 = T(0), u1 = T(0), sig0 = T(0), sig1 = T(0);
+  if (model == 0) {
+    x = qdiv<T>(vpre - c.q4, c.q5);
+    tr = sigm(x);
+    const T aa = c.q2 * tr;
+    rate = aa + c.q3;
+    s_inf = qdiv<T>(aa, rate);
+    decay = ex(-dt * rate);
+    s_new = s_inf + (s - s_inf) * decay;
+    w0 = vp - c.q1;
+    w1 = (vp + diff) - c.q1;
+    i0 = c.gs * s_new * w0;
+    i1 = c.gs * s_new * w1;
+  } else {
+    u0 = vpre - c.q1;
+    u1 = (vpre + diff) - c.q1;
+    sig0 = sigm(u0 * c.q2);
+    sig1 = sigm(u1 * c.q2);
+    i0 = -c.gs * sig0;
+    i1 = -c.gs * sig1;
+  }
+  const T d0 = qdiv<T>(i0, c.ar) * T(100000.0);
+  const T d1 = qdiv<T>(i1, c.ar) * T(100000.0);
+  const T vt = qdiv<T>(d1 - d0, diff);
+  const T g_vt = glin - gconst * vp;
+  g_vp = -gconst * vt;
+  const T g_d1 = qdiv<T>(g_vt, diff);
+  const T g_d0 = gconst - g_d1;
+  const T g_i0 = qdiv<T>(g_d0 * T(100000.0), c.ar) + g_cur;
+  const T g_i1 = qdiv<T>(g_d1 * T(100000.0), c.ar);
+  if (model == 0) {
+    const T g_w = g_i0 * w0 + g_i1 * w1;
+    const T g_sn = c.gs * g_w + g_sn_in;
+    g_vp += c.gs * s_new * (g_i0 + g_i1);
+    const T g_sinf = g_sn * (T(1) - decay);
+    const T g_rate = -dt * decay * g_sn * (s - s_inf) - qdiv<T>(g_sinf * s_inf, rate);
+    const T g_a = qdiv<T>(g_sinf, rate) + g_rate;
+    const T g_x = g_a * c.q2 * tr * (T(1) - tr);
+    g_vpre = qdiv<T>(g_x, c.q5);
+    g_s = g_sn * decay;
+    gp[0] += s_new * g_w;
+    gp[1] += -c.gs * s_new * (g_i0 + g_i1);
+    gp[2] += g_a * tr;
+    gp[3] += g_rate;
+    gp[4] += -g_vpre;
+    gp[5] += -g_vpre * x;
+  } else {
+    const T g_z0 = -c.gs * g_i0 * sig0 * (T(1) - sig0);
+    const T g_z1 = -c.gs * g_i1 * sig1 * (T(1) - sig1);
+    g_vpre = (g_z0 + g_z1) * c.q2;
+    g_s = T(0);
+    gp[0] += -(g_i0 * sig0 + g_i1 * sig1);
+    gp[1] += -g_vpre;
+    gp[2] += g_z0 * u0 + g_z1 * u1;
+  }
+}
+
+// Sum over the L lanes of a group (aligned groups of L consecutive lanes).
+template <int L, typename T>
+__device__ __forceinline__ T group_sum(T v) {
+#pragma unroll
+  for (int o = L / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+constexpr int kFwdWarps = 4;      // batch rows per forward CTA
+constexpr int kBwdWarps = 8;      // warps per backward CTA
+constexpr int kRowsPerWarp = 4;   // rows of a backward warp per pass
+
+template <typename T, int L>
+__global__ void __launch_bounds__(32 * kFwdWarps) syn_forward_kernel(JxbSynArgs a, SynP<T> P) {
+  constexpr int TPW = 32 / L;  // targets per warp
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = lane & (L - 1);
   const int nt = a.n_syn / a.k;
-  const int64_t e = (int64_t)tgt * a.k + (act ? kk : 0);
+  const int tgt = blockIdx.x * TPW + lane / L;
+  const int64_t b = (int64_t)blockIdx.y * kFwdWarps + warp;
+  const bool ok = tgt < nt && b < a.batch;
   const T* sc = (const T*)a.scalars;
   const T dt = sc[0], diff = sc[1];
-  const int node = a.targets_are_nodes ? tgt : a.targets[tgt];
-  const int pre = a.pre[e];
-  const T gs = P.p[0][e];
-  const T ar = ((const T*)a.area)[e];
-  const T q1 = P.p[1][e], q2 = P.p[2][e];
-  const T q3 = a.model == 0 ? P.p[3][e] : T(0), q4 = a.model == 0 ? P.p[4][e] : T(0),
-          q5 = a.model == 0 ? P.p[5][e] : T(1);
-  for (int b0 = 0; b0 < a.batch; b0 += kRowBlock) {
-    const int nr = min(kRowBlock, a.batch - b0);
-    T sums[2][kRowBlock];  // slope and offset of every row
-#pragma unroll
-    for (int r = 0; r < kRowBlock; ++r) {
-      sums[0][r] = sums[1][r] = T(0);
-      if (!act || r >= nr) continue;
-      const int64_t b = b0 + r;
-      const T* v = (const T*)a.v + b * a.n_nodes;
-      const T vp = v[node];
-      const T vpre = v[pre];
-      T i0, i1;
-      if (a.model == 0) {  // synapses/kinetic.py:37-63 (e_syn, alpha, beta, v_th, delta)
-        const T s = ((const T*)a.s)[b * a.n_syn + e];
-        const T tr = sigm(qdiv<T>(vpre - q4, q5));
-        const T aa = q2 * tr;
-        const T rate = aa + q3;
-        const T s_inf = qdiv<T>(aa, rate);
-        const T s_new = s_inf + (s - s_inf) * ex(-dt * rate);
-        ((T*)a.s_new)[b * a.n_syn + e] = s_new;
-        i0 = gs * s_new * (vp - q1);
-        i1 = gs * s_new * ((vp + diff) - q1);
-      } else {  // synapses/sigmoid_rate.py:43-50 (x_offset, slope)
-        i0 = -gs * sigm((vpre - q1) * q2);
-        i1 = -gs * sigm(((vpre + diff) - q1) * q2);
-      }
-      const T d0 = qdiv<T>(i0, ar) * T(100000.0);
-      const T d1 = qdiv<T>(i1, ar) * T(100000.0);
-      const T vt = qdiv<T>(d1 - d0, diff);
-      sums[0][r] = vt;
-      sums[1][r] = d0 - vt * vp;
+  T lin = T(0), cst = T(0);
+  if (ok) {
+    const int node = a.targets_are_nodes ? tgt : a.targets[tgt];
+    const T* v = (const T*)a.v + b * a.n_nodes;
+    const T vp = v[node];
+    const T* s_row = a.model == 0 ? (const T*)a.s + b * a.n_syn : nullptr;
+    T* sn_row = a.model == 0 ? (T*)a.s_new + b * a.n_syn : nullptr;
+    for (int kk = c; kk < a.k; kk += L) {
+      const int64_t e = (int64_t)tgt * a.k + kk;
+      const SynC<T> y = load_syn<T>(a, P, e);
+      T s_new, i0, vt, d0;
+      syn_forward_one<T>(a.model, y, s_row ? s_row[e] : T(0), v[y.pre], vp, dt, diff, s_new, i0, vt, d0);
+      if (sn_row) sn_row[e] = s_new;
       if (a.store_current) ((T*)a.current)[b * a.n_syn + e] = i0;
+      lin += vt;
+      cst += d0 - vt * vp;
     }
-    T tot[2];
-    block_row_sums<T, 2>(sums, nr, red, tot);
-    if ((int)threadIdx.x < nr) {
-      ((T*)a.lin)[(int64_t)(b0 + threadIdx.x) * nt + tgt] = tot[0];
-      ((T*)a.cst)[(int64_t)(b0 + threadIdx.x) * nt + tgt] = tot[1];
-    }
+  }
+  lin = group_sum<L>(lin);
+  cst = group_sum<L>(cst);
+  if (ok && c == 0) {
+    ((T*)a.lin)[b * nt + tgt] = lin;
+    ((T*)a.cst)[b * nt + tgt] = cst;
   }
 }
 
-template <typename T>
-__global__ void __launch_bounds__(1024) syn_backward_kernel(JxbSynArgs a, SynP<T> P) {
-  __shared__ T red[kMaxWarps * kRowBlock];
-  const int tgt = blockIdx.x;
-  const int kk = threadIdx.x;
-  const bool act = kk < a.k;
+template <typename T, int L>
+__global__ void __launch_bounds__(32 * kBwdWarps) syn_backward_kernel(JxbSynArgs a, SynP<T> P) {
+  constexpr int TPW = 32 / L;
+  constexpr int RP = kBwdWarps * kRowsPerWarp;  // rows per pass
+  // red[warp][lane][param]: the warps' parameter gradients of the current chunk;
+  // tile[lane][row of the pass]: its presynaptic voltage gradients.
+  __shared__ T red[kBwdWarps * 32 * 6];
+  __shared__ T tile[32 * RP];
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  const int c = lane & (L - 1);
   const int nt = a.n_syn / a.k;
-  const int64_t e = (int64_t)tgt * a.k + (act ? kk : 0);
+  const int tgt = blockIdx.x * TPW + lane / L;
+  const bool tok = tgt < nt;
   const T* sc = (const T*)a.scalars;
   const T dt = sc[0], diff = sc[1];
-  const int node = a.targets_are_nodes ? tgt : a.targets[tgt];
-  const int pre = a.pre[e];
-  const T gs = P.p[0][e];
-  const T ar = ((const T*)a.area)[e];
-  const T q1 = P.p[1][e], q2 = P.p[2][e];
-  const T q3 = a.model == 0 ? P.p[3][e] : T(0), q4 = a.model == 0 ? P.p[4][e] : T(0),
-          q5 = a.model == 0 ? P.p[5][e] : T(1);
-  T gp[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};  // parameter gradients over the rows
-  T* g_pre = (T*)a.g_pre;
-  for (int b0 = 0; b0 < a.batch; b0 += kRowBlock) {
-    const int nr = min(kRowBlock, a.batch - b0);
-    T gvp[1][kRowBlock];
-#pragma unroll
-    for (int r = 0; r < kRowBlock; ++r) {
-      gvp[0][r] = T(0);
-      if (!act || r >= nr) continue;
-      const int64_t b = b0 + r;
-      const T* v = (const T*)a.v + b * a.n_nodes;
-      const T vp = v[node];
-      const T vpre = v[pre];
-      const T glin = ((const T*)a.g_lin)[b * nt + tgt];
-      const T gconst = ((const T*)a.g_const)[b * nt + tgt];
-      // Forward quantities (kernels/synapse_step.py:225-255).
-      T i0, i1, w0 = T(0), w1 = T(0), s = T(0), s_new = T(0), tr = T(0), rate = T(1), s_inf = T(0),
-               decay = T(0), x = T(0), u0 = T(0), u1 = T(0), sig0 = T(0), sig1 = T(0);
-      if (a.model == 0) {
-        s = ((const T*)a.s)[b * a.n_syn + e];
-        x = qdiv<T>(vpre - q4, q5);
-        tr = sigm(x);
-        const T aa = q2 * tr;
-        rate = aa + q3;
-        s_inf = qdiv<T>(aa, rate);
-        decay = ex(-dt * rate);
-        s_new = s_inf + (s - s_inf) * decay;
-        w0 = vp - q1;
-        w1 = (vp + diff) - q1;
-        i0 = gs * s_new * w0;
-        i1 = gs * s_new * w1;
-      } else {
-        u0 = vpre - q1;
-        u1 = (vpre + diff) - q1;
-        sig0 = sigm(u0 * q2);
-        sig1 = sigm(u1 * q2);
-        i0 = -gs * sig0;
-        i1 = -gs * sig1;
-      }
-      const T d0 = qdiv<T>(i0, ar) * T(100000.0);
-      const T d1 = qdiv<T>(i1, ar) * T(100000.0);
-      const T vt = qdiv<T>(d1 - d0, diff);
-      // Backward (kernels/synapse_step.py:256-305).
-      const T g_vt = glin - gconst * vp;
-      T g_vp = -gconst * vt;
-      const T g_d1 = qdiv<T>(g_vt, diff);
-      const T g_d0 = gconst - g_d1;
-      T g_i0 = qdiv<T>(g_d0 * T(100000.0), ar);
-      const T g_i1 = qdiv<T>(g_d1 * T(100000.0), ar);
-      if (a.g_current) g_i0 += ((const T*)a.g_current)[b * a.n_syn + e];
-      T g_vpre;
-      if (a.model == 0) {
-        const T g_w = g_i0 * w0 + g_i1 * w1;
-        T g_sn = gs * g_w;
-        if (a.g_s_new) g_sn += ((const T*)a.g_s_new)[b * a.n_syn + e];
-        g_vp += gs * s_new * (g_i0 + g_i1);
-        const T g_sinf = g_sn * (T(1) - decay);
-        const T g_rate = -dt * decay * g_sn * (s - s_inf) - qdiv<T>(g_sinf * s_inf, rate);
-        const T g_a = qdiv<T>(g_sinf, rate) + g_rate;
-        const T g_x = g_a * q2 * tr * (T(1) - tr);
-        g_vpre = qdiv<T>(g_x, q5);
-        ((T*)a.g_s)[b * a.n_syn + e] = g_sn * decay;
-        gp[0] += s_new * g_w;
-        gp[1] += -gs * s_new * (g_i0 + g_i1);
-        gp[2] += g_a * tr;
-        gp[3] += g_rate;
-        gp[4] += -g_vpre;
-        gp[5] += -g_vpre * x;
-      } else {
-        const T g_z0 = -gs * g_i0 * sig0 * (T(1) - sig0);
-        const T g_z1 = -gs * g_i1 * sig1 * (T(1) - sig1);
-        g_vpre = (g_z0 + g_z1) * q2;
-        gp[0] += -(g_i0 * sig0 + g_i1 * sig1);
-        gp[1] += -g_vpre;
-        gp[2] += g_z0 * u0 + g_z1 * u1;
-      }
-      gvp[0][r] = g_vp;
-      g_pre[e * a.batch + b] = g_vpre;
-    }
-    T tot[1];
-    block_row_sums<T, 1>(gvp, nr, red, tot);
-    const T g = tot[0];
-    // The target-voltage gradient of row b0 + threadIdx.x: added to g_v here when
-    // accumulating (this CTA owns the (row, target) pair), else by syn_post_kernel.
-    if ((int)threadIdx.x < nr) {
-      const int64_t b = b0 + threadIdx.x;
-      if (a.accumulate) ((T*)a.g_v)[b * a.n_nodes + node] += g;
-      else ((T*)a.g_post)[b * nt + tgt] = g;
-    }
-  }
-  if (!act) return;
+  const int node = tok ? (a.targets_are_nodes ? tgt : a.targets[tgt]) : 0;
   const int np = a.model == 0 ? 6 : 3;
-  int row = 0;
-  for (int q = 0; q < np; ++q) {
-    if (!(a.need & (1 << q))) continue;
-    T& out = ((T*)a.g_params)[(int64_t)row * a.n_syn + e];
-    out = a.accumulate ? out + gp[q] : gp[q];
-    ++row;
+  int need_rows = 0;
+  for (int q = 0; q < np; ++q) need_rows += (a.need >> q) & 1;
+  T* g_pre = (T*)a.g_pre;
+  const int J = (a.k + L - 1) / L;  // synapse chunks
+  for (int b0 = 0; b0 < a.batch; b0 += RP) {  // passes over the rows
+    const int nr = min(RP, a.batch - b0);
+    T gvp[kRowsPerWarp];
+    T glin[kRowsPerWarp], gconst[kRowsPerWarp], vp[kRowsPerWarp];
+#pragma unroll
+    for (int m = 0; m < kRowsPerWarp; ++m) {
+      gvp[m] = T(0);
+      const int r = m * kBwdWarps + warp;
+      const int64_t b = b0 + r;
+      const bool row = tok && r < nr;
+      glin[m] = row ? ((const T*)a.g_lin)[b * nt + tgt] : T(0);
+      gconst[m] = row ? ((const T*)a.g_const)[b * nt + tgt] : T(0);
+      vp[m] = row ? ((const T*)a.v)[b * a.n_nodes + node] : T(0);
+    }
+    for (int i = 0; i < J; ++i) {
+      const int kk = i * L + c;
+      const bool act = tok && kk < a.k;
+      const int64_t e = (int64_t)(tok ? tgt : 0) * a.k + (act ? kk : 0);
+      SynC<T> y = load_syn<T>(a, P, e);
+      T gp[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
+#pragma unroll
+      for (int m = 0; m < kRowsPerWarp; ++m) {
+        const int r = m * kBwdWarps + warp;
+        T g_vpre = T(0);
+        if (act && r < nr) {
+          const int64_t b = b0 + r;
+          const T* v = (const T*)a.v + b * a.n_nodes;
+          const T s = a.model == 0 ? ((const T*)a.s)[b * a.n_syn + e] : T(0);
+          const T gsn = a.g_s_new ? ((const T*)a.g_s_new)[b * a.n_syn + e] : T(0);
+          const T gcu = a.g_current ? ((const T*)a.g_current)[b * a.n_syn + e] : T(0);
+          T g_s, g_vp;
+          syn_backward_one<T>(a.model, y, s, v[y.pre], vp[m], dt, diff, glin[m], gconst[m], gsn, gcu, gp, g_s,
+                              g_vp, g_vpre);
+          if (a.model == 0) ((T*)a.g_s)[b * a.n_syn + e] = g_s;
+          gvp[m] += g_vp;
+        }
+        tile[lane * RP + r] = g_vpre;
+      }
+#pragma unroll
+      for (int q = 0; q < 6; ++q) red[(warp * 32 + lane) * 6 + q] = gp[q];
+      __syncthreads();
+      // Parameter gradients of the chunk's synapses: summed over the warps in order.
+      for (int w = threadIdx.x; w < 32 * need_rows; w += blockDim.x) {
+        const int ln = w & 31, qi = w >> 5;
+        int q = 0, seen = -1;
+        for (; q < np; ++q)
+          if (((a.need >> q) & 1) && ++seen == qi) break;
+        const int t2 = blockIdx.x * TPW + ln / L, k2 = i * L + (ln & (L - 1));
+        if (t2 < nt && k2 < a.k) {
+          T acc = T(0);
+          for (int ww = 0; ww < kBwdWarps; ++ww) acc += red[(ww * 32 + ln) * 6 + q];
+          T& out = ((T*)a.g_params)[(int64_t)qi * a.n_syn + (int64_t)t2 * a.k + k2];
+          out = (a.accumulate || b0 > 0) ? out + acc : acc;
+        }
+      }
+      // Presynaptic voltage gradients of the chunk, row-contiguous per synapse.
+      for (int w = threadIdx.x; w < 32 * nr; w += blockDim.x) {
+        const int ln = w / nr, r = w - ln * nr;
+        const int t2 = blockIdx.x * TPW + ln / L, k2 = i * L + (ln & (L - 1));
+        if (t2 < nt && k2 < a.k) g_pre[((int64_t)t2 * a.k + k2) * a.batch + b0 + r] = tile[ln * RP + r];
+      }
+      __syncthreads();
+    }
+    // The target-voltage gradient of every (row, target): added to g_v here when
+    // accumulating (one lane group owns the pair), else by syn_post_kernel.
+#pragma unroll
+    for (int m = 0; m < kRowsPerWarp; ++m) {
+      const T g = group_sum<L>(gvp[m]);
+      const int r = m * kBwdWarps + warp;
+      if (tok && c == 0 && r < nr) {
+        const int64_t b = b0 + r;
+        if (a.accumulate) ((T*)a.g_v)[b * a.n_nodes + node] += g;
+        else ((T*)a.g_post)[b * nt + tgt] = g;
+      }
+    }
   }
 }
 
@@ -281,15 +342,29 @@ __global__ void syn_post_kernel(JxbSynArgs a) {
   ((T*)a.g_v)[b * a.n_nodes + node] += ((const T*)a.g_post)[b * nt + t];
 }
 
-// Threads per CTA: one per synapse of a target, rounded up to whole warps.
-inline int syn_threads(int k) { return 32 * ((k + 31) / 32); }
+// Lanes per (row, target): a power of two giving about 16 synapses per lane.
+inline int syn_lanes(int k) {
+  int L = 1;
+  while (L < 32 && L * 16 < k) L *= 2;
+  return L;
+}
 
 template <typename T>
 int fwd(const JxbSynArgs& a, cudaStream_t st) {
   SynP<T> P;
   for (int q = 0; q < 6; ++q) P.p[q] = (const T*)a.p[q];
   const int nt = a.n_syn / a.k;
-  syn_forward_kernel<T><<<nt, syn_threads(a.k), 0, st>>>(a, P);
+  const int L = syn_lanes(a.k);
+  const dim3 grid((unsigned)((nt + 32 / L - 1) / (32 / L)), (unsigned)((a.batch + kFwdWarps - 1) / kFwdWarps));
+  const int th = 32 * kFwdWarps;
+  switch (L) {
+    case 1: syn_forward_kernel<T, 1><<<grid, th, 0, st>>>(a, P); break;
+    case 2: syn_forward_kernel<T, 2><<<grid, th, 0, st>>>(a, P); break;
+    case 4: syn_forward_kernel<T, 4><<<grid, th, 0, st>>>(a, P); break;
+    case 8: syn_forward_kernel<T, 8><<<grid, th, 0, st>>>(a, P); break;
+    case 16: syn_forward_kernel<T, 16><<<grid, th, 0, st>>>(a, P); break;
+    default: syn_forward_kernel<T, 32><<<grid, th, 0, st>>>(a, P); break;
+  }
   cudaError_t e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_err("syn_forward_kernel", e);
@@ -311,7 +386,17 @@ int bwd(const JxbSynArgs& a, cudaStream_t st) {
       return JXB_ERR_LAUNCH;
     }
   }
-  syn_backward_kernel<T><<<nt, syn_threads(a.k), 0, st>>>(a, P);
+  const int L = syn_lanes(a.k);
+  const unsigned grid = (unsigned)((nt + 32 / L - 1) / (32 / L));
+  const int th = 32 * kBwdWarps;
+  switch (L) {
+    case 1: syn_backward_kernel<T, 1><<<grid, th, 0, st>>>(a, P); break;
+    case 2: syn_backward_kernel<T, 2><<<grid, th, 0, st>>>(a, P); break;
+    case 4: syn_backward_kernel<T, 4><<<grid, th, 0, st>>>(a, P); break;
+    case 8: syn_backward_kernel<T, 8><<<grid, th, 0, st>>>(a, P); break;
+    case 16: syn_backward_kernel<T, 16><<<grid, th, 0, st>>>(a, P); break;
+    default: syn_backward_kernel<T, 32><<<grid, th, 0, st>>>(a, P); break;
+  }
   const int threads = 256;
   const int64_t n1 = (int64_t)a.n_pre_nodes * a.batch;
   if (n1 > 0) syn_presum_kernel<T><<<(unsigned)((n1 + threads - 1) / threads), threads, 0, st>>>(a);
@@ -329,10 +414,6 @@ int check(const JxbSynArgs* a, bool backward) {
   if (!a || a->k <= 0 || a->n_syn % a->k != 0 || a->batch <= 0 || !a->v || !a->pre ||
       !a->area || !a->scalars || !a->p[0])
     return JXB_ERR_ARG;
-  if (a->k > 32 * kMaxWarps) {
-    snprintf(g_err, sizeof(g_err), "synapse step: %d synapses per target exceed %d", a->k, 32 * kMaxWarps);
-    return JXB_ERR_TOO_LARGE;
-  }
   if (a->model != 0 && a->model != 1) return JXB_ERR_ARG;
   if (a->model == 0 && (!a->s || !a->p[5])) return JXB_ERR_ARG;
   if (!a->targets_are_nodes && !a->targets) return JXB_ERR_ARG;

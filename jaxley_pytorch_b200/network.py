@@ -110,7 +110,7 @@ class NetworkSimulation:
 
     def __init__(self, problem: Problem, dtype=torch.float32, device="cuda", checkpoint: int = 50,
                  threads: int = 256, max_block_nodes: int = 256, rows_per_item: int = 1,
-                 init_steady: bool = False):
+                 init_steady: bool = False, store_trajectory="auto", store_fraction: float = 0.5):
         if not problem.synapses:
             raise ValueError("the problem has no synapses (use Simulation)")
         self.problem = problem
@@ -145,6 +145,30 @@ class NetworkSimulation:
         self.syn_off = i32([e[1] for e in entries] or [0])
         self.syn_rs = i32([e[2] for e in entries] or [1])
         self.syn_launches = 0  # synapse kernel launches issued (forward and adjoint)
+        # With a stored trajectory the differentiable forward keeps every step's
+        # kinetic states and synaptic slopes and offsets, and the adjoint reads them
+        # instead of recomputing each checkpoint segment ("auto": when they take at
+        # most `store_fraction` of the free device memory).
+        if store_trajectory not in (True, False, "auto"):
+            raise ValueError("store_trajectory must be True, False or 'auto'")
+        self.store_trajectory = store_trajectory
+        self.store_fraction = float(store_fraction)
+        self._store_free: Optional[int] = None
+
+    def trajectory_bytes(self, T: int) -> int:
+        """Device bytes of the synapse trajectory of T steps (states and slopes)."""
+        item = torch.empty((), dtype=self.dtype).element_size()
+        states = sum((T + 1) * self.B * ty.E for ty in self.types if ty.kinetic)
+        return (states + 2 * T * self.syn_size) * item
+
+    def stores_trajectory(self, T: int) -> bool:
+        if self.store_trajectory != "auto":
+            return bool(self.store_trajectory)
+        if self._store_free is None:  # sampled once, outside any graph capture
+            if torch.cuda.is_current_stream_capturing():
+                return False
+            self._store_free = torch.cuda.mem_get_info(self.device)[0]
+        return self.trajectory_bytes(T) <= self.store_fraction * self._store_free
 
     def _zeros(self, *shape, dtype=None):
         return torch.zeros(shape, dtype=dtype or self.dtype, device=self.device)
@@ -175,18 +199,32 @@ class NetworkSimulation:
         state = m.initial_state()
         rec = self._zeros(T + 1, B, low.n_rec)
         m.launch_forward(m.args(state, 0, 0, rec, mode=2 if self.init_steady else 1, pscale=pscale))
-        lin = self._zeros(self.syn_size)
-        cst = self._zeros(self.syn_size)
         K = self.checkpoint
-        s_cur = [ty.s0.clone() if ty.kinetic else None for ty in self.types]
-        s_nxt = [torch.empty_like(s) if s is not None else None for s in s_cur]
+        stored = keep and self.stores_trajectory(T)
         saved = None
         if keep:
-            saved = {"states": self._zeros(T, B, low.n_slots),
-                     "s_ckpt": [self._zeros((T + K - 1) // K, B, ty.E) if ty.kinetic else None
-                                for ty in self.types]}
+            saved = {"states": self._zeros(T, B, low.n_slots), "stored": stored}
+            if stored:  # every step's kinetic states, slopes and offsets
+                saved["s_traj"] = [self._zeros(T + 1, B, ty.E) if ty.kinetic else None for ty in self.types]
+                saved["lin"] = self._zeros(T, self.syn_size)
+                saved["cst"] = self._zeros(T, self.syn_size)
+                for q, ty in enumerate(self.types):
+                    if ty.kinetic:
+                        saved["s_traj"][q][0].copy_(ty.s0)
+            else:
+                saved["s_ckpt"] = [self._zeros((T + K - 1) // K, B, ty.E) if ty.kinetic else None
+                                   for ty in self.types]
+        if not stored:
+            lin = self._zeros(self.syn_size)
+            cst = self._zeros(self.syn_size)
+            s_cur = [ty.s0.clone() if ty.kinetic else None for ty in self.types]
+            s_nxt = [torch.empty_like(s) if s is not None else None for s in s_cur]
         for t in range(T):
-            if keep and t % K == 0:
+            if stored:
+                lin, cst = saved["lin"][t], saved["cst"][t]
+                s_cur = [st[t] if st is not None else None for st in saved["s_traj"]]
+                s_nxt = [st[t + 1] if st is not None else None for st in saved["s_traj"]]
+            elif keep and t % K == 0:
                 for q, ty in enumerate(self.types):
                     if ty.kinetic:
                         saved["s_ckpt"][q][t // K].copy_(s_cur[q])
@@ -196,7 +234,8 @@ class NetworkSimulation:
                        ckpt_every=1 if keep else 0)
             self._set_syn(a, lin, cst)
             m.launch_forward(a)
-            s_cur, s_nxt = s_nxt, s_cur
+            if not stored:
+                s_cur, s_nxt = s_nxt, s_cur
         return rec, saved
 
     def backward_raw(self, pscale, syn_params, T: int, saved, rec_grad: torch.Tensor):
@@ -207,11 +246,12 @@ class NetworkSimulation:
         pgrad = self._zeros(B, low.n_cols, dtype=torch.float64)
         traj = self._zeros(1, B, low.n_slots)
         piv = self._zeros(1, B, low.n_nodes)
-        LC_lin = self._zeros(K, self.syn_size)
-        LC_cst = self._zeros(K, self.syn_size)
+        if not saved["stored"]:
+            LC_lin = self._zeros(K, self.syn_size)
+            LC_cst = self._zeros(K, self.syn_size)
+            s_seg = [self._zeros(K + 1, B, ty.E) if ty.kinetic else None for ty in self.types]
         g_lin = self._zeros(self.syn_size)
         g_cst = self._zeros(self.syn_size)
-        s_seg = [self._zeros(K + 1, B, ty.E) if ty.kinetic else None for ty in self.types]
         g_s = [self._zeros(B, ty.E) if ty.kinetic else None for ty in self.types]
         g_s2 = [self._zeros(B, ty.E) if ty.kinetic else None for ty in self.types]
         g_pre = [self._zeros(ty.E, B) for ty in self.types]
@@ -221,18 +261,22 @@ class NetworkSimulation:
         g_par_acc = [self._zeros(n_par[q], ty.E) for q, ty in enumerate(self.types)]
         states = saved["states"]
         rec_grad = rec_grad.contiguous()
+        stored = saved["stored"]
         for seg in range((T + K - 1) // K - 1, -1, -1):
             t0 = seg * K
             k = min(K, T - t0)
-            # recompute the segment's kinetic states and synaptic terms
-            for q, ty in enumerate(self.types):
-                if ty.kinetic:
-                    s_seg[q][0].copy_(saved["s_ckpt"][q][seg])
-            for i in range(k):
+            if stored:  # the forward kept the segment's kinetic states and synaptic terms
+                s_seg = [st[t0:t0 + k + 1] if st is not None else None for st in saved["s_traj"]]
+                LC_lin, LC_cst = saved["lin"][t0:t0 + k], saved["cst"][t0:t0 + k]
+            else:  # recompute them from the segment's checkpoint
                 for q, ty in enumerate(self.types):
-                    self._syn_forward(ty, q, states[t0 + i], s_seg[q][i] if ty.kinetic else None,
-                                      s_seg[q][i + 1] if ty.kinetic else None, LC_lin[i], LC_cst[i],
-                                      syn_params[q])
+                    if ty.kinetic:
+                        s_seg[q][0].copy_(saved["s_ckpt"][q][seg])
+                for i in range(k):
+                    for q, ty in enumerate(self.types):
+                        self._syn_forward(ty, q, states[t0 + i], s_seg[q][i] if ty.kinetic else None,
+                                          s_seg[q][i + 1] if ty.kinetic else None, LC_lin[i], LC_cst[i],
+                                          syn_params[q])
             for i in range(k - 1, -1, -1):
                 t = t0 + i
                 a = m.args(states[t], 1, t, None, pscale=pscale, traj=traj, adj=adj, rec_grad=rec_grad,

@@ -124,20 +124,32 @@ def test_graphed_adam_training_step_matches_eager(cuda_device):
     assert (wg.detach() - we.detach()).abs().max().item() <= 1e-12
 
 
+def _net_grads(prob, w, device, k, store):
+    net = NetworkSimulation(prob, dtype=torch.float64, device=device, checkpoint=k, max_block_nodes=16,
+                            store_trajectory=store)
+    params = [[p.clone().requires_grad_(True) for p in ty.params] for ty in net.types]
+    ps = net.model.pscale.clone().requires_grad_(True)
+    loss = (net.run(ps, params) * w).sum()
+    return [g.cpu().numpy() for g in torch.autograd.grad(loss, [ps] + [p for ty in params for p in ty])]
+
+
 @pytest.mark.parametrize("K", [1, 7])
 def test_gradients_independent_of_checkpoint_interval(cuda_device, K):
-    """The adjoint recomputes each segment's kinetic synapse states from the stored
-    ones; every checkpoint interval must give the gradients of a single segment."""
+    """Without a stored trajectory the adjoint recomputes each segment's kinetic
+    synapse states from its checkpoint; every checkpoint interval must give the
+    gradients of a single segment."""
     prob = _small(n_steps=40, batch=2)
     w = torch.as_tensor(np.random.default_rng(3).normal(size=(2, len(prob.recordings), 41)), device=cuda_device)
-
-    def grads(k):
-        net = NetworkSimulation(prob, dtype=torch.float64, device=cuda_device, checkpoint=k, max_block_nodes=16)
-        params = [[p.clone().requires_grad_(True) for p in ty.params] for ty in net.types]
-        ps = net.model.pscale.clone().requires_grad_(True)
-        loss = (net.run(ps, params) * w).sum()
-        return [g.cpu().numpy() for g in torch.autograd.grad(loss, [ps] + [p for ty in params for p in ty])]
-
-    ref, got = grads(40), grads(K)
+    ref, got = _net_grads(prob, w, cuda_device, 40, False), _net_grads(prob, w, cuda_device, K, False)
     for a, b in zip(ref, got):
         assert np.abs(a - b).max() <= 1e-10 * max(1.0, np.abs(a).max()), np.abs(a - b).max()
+
+
+def test_stored_synapse_trajectory_equals_recompute(cuda_device):
+    """The adjoint over the stored kinetic states and synaptic terms gives the
+    gradients of the recompute form (the same arithmetic on the same values)."""
+    prob = _small(n_steps=40, batch=2)
+    w = torch.as_tensor(np.random.default_rng(4).normal(size=(2, len(prob.recordings), 41)), device=cuda_device)
+    ref, got = _net_grads(prob, w, cuda_device, 7, False), _net_grads(prob, w, cuda_device, 7, True)
+    for a, b in zip(ref, got):
+        assert np.abs(a - b).max() <= 1e-12 * max(1.0, np.abs(a).max()), np.abs(a - b).max()
