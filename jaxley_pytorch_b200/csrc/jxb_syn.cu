@@ -60,17 +60,23 @@ struct SynC {
   int pre;
 };
 
+// Read-only loads through the non-coherent path: the arrays a launch reads are never
+// written by it, which also lets the compiler issue the loads of several synapses
+// before their arithmetic.
+template <typename T>
+__device__ __forceinline__ T rd(const T* p) { return __ldg(p); }
+
 template <typename T>
 __device__ __forceinline__ SynC<T> load_syn(const JxbSynArgs& a, const SynP<T>& P, int64_t e) {
   SynC<T> c;
-  c.pre = a.pre[e];
-  c.gs = P.p[0][e];
-  c.ar = ((const T*)a.area)[e];
-  c.q1 = P.p[1][e];
-  c.q2 = P.p[2][e];
-  c.q3 = a.model == 0 ? P.p[3][e] : T(0);
-  c.q4 = a.model == 0 ? P.p[4][e] : T(0);
-  c.q5 = a.model == 0 ? P.p[5][e] : T(1);
+  c.pre = rd(a.pre + e);
+  c.gs = rd(P.p[0] + e);
+  c.ar = rd((const T*)a.area + e);
+  c.q1 = rd(P.p[1] + e);
+  c.q2 = rd(P.p[2] + e);
+  c.q3 = a.model == 0 ? rd(P.p[3] + e) : T(0);
+  c.q4 = a.model == 0 ? rd(P.p[4] + e) : T(0);
+  c.q5 = a.model == 0 ? rd(P.p[5] + e) : T(1);
   return c;
 }
 
@@ -192,14 +198,16 @@ __global__ void __launch_bounds__(32 * kFwdWarps) syn_forward_kernel(JxbSynArgs 
   if (ok) {
     const int node = a.targets_are_nodes ? tgt : a.targets[tgt];
     const T* v = (const T*)a.v + b * a.n_nodes;
-    const T vp = v[node];
+    const T vp = rd(v + node);
     const T* s_row = a.model == 0 ? (const T*)a.s + b * a.n_syn : nullptr;
     T* sn_row = a.model == 0 ? (T*)a.s_new + b * a.n_syn : nullptr;
+#pragma unroll 4
     for (int kk = c; kk < a.k; kk += L) {
       const int64_t e = (int64_t)tgt * a.k + kk;
       const SynC<T> y = load_syn<T>(a, P, e);
       T s_new, i0, vt, d0;
-      syn_forward_one<T>(a.model, y, s_row ? s_row[e] : T(0), v[y.pre], vp, dt, diff, s_new, i0, vt, d0);
+      syn_forward_one<T>(a.model, y, s_row ? rd(s_row + e) : T(0), rd(v + y.pre), vp, dt, diff, s_new, i0, vt,
+                         d0);
       if (sn_row) sn_row[e] = s_new;
       if (a.store_current) ((T*)a.current)[b * a.n_syn + e] = i0;
       lin += vt;
@@ -245,9 +253,9 @@ __global__ void __launch_bounds__(32 * kBwdWarps) syn_backward_kernel(JxbSynArgs
       const int r = m * kBwdWarps + warp;
       const int64_t b = b0 + r;
       const bool row = tok && r < nr;
-      glin[m] = row ? ((const T*)a.g_lin)[b * nt + tgt] : T(0);
-      gconst[m] = row ? ((const T*)a.g_const)[b * nt + tgt] : T(0);
-      vp[m] = row ? ((const T*)a.v)[b * a.n_nodes + node] : T(0);
+      glin[m] = row ? rd((const T*)a.g_lin + b * nt + tgt) : T(0);
+      gconst[m] = row ? rd((const T*)a.g_const + b * nt + tgt) : T(0);
+      vp[m] = row ? rd((const T*)a.v + b * a.n_nodes + node) : T(0);
     }
     for (int i = 0; i < J; ++i) {
       const int kk = i * L + c;
@@ -262,12 +270,12 @@ __global__ void __launch_bounds__(32 * kBwdWarps) syn_backward_kernel(JxbSynArgs
         if (act && r < nr) {
           const int64_t b = b0 + r;
           const T* v = (const T*)a.v + b * a.n_nodes;
-          const T s = a.model == 0 ? ((const T*)a.s)[b * a.n_syn + e] : T(0);
-          const T gsn = a.g_s_new ? ((const T*)a.g_s_new)[b * a.n_syn + e] : T(0);
-          const T gcu = a.g_current ? ((const T*)a.g_current)[b * a.n_syn + e] : T(0);
+          const T s = a.model == 0 ? rd((const T*)a.s + b * a.n_syn + e) : T(0);
+          const T gsn = a.g_s_new ? rd((const T*)a.g_s_new + b * a.n_syn + e) : T(0);
+          const T gcu = a.g_current ? rd((const T*)a.g_current + b * a.n_syn + e) : T(0);
           T g_s, g_vp;
-          syn_backward_one<T>(a.model, y, s, v[y.pre], vp[m], dt, diff, glin[m], gconst[m], gsn, gcu, gp, g_s,
-                              g_vp, g_vpre);
+          syn_backward_one<T>(a.model, y, s, rd(v + y.pre), vp[m], dt, diff, glin[m], gconst[m], gsn, gcu, gp,
+                              g_s, g_vp, g_vpre);
           if (a.model == 0) ((T*)a.g_s)[b * a.n_syn + e] = g_s;
           gvp[m] += g_vp;
         }
@@ -322,10 +330,12 @@ __global__ void syn_presum_kernel(JxbSynArgs a) {
   const int j = idx / a.batch;
   const int64_t b = idx % a.batch;
   const T* g_pre = (const T*)a.g_pre;
+  const int* inv = a.inv + (int64_t)j * a.inv_width;
   T acc = T(0);
+#pragma unroll 8
   for (int q = 0; q < a.inv_width; ++q) {
-    const int e = a.inv[(int64_t)j * a.inv_width + q];
-    if (e >= 0) acc += g_pre[(int64_t)e * a.batch + b];
+    const int e = rd(inv + q);
+    if (e >= 0) acc += rd(g_pre + (int64_t)e * a.batch + b);
   }
   T& out = ((T*)a.g_v)[b * a.n_nodes + a.pre_nodes[j]];
   out = a.accumulate ? out + acc : acc;

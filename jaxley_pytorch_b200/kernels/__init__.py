@@ -2,13 +2,9 @@
 `kernels/synapse_step.py` of jaxley-pytorch)."""
 
 
-def op_namespace(names) -> str:
-    """The namespace for this package's custom ops named `names`: the reference's
-    `jaxley_pytorch` when none of them is registered there yet, else
-    `jaxley_pytorch_b200` (a second definition under a taken name would silently
-    replace the reference's op for every caller in the process)."""
-    import torch
-
-    if any(hasattr(torch.ops.jaxley_pytorch, n) for n in names):
-        return "jaxley_pytorch_b200"
-    return "jaxley_pytorch"
+# Namespace of this package's custom ops. They keep the reference's op names and
+# schemas (`tree_solve`, `tree_solve_levels`, `synapse_step`, `synapse_step_backward`)
+# under a namespace of their own: torch replaces a custom op that is defined twice
+# under one name, silently and for every holder of the first definition, so sharing
+# `jaxley_pytorch::` would break whichever of the two packages registered first.
+OP_NAMESPACE = "jaxley_pytorch_b200"

@@ -4,13 +4,14 @@
 Same public surface as the reference module (`synapse_step.py:43-498`): `KINETIC`,
 `SIGMOID_RATE`, `kernel_plan(synapse_type, pre, targets, n_nodes, device)`,
 `kernel_scalars(delta_t, diff, dtype, device)`, the custom ops `synapse_step` and
-`synapse_step_backward` with the reference's argument lists and autograd, and
-`fused_step(states, delta_t, sp, gp)`. The kernels are `jxb_synapse_forward` /
-`jxb_synapse_backward` of libjxb: warp reductions over the k synapses of a target
-(forward), batch-sliced warps with a fixed-order reduction of the parameter
-gradients and the transposed index for the presynaptic voltages (backward) — no
-atomics at any width. `JAXLEY_PYTORCH_SYNAPSE_KERNEL=off` disables the plan (then
-the caller runs its own code, as in the reference).
+`synapse_step_backward` with the reference's argument lists and autograd
+(registered as `jaxley_pytorch_b200::synapse_step[_backward]`, beside the
+reference's own ops), and `fused_step(states, delta_t, sp, gp)`. The kernels are
+`jxb_synapse_forward` / `jxb_synapse_backward` of libjxb: lane groups per (row,
+target) with shuffle sums over the target's synapses, a fixed-order reduction of
+the parameter gradients over the batch and the transposed index for the
+presynaptic voltages — no atomics at any width. `JAXLEY_PYTORCH_SYNAPSE_KERNEL=off`
+disables the plan (then the caller runs its own code, as in the reference).
 """
 from __future__ import annotations
 
@@ -23,7 +24,7 @@ import torch
 
 from .. import _lib
 from ..lower import presynaptic_lists
-from . import op_namespace
+from . import OP_NAMESPACE
 
 KINETIC, SIGMOID_RATE = 0, 1
 _NAMES = {
@@ -251,7 +252,7 @@ def _define_in(ns: str):
 def _ensure_ops():
     if synapse_step_op is not None:
         return
-    _define_in(op_namespace(("synapse_step", "synapse_step_backward")))
+    _define_in(OP_NAMESPACE)
 
 
 def _scatter_to_nodes(per_target: torch.Tensor, targets: torch.Tensor, n: int) -> torch.Tensor:

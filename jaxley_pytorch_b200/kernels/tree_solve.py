@@ -12,9 +12,9 @@ schedule, warp-register blocks); the kernels are `jxb_tree_solve_levels` and
 `jxb_tree_solve_registers` of libjxb. There is no torch fallback: the reference
 returns `None` for orders it cannot handle, this module raises.
 
-The custom ops are registered as `jaxley_pytorch::tree_solve[_levels]` when that
-namespace is free, else (the reference's Triton module already registered it in the
-same process) as `jaxley_pytorch_b200::tree_solve[_levels]`.
+The custom ops are registered as `jaxley_pytorch_b200::tree_solve[_levels]`: the
+reference's names and schemas under a namespace of their own, so that this module
+and the reference's Triton module can be loaded in one process.
 """
 from __future__ import annotations
 
@@ -29,7 +29,7 @@ import torch
 
 from .. import _lib
 from ..lower import block_schedule, chain_table
-from . import op_namespace
+from . import OP_NAMESPACE
 
 MAX_BLOCK = 8192  # registers variant: up to 256 nodes in one warp, larger blocks in a CTA
 LEVEL_BLOCK = 4096  # levels variant: nodes per block of trees (shared memory bound)
@@ -324,9 +324,8 @@ def _transposed_backward(kernel_op, ctx, grad_x, args_after):
 
 def _define_ops():
     global _NS
-    ns = op_namespace(("tree_solve", "tree_solve_levels"))
-    _define_in(ns)
-    _NS = ns
+    _define_in(OP_NAMESPACE)
+    _NS = OP_NAMESPACE
 
 
 def _define_in(ns: str):
