@@ -74,7 +74,7 @@ __host__ __device__ inline size_t sim_smem_layout(const JxbSimArgs& a, bool back
   };
   SimSmem<T> s;
   // 8-byte types first.
-  s.st = (T*)take(sizeof(T) * R * ns);
+  s.st = (T*)take(sizeof(T) * R * ns + 16);  // + room to shift a row to its source's 16-byte phase
   s.adj = backward ? (T*)take(sizeof(T) * R * ns) : nullptr;
   s.D = (T*)take(sizeof(T) * R * nn);
   s.S = (T*)take(sizeof(T) * R * nn);
@@ -912,19 +912,37 @@ __device__ __forceinline__ void cp_async_elem(T* smem_dst, const T* gsrc) {
   else
     asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(s), "l"(gsrc) : "memory");
 }
+// 16-byte asynchronous copy global -> shared (both addresses 16-byte aligned).
+__device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
+  const unsigned s = (unsigned)__cvta_generic_to_shared(smem_dst);
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gsrc) : "memory");
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// Stages one contiguous range of `cnt` elements asynchronously: 16-byte copies for
+// the part where source and destination share their 16-byte phase, element copies
+// for the ends (and for the whole range when the phases differ).
+template <typename T>
+__device__ __forceinline__ void stage_range_async(T* dst, const T* src, int cnt) {
+  constexpr int V = 16 / (int)sizeof(T);
+  int head = cnt, nvec = 0;
+  if ((((uintptr_t)dst ^ (uintptr_t)src) & 15) == 0) {
+    head = min(cnt, (int)(((16 - ((uintptr_t)src & 15)) & 15) / sizeof(T)));
+    nvec = (cnt - head) / V;
+  }
+  for (int q = threadIdx.x; q < head; q += blockDim.x) cp_async_elem(dst + q, src + q);
+  for (int q = threadIdx.x; q < nvec; q += blockDim.x) cp_async16(dst + head + q * V, src + head + q * V);
+  for (int q = head + nvec * V + threadIdx.x; q < cnt; q += blockDim.x) cp_async_elem(dst + q, src + q);
+}
 
 // Stages the item's rows of a (steps, batch, width) array at `step` (the block's
 // range starting at `off`, `cnt` wide) into shared memory rows of stride `cnt`.
 template <typename T>
 __device__ __forceinline__ void stage_rows_async(T* dst, const T* src, int step, int batch, int width, int off,
                                                  int cnt, int row0, int rows) {
-  for (int r = 0; r < rows; ++r) {
-    const T* g = src + ((size_t)step * batch + row0 + r) * width + off;
-    T* d = dst + (size_t)r * cnt;
-    for (int q = threadIdx.x; q < cnt; q += blockDim.x) cp_async_elem(d + q, g + q);
-  }
+  for (int r = 0; r < rows; ++r)
+    stage_range_async<T>(dst + (size_t)r * cnt, src + ((size_t)step * batch + row0 + r) * width + off, cnt);
   cp_async_commit();
 }
 
@@ -938,6 +956,10 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
   const JxbBlock blk = a.blocks[item.block];
   sm.gbase = a.gbase + blk.node0;
   if (L.gacc) sm.gacc = (T*)((char*)L.gacc + (size_t)blockIdx.x * (size_t)L.gacc_stride);
+  // A one-row item's state row starts at the 16-byte phase of its rows in the
+  // trajectory (rows of a multiple of 16 bytes, block at slot0), so that staging it
+  // takes 16-byte copies.
+  if (item.n_rows == 1 && sizeof(T) <= 8) sm.st += blk.slot0 % (16 / (int)sizeof(T));
   const int gslots = L.max_gslots;
   const int rows = item.n_rows, row0 = item.row0;
   const int tid = threadIdx.x, nthr = blockDim.x;

@@ -132,7 +132,9 @@ class Lowered:
 
     @property
     def n_slots(self) -> int:
-        return int(self.soff[-1])
+        """Length of a row of the state vector: the nodes' slots, padded to a multiple
+        of 4 (16 bytes of float32) so that rows start on the same 16-byte phase."""
+        return int(self.state0.shape[1])
 
     @property
     def n_pslots(self) -> int:
@@ -664,7 +666,7 @@ def lower(problem: Problem, max_block_nodes: int = 4096, dtype=np.float64,
 
     # ---- initial state ----
     L = int(soff[-1])
-    state0 = np.zeros((B, L), dtype=np.float64)
+    state0 = np.zeros((B, (L + 3) // 4 * 4), dtype=np.float64)  # padded row (unused tail)
     for g in range(G):
         I = grp_nodes[g]
         R = int2node[I]
