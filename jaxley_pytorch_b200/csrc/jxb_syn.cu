@@ -180,6 +180,7 @@ __device__ __forceinline__ T group_sum(T v) {
 }
 
 constexpr int kFwdWarps = 4;      // batch rows per forward CTA
+constexpr int kFwdBatch = 4;      // synapses of a lane loaded together in the forward
 constexpr int kBwdWarps = 8;      // warps per backward CTA
 constexpr int kRowsPerWarp = 4;   // rows of a backward warp per pass
 
@@ -201,17 +202,32 @@ __global__ void __launch_bounds__(32 * kFwdWarps) syn_forward_kernel(JxbSynArgs 
     const T vp = rd(v + node);
     const T* s_row = a.model == 0 ? (const T*)a.s + b * a.n_syn : nullptr;
     T* sn_row = a.model == 0 ? (T*)a.s_new + b * a.n_syn : nullptr;
-#pragma unroll 4
-    for (int kk = c; kk < a.k; kk += L) {
-      const int64_t e = (int64_t)tgt * a.k + kk;
-      const SynC<T> y = load_syn<T>(a, P, e);
-      T s_new, i0, vt, d0;
-      syn_forward_one<T>(a.model, y, s_row ? rd(s_row + e) : T(0), rd(v + y.pre), vp, dt, diff, s_new, i0, vt,
-                         d0);
-      if (sn_row) sn_row[e] = s_new;
-      if (a.store_current) ((T*)a.current)[b * a.n_syn + e] = i0;
-      lin += vt;
-      cst += d0 - vt * vp;
+    // kFwdBatch synapses of the lane at a time: all their loads first (indices
+    // clamped to the target's range), then the presynaptic voltages, then the
+    // arithmetic, so that a warp keeps that many independent loads in flight.
+    for (int kb = c; kb < a.k; kb += kFwdBatch * L) {
+      SynC<T> y[kFwdBatch];
+      T sv[kFwdBatch], vv[kFwdBatch];
+#pragma unroll
+      for (int u = 0; u < kFwdBatch; ++u) {
+        const int64_t e = (int64_t)tgt * a.k + min(kb + u * L, a.k - 1);
+        y[u] = load_syn<T>(a, P, e);
+        sv[u] = s_row ? rd(s_row + e) : T(0);
+      }
+#pragma unroll
+      for (int u = 0; u < kFwdBatch; ++u) vv[u] = rd(v + y[u].pre);
+#pragma unroll
+      for (int u = 0; u < kFwdBatch; ++u) {
+        const int kk = kb + u * L;
+        if (kk >= a.k) break;
+        const int64_t e = (int64_t)tgt * a.k + kk;
+        T s_new, i0, vt, d0;
+        syn_forward_one<T>(a.model, y[u], sv[u], vv[u], vp, dt, diff, s_new, i0, vt, d0);
+        if (sn_row) sn_row[e] = s_new;
+        if (a.store_current) ((T*)a.current)[b * a.n_syn + e] = i0;
+        lin += vt;
+        cst += d0 - vt * vp;
+      }
     }
   }
   lin = group_sum<L>(lin);
@@ -332,10 +348,16 @@ __global__ void syn_presum_kernel(JxbSynArgs a) {
   const T* g_pre = (const T*)a.g_pre;
   const int* inv = a.inv + (int64_t)j * a.inv_width;
   T acc = T(0);
-#pragma unroll 8
-  for (int q = 0; q < a.inv_width; ++q) {
-    const int e = rd(inv + q);
-    if (e >= 0) acc += rd(g_pre + (int64_t)e * a.batch + b);
+  constexpr int U = 8;  // entries loaded together
+  for (int q0 = 0; q0 < a.inv_width; q0 += U) {
+    int e[U];
+    T g[U];
+#pragma unroll
+    for (int u = 0; u < U; ++u) e[u] = q0 + u < a.inv_width ? rd(inv + q0 + u) : -1;
+#pragma unroll
+    for (int u = 0; u < U; ++u) g[u] = e[u] >= 0 ? rd(g_pre + (int64_t)e[u] * a.batch + b) : T(0);
+#pragma unroll
+    for (int u = 0; u < U; ++u) acc += g[u];
   }
   T& out = ((T*)a.g_v)[b * a.n_nodes + a.pre_nodes[j]];
   out = a.accumulate ? out + acc : acc;
