@@ -248,8 +248,9 @@ typedef struct JxbSimArgs_ {
   int32_t n_clamp, clamp_steps, clamp_rows, pad6;
   /* Optional failure flag (device int32, may be null): a launch whose final states
    * (forward) or state adjoints and parameter gradients (adjoint) hold a value that is
-   * not finite ORs JXB_NONFINITE into it. The host reads and clears it between
-   * launches; the kernels never stop or fault on a non-finite value. */
+   * not finite ORs JXB_NONFINITE into it; an adjoint launch whose bounded wait for
+   * a bulk copy gave up ORs JXB_TIMEOUT (its results are then invalid). The host reads
+   * and clears it between launches; the kernels never stop or fault on either. */
   int32_t* status;
   /* Step scheme of the voltage (modules/base.py:3327-3365): JXB_SCHEME_BWD_EULER, or
    * JXB_SCHEME_CN (Crank-Nicolson: the implicit system of half a step, then
@@ -257,7 +258,7 @@ typedef struct JxbSimArgs_ {
   int32_t scheme, pad7;
 } JxbSimArgs;
 
-enum { JXB_NONFINITE = 1 };
+enum { JXB_NONFINITE = 1, JXB_TIMEOUT = 2 };
 enum { JXB_SCHEME_BWD_EULER = 0, JXB_SCHEME_CN = 1 };
 
 int jxb_sim_forward(const JxbSimArgs* args, void* stream);

@@ -15,6 +15,7 @@ LIB_PATH = os.path.join(_HERE, "_build", "libjxb.so")
 
 JXB_OK = 0
 JXB_NONFINITE = 1  # bit of JxbSimArgs.status: a launch produced a value that is not finite
+JXB_TIMEOUT = 2  # bit of JxbSimArgs.status: a bounded wait of a launch gave up
 F32, F64 = 0, 1
 SCHEME_BWD_EULER, SCHEME_CN = 0, 1  # JxbSimArgs.scheme
 

@@ -49,6 +49,7 @@ struct SimSmem {
   T* V;                      // rows * n_nodes: voltages during the segment
   // adjoint
   T *adj, *X1;               // rows * n_slots, rows * n_nodes
+  unsigned long long* mbar;  // completion barrier of the bulk copies of the state row
 };
 
 __host__ __device__ inline size_t align_up(size_t x, size_t a) { return (x + a - 1) / a * a; }
@@ -74,7 +75,10 @@ __host__ __device__ inline size_t sim_smem_layout(const JxbSimArgs& a, bool back
   };
   SimSmem<T> s;
   // 8-byte types first.
-  s.st = (T*)take(sizeof(T) * R * ns + 16);  // + room to shift a row to its source's 16-byte phase
+  // + room to place a row at its source's 16-byte phase and round a bulk copy up to
+  // whole 16-byte units
+  s.st = (T*)take(sizeof(T) * R * ns + 32);
+  s.mbar = backward ? (unsigned long long*)take(16) : nullptr;
   s.adj = backward ? (T*)take(sizeof(T) * R * ns) : nullptr;
   s.D = (T*)take(sizeof(T) * R * nn);
   s.S = (T*)take(sizeof(T) * R * nn);
@@ -920,6 +924,62 @@ __device__ __forceinline__ void cp_async16(void* smem_dst, const void* gsrc) {
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Bulk copies global -> shared (the copy engine, one instruction for a whole row)
+// completing on an mbarrier; no cluster multicast.
+__device__ __forceinline__ unsigned smem_addr(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(unsigned long long* m, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(smem_addr(m)), "r"(count) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(unsigned long long* m, unsigned bytes) {
+  asm volatile("{\n .reg .b64 st;\n mbarrier.arrive.expect_tx.shared::cta.b64 st, [%0], %1;\n}\n" ::"r"(
+                   smem_addr(m)),
+               "r"(bytes)
+               : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, unsigned bytes, unsigned long long* m) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_addr(dst)),
+               "l"(src), "r"(bytes), "r"(smem_addr(m))
+               : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(unsigned long long* m, unsigned parity) {
+  unsigned ok;
+  asm volatile(
+      "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(m)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+// Waits for phase `parity` of `m` at most kMaxWaitPolls polls; false when it gave up
+// (the launch then reports JXB_TIMEOUT instead of hanging).
+constexpr int kMaxWaitPolls = 1 << 20;
+__device__ __forceinline__ bool mbar_wait(unsigned long long* m, unsigned parity) {
+  for (int i = 0; i < kMaxWaitPolls; ++i)
+    if (mbar_try_wait(m, parity)) return true;
+  return false;
+}
+
+// Orders this thread's earlier ordinary accesses (shared and global) before later
+// bulk copies; every thread calls it before the barrier that precedes a copy.
+__device__ __forceinline__ void fence_proxy_async() { asm volatile("fence.proxy.async;\n" ::: "memory"); }
+
+// Issues (thread 0) the bulk copy of `cnt` elements at `src` into the row buffer
+// `base` (16-byte aligned, 32 bytes longer than the row) so that element 0 lands at
+// base + shift, where shift puts the row at its source's 16-byte phase; the copy is
+// widened to whole 16-byte units on both ends. Every thread gets the shift.
+template <typename T>
+__device__ __forceinline__ int bulk_stage_row(T* base, const T* src, int cnt, unsigned long long* m) {
+  const int shift = (int)(((uintptr_t)src & 15) / sizeof(T));
+  const unsigned bytes = (unsigned)(((size_t)(cnt + shift) * sizeof(T) + 15) & ~(size_t)15);
+  if (threadIdx.x == 0) {
+    mbar_expect_tx(m, bytes);
+    bulk_copy_g2s(base, src - shift, bytes, m);
+  }
+  return shift;
+}
+
 // Stages one contiguous range of `cnt` elements asynchronously: 16-byte copies for
 // the part where source and destination share their 16-byte phase, element copies
 // for the ends (and for the whole range when the phases differ).
@@ -956,10 +1016,12 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
   const JxbBlock blk = a.blocks[item.block];
   sm.gbase = a.gbase + blk.node0;
   if (L.gacc) sm.gacc = (T*)((char*)L.gacc + (size_t)blockIdx.x * (size_t)L.gacc_stride);
-  // A one-row item's state row starts at the 16-byte phase of its rows in the
-  // trajectory (rows of a multiple of 16 bytes, block at slot0), so that staging it
-  // takes 16-byte copies.
-  if (item.n_rows == 1 && sizeof(T) <= 8) sm.st += blk.slot0 % (16 / (int)sizeof(T));
+  // One-row items stage each step's state row with one bulk copy (rows of a multiple
+  // of 16 bytes: the copy, widened to 16-byte units, stays inside the row).
+  T* const st_base = sm.st;
+  bool bulk = !GM && item.n_rows == 1 && (a.n_slots * (int)sizeof(T)) % 16 == 0 && a.traj != nullptr &&
+              ((uintptr_t)a.traj & 15) == 0;
+  if (bulk) sm.st = st_base + blk.slot0 % (16 / (int)sizeof(T));
   const int gslots = L.max_gslots;
   const int rows = item.n_rows, row0 = item.row0;
   const int tid = threadIdx.x, nthr = blockDim.x;
@@ -998,13 +1060,23 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
   // and the transposed solve, which do not use st) asynchronously, so that the
   // per-node phases do not wait on global memory.
   if constexpr (!GM) {
+    if (bulk && tid == 0) mbar_init(sm.mbar, 1);
     stage_rows_async<T>(sm.D, piv, K - 1, a.batch, a.n_nodes, blk.node0, nn, row0, rows);
     cp_async_wait_all();
+    if (bulk) fence_proxy_async();  // the recompute's trajectory stores before the copies
     __syncthreads();
   }
+  unsigned parity = 0;  // phase of the state-row barrier the next wait expects
+  int timed_out = 0;
   for (int step = K - 1; step >= 0; --step) {
     const int t = a.t0 + step;
-    if constexpr (!GM) stage_rows_async<T>(sm.st, traj, step, a.batch, a.n_slots, blk.slot0, ns, row0, rows);
+    if constexpr (!GM) {
+      if (bulk)
+        sm.st = st_base + bulk_stage_row<T>(st_base, traj + ((size_t)step * a.batch + row0) * a.n_slots +
+                                                         blk.slot0, ns, sm.mbar);
+      else
+        stage_rows_async<T>(sm.st, traj, step, a.batch, a.n_slots, blk.slot0, ns, row0, rows);
+    }
     // Phase 1: recording gradients at t + 1, the pivots of the step's matrix and the
     // right-hand side of the transposed solve.
     for (int w = tid; w < total; w += nthr) {
@@ -1028,7 +1100,11 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
     // the forward elimination.
     block_solve_pivots<T>(blk, sm, rows, sm.au, sm.al);
     if constexpr (!GM) {
-      cp_async_wait_all();  // the step's states
+      cp_async_wait_all();  // the step's states (element copies)
+      if (bulk) {           // the step's states (bulk copy)
+        if (!mbar_wait(sm.mbar, parity)) timed_out = 1;
+        parity ^= 1u;
+      }
       __syncthreads();
       if (step > 0) stage_rows_async<T>(sm.D, piv, step - 1, a.batch, a.n_nodes, blk.node0, nn, row0, rows);
     }
@@ -1080,7 +1156,10 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
       lam[0] = lv;
       sm.X1[(size_t)r * nn + j] = x[solve_slot<T>(sm, j, nn, ns)];
     }
-    if constexpr (!GM) cp_async_wait_all();  // the next step's pivots
+    if constexpr (!GM) {
+      cp_async_wait_all();            // the next step's pivots
+      if (bulk) fence_proxy_async();  // this step's accesses to the state row before the next copy
+    }
     __syncthreads();
   }
   if (a.t0 == 0) {
@@ -1106,6 +1185,12 @@ __device__ __forceinline__ void sim_backward_body(const JxbSimArgs& a, const Jxb
       node_initial_current_adjoint<T>(sm, j, x, lam, sm.pv + (size_t)r * np, sm.gacc + (size_t)r * gslots);
     }
     __syncthreads();
+  }
+  // A bulk copy whose wait gave up may still be in flight: wait for it once more
+  // (bounded) before the CTA leaves, and report the timeout.
+  if (__syncthreads_or(timed_out)) {
+    if (bulk) mbar_wait(sm.mbar, parity ^ 1u);
+    if (tid == 0 && a.status) atomicOr(a.status, JXB_TIMEOUT);
   }
   int bad = 0;  // a value that is not finite seen by this thread
   // Fold the nodes' gradient slots into the columns (float64, global), once per

@@ -412,6 +412,8 @@ class DeviceModel:
         flag = int(self.status.item())
         if flag:
             self.status.zero_()
+            if flag & _lib.JXB_TIMEOUT:
+                raise RuntimeError(f"a wait for an asynchronous copy in the {what} gave up (results invalid)")
             raise FloatingPointError(f"the {what} produced values that are not finite (NaN or inf)")
 
     def launch_forward(self, args: _lib.JxbSimArgs, stream=None) -> None:
