@@ -238,8 +238,11 @@ class NetworkSimulation:
                 s_cur, s_nxt = s_nxt, s_cur
         return rec, saved
 
-    def backward_raw(self, pscale, syn_params, T: int, saved, rec_grad: torch.Tensor):
-        """Returns `(d loss / d pscale (B, n_cols) float64, [per type: (n_params, E)])`."""
+    def backward_raw(self, pscale, syn_params, T: int, saved, rec_grad: torch.Tensor,
+                     need: Optional[List[int]] = None):
+        """Returns `(d loss / d pscale (B, n_cols) float64, [per type: (n_params, E)])`.
+        `need` (per type, a bit mask of its parameters; default all) selects the
+        parameter gradients the synapse adjoint computes; the others are zero."""
         m, low, B = self.model, self.low, self.B
         K = self.checkpoint
         adj = self._zeros(B, low.n_slots)
@@ -258,7 +261,9 @@ class NetworkSimulation:
         n_par = [len(p) for p in syn_params]
         # the synapse adjoint adds every step's parameter gradients here and its
         # voltage gradients straight into the state adjoint (accumulate mode)
-        g_par_acc = [self._zeros(n_par[q], ty.E) for q, ty in enumerate(self.types)]
+        if need is None:
+            need = [(1 << n) - 1 for n in n_par]
+        g_rows = [self._zeros(bin(need[q]).count("1"), ty.E) for q, ty in enumerate(self.types)]
         states = saved["states"]
         rec_grad = rec_grad.contiguous()
         stored = saved["stored"]
@@ -298,13 +303,24 @@ class NetworkSimulation:
                     b.g_s = g_s2[q].data_ptr() if ty.kinetic else None
                     b.g_v = adj.data_ptr()
                     b.accumulate = 1
-                    b.need = (1 << n_par[q]) - 1
-                    b.g_params = g_par_acc[q].data_ptr()
+                    b.need = need[q]
+                    b.g_params = g_rows[q].data_ptr() if need[q] else None
                     b.g_pre = g_pre[q].data_ptr()
                     _lib.check(_lib.load().jxb_synapse_backward(C.byref(b), _stream()), "jxb_synapse_backward")
                     self.syn_launches += 1
                     if ty.kinetic:
                         g_s[q], g_s2[q] = g_s2[q], g_s[q]
+        # the rows of the computed parameters in parameter order, zeros for the others
+        g_par_acc = []
+        for q, ty in enumerate(self.types):
+            rows, k = [], 0
+            for i in range(n_par[q]):
+                if (need[q] >> i) & 1:
+                    rows.append(g_rows[q][k])
+                    k += 1
+                else:
+                    rows.append(torch.zeros(ty.E, dtype=self.dtype, device=self.device))
+            g_par_acc.append(rows)
         return pgrad, g_par_acc
 
     def run(self, pscale: Optional[torch.Tensor] = None, syn_params: Optional[List[List[torch.Tensor]]] = None,
@@ -338,6 +354,7 @@ class _NetFn(torch.autograd.Function):
             net.model.check_finite("network simulation")
         ctx.net, ctx.T, ctx.counts, ctx.saved_data = net, T, counts, saved
         ctx.params = params
+        ctx.wants = [p.requires_grad for p in flat]
         ctx.save_for_backward(ps)
         ctx.dtypes = (pscale.dtype, [p.dtype for p in flat])
         return rec.permute(1, 2, 0)
@@ -347,7 +364,11 @@ class _NetFn(torch.autograd.Function):
         (ps,) = ctx.saved_tensors
         net = ctx.net
         rec_grad = grad_out.to(net.dtype).permute(2, 0, 1).contiguous()
-        pgrad, g_par = net.backward_raw(ps, ctx.params, ctx.T, ctx.saved_data, rec_grad)
+        need, q = [], 0
+        for c in ctx.counts:
+            need.append(sum(1 << i for i in range(c) if ctx.wants[q + i]))
+            q += c
+        pgrad, g_par = net.backward_raw(ps, ctx.params, ctx.T, ctx.saved_data, rec_grad, need=need)
         if net.sim.check_finite:
             net.model.check_finite("network adjoint")
         out = [None, None, None, pgrad.to(ctx.dtypes[0])]
@@ -355,7 +376,7 @@ class _NetFn(torch.autograd.Function):
         q = 0
         for t, c in enumerate(ctx.counts):
             for i in range(c):
-                out.append(g_par[t][i].to(dts[q]))
+                out.append(g_par[t][i].to(dts[q]) if ctx.wants[q] else None)
                 q += 1
         return tuple(out)
 
