@@ -11,14 +11,15 @@
 //
 // forward:  warps over batch rows (4 per CTA, the same targets, so that the
 //           parameters are reused from L1), 32 / L targets per warp.
-// backward: one CTA per group of 32 / L targets with 8 warps over the batch rows
-//           (each warp up to kRowsPerWarp rows per pass). Per synapse chunk (one
+// backward: one CTA per group of 32 / L targets (one target once k > 32) with 8
+//           warps over the batch rows (each warp up to kRowsPerWarp rows per pass). Per synapse chunk (one
 //           value of i in c + i L) the parameter gradients are summed over the
 //           warp's rows in registers and over the warps in shared memory in a fixed
 //           order, and the presynaptic voltage gradients of the chunk are staged in
 //           shared memory and written to an (E, batch) buffer row-contiguously; a
 //           second kernel sums them per presynaptic node through the transposed
-//           index. No atomics, deterministic.
+//           index (four warps per node, each over a quarter of its synapses). No
+//           atomics, deterministic.
 // float: fast reciprocal / division / exp (jxb_math.cuh); float64 stays exact.
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -339,28 +340,44 @@ __global__ void __launch_bounds__(32 * kBwdWarps) syn_backward_kernel(JxbSynArgs
 
 // g_v[b, pre_nodes[j]] = sum over the synapses of node j of g_pre[e, b]; then the
 // postsynaptic terms g_post[b, t] are added at the targets.
+constexpr int kPresumParts = 4;  // warps per presynaptic node, each summing a quarter of its synapses
+
+// g_v[b, pre_nodes[j]] = sum over the synapses e of node j of g_pre[e, b]: one CTA per
+// (node, 32 rows), warp p sums the entries p, p + 4, ... of the node's list for its
+// lane's row (coalesced rows of g_pre), the four partial sums are added in order.
 template <typename T>
-__global__ void syn_presum_kernel(JxbSynArgs a) {
-  const int64_t idx = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-  if (idx >= (int64_t)a.n_pre_nodes * a.batch) return;
-  const int j = idx / a.batch;
-  const int64_t b = idx % a.batch;
+__global__ void __launch_bounds__(32 * kPresumParts) syn_presum_kernel(JxbSynArgs a) {
+  __shared__ T part[kPresumParts][32];
+  const int j = blockIdx.x;
+  const int lane = threadIdx.x & 31, p = threadIdx.x >> 5;
+  const int64_t b = (int64_t)blockIdx.y * 32 + lane;
+  const bool ok = b < a.batch;
   const T* g_pre = (const T*)a.g_pre;
   const int* inv = a.inv + (int64_t)j * a.inv_width;
   T acc = T(0);
   constexpr int U = 8;  // entries loaded together
-  for (int q0 = 0; q0 < a.inv_width; q0 += U) {
+  for (int q0 = p; q0 < a.inv_width; q0 += U * kPresumParts) {
     int e[U];
     T g[U];
 #pragma unroll
-    for (int u = 0; u < U; ++u) e[u] = q0 + u < a.inv_width ? rd(inv + q0 + u) : -1;
+    for (int u = 0; u < U; ++u) {
+      const int q = q0 + u * kPresumParts;
+      e[u] = q < a.inv_width ? rd(inv + q) : -1;
+    }
 #pragma unroll
-    for (int u = 0; u < U; ++u) g[u] = e[u] >= 0 ? rd(g_pre + (int64_t)e[u] * a.batch + b) : T(0);
+    for (int u = 0; u < U; ++u) g[u] = (ok && e[u] >= 0) ? rd(g_pre + (int64_t)e[u] * a.batch + b) : T(0);
 #pragma unroll
     for (int u = 0; u < U; ++u) acc += g[u];
   }
-  T& out = ((T*)a.g_v)[b * a.n_nodes + a.pre_nodes[j]];
-  out = a.accumulate ? out + acc : acc;
+  part[p][lane] = acc;
+  __syncthreads();
+  if (p == 0 && ok) {
+    T sum = part[0][lane];
+#pragma unroll
+    for (int w = 1; w < kPresumParts; ++w) sum += part[w][lane];
+    T& out = ((T*)a.g_v)[b * a.n_nodes + a.pre_nodes[j]];
+    out = a.accumulate ? out + sum : sum;
+  }
 }
 
 template <typename T>
@@ -418,7 +435,9 @@ int bwd(const JxbSynArgs& a, cudaStream_t st) {
       return JXB_ERR_LAUNCH;
     }
   }
-  const int L = syn_lanes(a.k);
+  // One target per CTA (L = 32) once a target has more than 32 synapses: four times
+  // the CTAs of the forward's lane groups, which keeps more warps in flight.
+  const int L = a.k > 32 ? 32 : syn_lanes(a.k);
   const unsigned grid = (unsigned)((nt + 32 / L - 1) / (32 / L));
   const int th = 32 * kBwdWarps;
   switch (L) {
@@ -431,7 +450,8 @@ int bwd(const JxbSynArgs& a, cudaStream_t st) {
   }
   const int threads = 256;
   const int64_t n1 = (int64_t)a.n_pre_nodes * a.batch;
-  if (n1 > 0) syn_presum_kernel<T><<<(unsigned)((n1 + threads - 1) / threads), threads, 0, st>>>(a);
+  if (n1 > 0)
+    syn_presum_kernel<T><<<dim3((unsigned)a.n_pre_nodes, (unsigned)((a.batch + 31) / 32)), 32 * kPresumParts, 0, st>>>(a);
   const int64_t n2 = (int64_t)nt * a.batch;
   if (!a.accumulate) syn_post_kernel<T><<<(unsigned)((n2 + threads - 1) / threads), threads, 0, st>>>(a);
   e = cudaGetLastError();
