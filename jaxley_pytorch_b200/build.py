@@ -49,7 +49,8 @@ def units():
             continue
         for tname, tag in (("float", "f32"), ("double", "f64")):
             for bwd, kind in ((0, "fwd"), (1, "bwd")):
-                for nt in (256, 512, 1024):
+                # 384: float adjoint CTAs of 12 warps, two per SM with up to 80 registers
+                for nt in (256, 384, 512, 1024) if (tag, kind) == ("f32", "bwd") else (256, 512, 1024):
                     fn = f"sim_kernel_{tag}_{kind}_{nt}"
                     out.append((src, os.path.join(OUT_DIR, f"{base}_{tag}_{kind}_{nt}.o"),
                                 [f"-DJXB_INST_T={tname}", f"-DJXB_INST_BWD={bwd}",

@@ -43,6 +43,7 @@ SimKernel pick_kernel(bool backward, int threads, bool gm, bool multi, bool wide
     if (f) return backward ? sim_kernel_f32_bwd_256(gm, multi, wide) : sim_kernel_f32_fwd_256(gm, multi, wide);
     return backward ? sim_kernel_f64_bwd_256(gm, multi, wide) : sim_kernel_f64_fwd_256(gm, multi, wide);
   }
+  if (threads <= 384 && f && backward) return sim_kernel_f32_bwd_384(gm, multi, false);
   if (threads <= 512) {
     if (f) return backward ? sim_kernel_f32_bwd_512(gm, multi, false) : sim_kernel_f32_fwd_512(gm, multi, false);
     return backward ? sim_kernel_f64_bwd_512(gm, multi, false) : sim_kernel_f64_fwd_512(gm, multi, false);

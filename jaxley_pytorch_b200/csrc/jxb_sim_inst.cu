@@ -2,7 +2,7 @@
 // size class. The build compiles this unit once per combination, defining
 //   JXB_INST_T    float or double
 //   JXB_INST_BWD  0 forward, 1 adjoint
-//   JXB_INST_NT   256, 512 or 1024 (threads per CTA the kernels are bounded for)
+//   JXB_INST_NT   256, 384, 512 or 1024 (threads per CTA the kernels are bounded for)
 //   JXB_INST_FN   the name of the selector it defines (declared in jxb_sim_kernels.cuh)
 // so that the instantiations compile in parallel.
 #include "jxb_sim_kernels.cuh"

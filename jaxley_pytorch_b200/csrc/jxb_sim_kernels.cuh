@@ -1286,6 +1286,7 @@ SimKernel sim_kernel_f32_fwd_256(bool gm, bool multi, bool wide);
 SimKernel sim_kernel_f32_fwd_512(bool gm, bool multi, bool wide);
 SimKernel sim_kernel_f32_fwd_1024(bool gm, bool multi, bool wide);
 SimKernel sim_kernel_f32_bwd_256(bool gm, bool multi, bool wide);
+SimKernel sim_kernel_f32_bwd_384(bool gm, bool multi, bool wide);
 SimKernel sim_kernel_f32_bwd_512(bool gm, bool multi, bool wide);
 SimKernel sim_kernel_f32_bwd_1024(bool gm, bool multi, bool wide);
 SimKernel sim_kernel_f64_fwd_256(bool gm, bool multi, bool wide);

@@ -109,3 +109,22 @@ def test_forward_launch_shape_does_not_change_results(cuda_device, dtype):
     assert torch.equal(r0, r1)
     scale = g0.abs().max().item()
     assert (g0 - g1).abs().max().item() <= 1e-12 * scale
+
+
+@pytest.mark.parametrize("dtype", [torch.float64, torch.float32])
+def test_adjoint_cta_sizes_agree(cuda_device, dtype):
+    """The adjoint at 384 threads (float: the kernels bounded for two 12-warp CTAs per
+    SM with up to 80 registers) gives the 512-thread launch's gradients: the CTA size
+    only changes which thread handles which node."""
+    prob = synth.config_uneven(n_cells=16, n_steps=60, max_comp=400, seed=9)
+    low = lower(prob, max_block_nodes=512, keep_currents=False)
+    runs = []
+    for th in (512, 384):
+        sim = Simulation(prob, low=low, dtype=dtype, device=cuda_device, checkpoint=25, threads=th,
+                         forward_threads=256)
+        assert sim.model.kind_threads["backward"] == th
+        runs.append(_grad_run(sim, 60))
+    torch.cuda.synchronize()
+    (r0, g0), (r1, g1) = runs
+    assert torch.equal(r0, r1)
+    assert (g0 - g1).abs().max().item() <= 1e-12 * g0.abs().max().item()
