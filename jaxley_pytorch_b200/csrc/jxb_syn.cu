@@ -81,29 +81,37 @@ __device__ __forceinline__ SynC<T> load_syn(const JxbSynArgs& a, const SynP<T>& 
   return c;
 }
 
-// Forward of one synapse and row (synapses/kinetic.py:37-63, sigmoid_rate.py:43-50,
-// the slope and offset of kernels/synapse_step.py:150-180): the new kinetic state,
-// the current i0 at vp and the slope vt / offset d0 - vt vp in uA/cm^2.
+// Forward of one synapse and row (synapses/kinetic.py:37-63, sigmoid_rate.py:43-50):
+// the new kinetic state, the current i0 at vp, and the synapse's terms of the
+// target's slope and offset in uA/cm^2 (kernels/synapse_step.py:150-180 take them as
+// the finite difference of the current over `diff` and its value less slope x vp).
+// The kinetic current gS s (v - e_syn) is linear in v: its slope is exactly
+// gS s 1e5 / area and its offset -slope e_syn, which is what the finite difference
+// evaluates to up to rounding (here without the float32 cancellation of a 1e-3 mV
+// difference of two currents of tens of mV). The rate synapse keeps the reference's
+// difference quotient.
 template <typename T>
 __device__ __forceinline__ void syn_forward_one(int model, const SynC<T>& c, T s, T vpre, T vp, T dt, T diff,
-                                                T& s_new, T& i0, T& vt, T& d0) {
-  T i1;
+                                                T& s_new, T& i0, T& lin_t, T& cst_t) {
   if (model == 0) {
     const T tr = sigm(qdiv<T>(vpre - c.q4, c.q5));
     const T aa = c.q2 * tr;
     const T rate = aa + c.q3;
     const T s_inf = qdiv<T>(aa, rate);
     s_new = s_inf + (s - s_inf) * ex(-dt * rate);
-    i0 = c.gs * s_new * (vp - c.q1);
-    i1 = c.gs * s_new * ((vp + diff) - c.q1);
+    const T gsn = c.gs * s_new;
+    i0 = gsn * (vp - c.q1);
+    lin_t = qdiv<T>(gsn, c.ar) * T(100000.0);
+    cst_t = -lin_t * c.q1;
   } else {
     s_new = T(0);
     i0 = -c.gs * sigm((vpre - c.q1) * c.q2);
-    i1 = -c.gs * sigm(((vpre + diff) - c.q1) * c.q2);
+    const T i1 = -c.gs * sigm(((vpre + diff) - c.q1) * c.q2);
+    const T d0 = qdiv<T>(i0, c.ar) * T(100000.0);
+    const T d1 = qdiv<T>(i1, c.ar) * T(100000.0);
+    lin_t = qdiv<T>(d1 - d0, diff);
+    cst_t = d0 - lin_t * vp;
   }
-  d0 = qdiv<T>(i0, c.ar) * T(100000.0);
-  const T d1 = qdiv<T>(i1, c.ar) * T(100000.0);
-  vt = qdiv<T>(d1 - d0, diff);
 }
 
 // Adjoint of one synapse and row (kernels/synapse_step.py:256-305) given the
@@ -114,54 +122,49 @@ template <typename T>
 __device__ __forceinline__ void syn_backward_one(int model, const SynC<T>& c, T s, T vpre, T vp, T dt, T diff,
                                                  T glin, T gconst, T g_sn_in, T g_cur, T (&gp)[6], T& g_s,
                                                  T& g_vp, T& g_vpre) {
-  T i0, i1, w0 = T(0), w1 = T(0), s_new = T(0), tr = T(0), rate = T(1), s_inf = T(0), decay = T(0),
-           x = T(0), u0 = T(0), u1 = T(0), sig0 = T(0), sig1 = T(0);
   if (model == 0) {
-    x = qdiv<T>(vpre - c.q4, c.q5);
-    tr = sigm(x);
+    // slope K gS s_new and offset -K gS s_new e_syn (K = 1e5 / area), current
+    // gS s_new (vp - e_syn): the target voltage enters through the current only.
+    const T x = qdiv<T>(vpre - c.q4, c.q5);
+    const T tr = sigm(x);
     const T aa = c.q2 * tr;
-    rate = aa + c.q3;
-    s_inf = qdiv<T>(aa, rate);
-    decay = ex(-dt * rate);
-    s_new = s_inf + (s - s_inf) * decay;
-    w0 = vp - c.q1;
-    w1 = (vp + diff) - c.q1;
-    i0 = c.gs * s_new * w0;
-    i1 = c.gs * s_new * w1;
-  } else {
-    u0 = vpre - c.q1;
-    u1 = (vpre + diff) - c.q1;
-    sig0 = sigm(u0 * c.q2);
-    sig1 = sigm(u1 * c.q2);
-    i0 = -c.gs * sig0;
-    i1 = -c.gs * sig1;
-  }
-  const T d0 = qdiv<T>(i0, c.ar) * T(100000.0);
-  const T d1 = qdiv<T>(i1, c.ar) * T(100000.0);
-  const T vt = qdiv<T>(d1 - d0, diff);
-  const T g_vt = glin - gconst * vp;
-  g_vp = -gconst * vt;
-  const T g_d1 = qdiv<T>(g_vt, diff);
-  const T g_d0 = gconst - g_d1;
-  const T g_i0 = qdiv<T>(g_d0 * T(100000.0), c.ar) + g_cur;
-  const T g_i1 = qdiv<T>(g_d1 * T(100000.0), c.ar);
-  if (model == 0) {
-    const T g_w = g_i0 * w0 + g_i1 * w1;
-    const T g_sn = c.gs * g_w + g_sn_in;
-    g_vp += c.gs * s_new * (g_i0 + g_i1);
+    const T rate = aa + c.q3;
+    const T s_inf = qdiv<T>(aa, rate);
+    const T decay = ex(-dt * rate);
+    const T s_new = s_inf + (s - s_inf) * decay;
+    const T K = qdiv<T>(T(100000.0), c.ar);
+    const T w0 = vp - c.q1;
+    const T g_c = (glin - gconst * c.q1) * K + g_cur * w0;  // d loss / d (gS s_new)
+    const T g_sn = c.gs * g_c + g_sn_in;
+    g_vp = g_cur * c.gs * s_new;
     const T g_sinf = g_sn * (T(1) - decay);
     const T g_rate = -dt * decay * g_sn * (s - s_inf) - qdiv<T>(g_sinf * s_inf, rate);
     const T g_a = qdiv<T>(g_sinf, rate) + g_rate;
     const T g_x = g_a * c.q2 * tr * (T(1) - tr);
     g_vpre = qdiv<T>(g_x, c.q5);
     g_s = g_sn * decay;
-    gp[0] += s_new * g_w;
-    gp[1] += -c.gs * s_new * (g_i0 + g_i1);
+    gp[0] += s_new * g_c;
+    gp[1] += -c.gs * s_new * (gconst * K + g_cur);
     gp[2] += g_a * tr;
     gp[3] += g_rate;
     gp[4] += -g_vpre;
     gp[5] += -g_vpre * x;
   } else {
+    const T u0 = vpre - c.q1;
+    const T u1 = (vpre + diff) - c.q1;
+    const T sig0 = sigm(u0 * c.q2);
+    const T sig1 = sigm(u1 * c.q2);
+    const T i0 = -c.gs * sig0;
+    const T i1 = -c.gs * sig1;
+    const T d0 = qdiv<T>(i0, c.ar) * T(100000.0);
+    const T d1 = qdiv<T>(i1, c.ar) * T(100000.0);
+    const T vt = qdiv<T>(d1 - d0, diff);
+    const T g_vt = glin - gconst * vp;
+    g_vp = -gconst * vt;
+    const T g_d1 = qdiv<T>(g_vt, diff);
+    const T g_d0 = gconst - g_d1;
+    const T g_i0 = qdiv<T>(g_d0 * T(100000.0), c.ar) + g_cur;
+    const T g_i1 = qdiv<T>(g_d1 * T(100000.0), c.ar);
     const T g_z0 = -c.gs * g_i0 * sig0 * (T(1) - sig0);
     const T g_z1 = -c.gs * g_i1 * sig1 * (T(1) - sig1);
     g_vpre = (g_z0 + g_z1) * c.q2;
@@ -222,12 +225,12 @@ __global__ void __launch_bounds__(32 * kFwdWarps) syn_forward_kernel(JxbSynArgs 
         const int kk = kb + u * L;
         if (kk >= a.k) break;
         const int64_t e = (int64_t)tgt * a.k + kk;
-        T s_new, i0, vt, d0;
-        syn_forward_one<T>(a.model, y[u], sv[u], vv[u], vp, dt, diff, s_new, i0, vt, d0);
+        T s_new, i0, lt, ct;
+        syn_forward_one<T>(a.model, y[u], sv[u], vv[u], vp, dt, diff, s_new, i0, lt, ct);
         if (sn_row) sn_row[e] = s_new;
         if (a.store_current) ((T*)a.current)[b * a.n_syn + e] = i0;
-        lin += vt;
-        cst += d0 - vt * vp;
+        lin += lt;
+        cst += ct;
       }
     }
   }
