@@ -9,8 +9,8 @@
 // synapses in registers and combine them with log2(L) shuffles. No shared-memory
 // reductions and no block barriers in the forward.
 //
-// forward:  warps over batch rows (4 per CTA, the same targets, so that the
-//           parameters are reused from L1), 32 / L targets per warp.
+// forward:  32 / L targets per warp, 4 rows per warp (the synapse constants loaded
+//           once for them), 4 warps per CTA over further rows.
 // backward: one CTA per group of 32 / L targets (one target once k > 32) with 8
 //           warps over the batch rows (each warp up to kRowsPerWarp rows per pass). Per synapse chunk (one
 //           value of i in c + i L) the parameter gradients are summed over the
@@ -183,7 +183,8 @@ __device__ __forceinline__ T group_sum(T v) {
   return v;
 }
 
-constexpr int kFwdWarps = 4;      // batch rows per forward CTA
+constexpr int kFwdWarps = 4;      // warps per forward CTA
+constexpr int kFwdRows = 4;       // batch rows of a forward warp
 constexpr int kFwdBatch = 4;      // synapses of a lane loaded together in the forward
 constexpr int kBwdWarps = 8;      // warps per backward CTA
 constexpr int kRowsPerWarp = 4;   // rows of a backward warp per pass
@@ -195,50 +196,67 @@ __global__ void __launch_bounds__(32 * kFwdWarps) syn_forward_kernel(JxbSynArgs 
   const int c = lane & (L - 1);
   const int nt = a.n_syn / a.k;
   const int tgt = blockIdx.x * TPW + lane / L;
-  const int64_t b = (int64_t)blockIdx.y * kFwdWarps + warp;
-  const bool ok = tgt < nt && b < a.batch;
+  // the warp's rows: b0, b0 + 1, ..., b0 + kFwdRows - 1 (the synapse constants are
+  // loaded once for all of them)
+  const int64_t b0 = ((int64_t)blockIdx.y * kFwdWarps + warp) * kFwdRows;
+  const bool ok = tgt < nt && b0 < a.batch;
+  const int nr = ok ? (int)min((int64_t)kFwdRows, (int64_t)a.batch - b0) : 0;
   const T* sc = (const T*)a.scalars;
   const T dt = sc[0], diff = sc[1];
-  T lin = T(0), cst = T(0);
+  T lin[kFwdRows], cst[kFwdRows], vp[kFwdRows];
+  const int node = ok ? (a.targets_are_nodes ? tgt : a.targets[tgt]) : 0;
+#pragma unroll
+  for (int r = 0; r < kFwdRows; ++r) {
+    lin[r] = cst[r] = T(0);
+    vp[r] = r < nr ? rd((const T*)a.v + (b0 + r) * a.n_nodes + node) : T(0);
+  }
   if (ok) {
-    const int node = a.targets_are_nodes ? tgt : a.targets[tgt];
-    const T* v = (const T*)a.v + b * a.n_nodes;
-    const T vp = rd(v + node);
-    const T* s_row = a.model == 0 ? (const T*)a.s + b * a.n_syn : nullptr;
-    T* sn_row = a.model == 0 ? (T*)a.s_new + b * a.n_syn : nullptr;
-    // kFwdBatch synapses of the lane at a time: all their loads first (indices
-    // clamped to the target's range), then the presynaptic voltages, then the
-    // arithmetic, so that a warp keeps that many independent loads in flight.
+    // kFwdBatch synapses of the lane at a time: their constants (indices clamped to
+    // the target's range), then per row the states and presynaptic voltages of all
+    // of them, then the arithmetic, so that a warp keeps many independent loads in
+    // flight.
     for (int kb = c; kb < a.k; kb += kFwdBatch * L) {
       SynC<T> y[kFwdBatch];
-      T sv[kFwdBatch], vv[kFwdBatch];
+      int64_t e[kFwdBatch];
 #pragma unroll
       for (int u = 0; u < kFwdBatch; ++u) {
-        const int64_t e = (int64_t)tgt * a.k + min(kb + u * L, a.k - 1);
-        y[u] = load_syn<T>(a, P, e);
-        sv[u] = s_row ? rd(s_row + e) : T(0);
+        e[u] = (int64_t)tgt * a.k + min(kb + u * L, a.k - 1);
+        y[u] = load_syn<T>(a, P, e[u]);
       }
 #pragma unroll
-      for (int u = 0; u < kFwdBatch; ++u) vv[u] = rd(v + y[u].pre);
+      for (int r = 0; r < kFwdRows; ++r) {
+        if (r >= nr) break;
+        const int64_t b = b0 + r;
+        const T* v = (const T*)a.v + b * a.n_nodes;
+        const T* s_row = a.model == 0 ? (const T*)a.s + b * a.n_syn : nullptr;
+        T* sn_row = a.model == 0 ? (T*)a.s_new + b * a.n_syn : nullptr;
+        T sv[kFwdBatch], vv[kFwdBatch];
 #pragma unroll
-      for (int u = 0; u < kFwdBatch; ++u) {
-        const int kk = kb + u * L;
-        if (kk >= a.k) break;
-        const int64_t e = (int64_t)tgt * a.k + kk;
-        T s_new, i0, lt, ct;
-        syn_forward_one<T>(a.model, y[u], sv[u], vv[u], vp, dt, diff, s_new, i0, lt, ct);
-        if (sn_row) sn_row[e] = s_new;
-        if (a.store_current) ((T*)a.current)[b * a.n_syn + e] = i0;
-        lin += lt;
-        cst += ct;
+        for (int u = 0; u < kFwdBatch; ++u) {
+          sv[u] = s_row ? rd(s_row + e[u]) : T(0);
+          vv[u] = rd(v + y[u].pre);
+        }
+#pragma unroll
+        for (int u = 0; u < kFwdBatch; ++u) {
+          if (kb + u * L >= a.k) break;
+          T s_new, i0, lt, ct;
+          syn_forward_one<T>(a.model, y[u], sv[u], vv[u], vp[r], dt, diff, s_new, i0, lt, ct);
+          if (sn_row) sn_row[e[u]] = s_new;
+          if (a.store_current) ((T*)a.current)[b * a.n_syn + e[u]] = i0;
+          lin[r] += lt;
+          cst[r] += ct;
+        }
       }
     }
   }
-  lin = group_sum<L>(lin);
-  cst = group_sum<L>(cst);
-  if (ok && c == 0) {
-    ((T*)a.lin)[b * nt + tgt] = lin;
-    ((T*)a.cst)[b * nt + tgt] = cst;
+#pragma unroll
+  for (int r = 0; r < kFwdRows; ++r) {
+    const T l = group_sum<L>(lin[r]);
+    const T q = group_sum<L>(cst[r]);
+    if (c == 0 && r < nr) {
+      ((T*)a.lin)[(b0 + r) * nt + tgt] = l;
+      ((T*)a.cst)[(b0 + r) * nt + tgt] = q;
+    }
   }
 }
 
@@ -318,11 +336,13 @@ __global__ void __launch_bounds__(32 * kBwdWarps) syn_backward_kernel(JxbSynArgs
           out = (a.accumulate || b0 > 0) ? out + acc : acc;
         }
       }
-      // Presynaptic voltage gradients of the chunk, row-contiguous per synapse.
-      for (int w = threadIdx.x; w < 32 * nr; w += blockDim.x) {
-        const int ln = w / nr, r = w - ln * nr;
+      // Presynaptic voltage gradients of the chunk, row-contiguous per synapse (a
+      // warp writes one synapse's rows of the pass).
+      static_assert(RP == 32, "one warp per synapse row of the tile");
+      for (int w = threadIdx.x; w < 32 * 32; w += blockDim.x) {
+        const int ln = w >> 5, r = w & 31;
         const int t2 = blockIdx.x * TPW + ln / L, k2 = i * L + (ln & (L - 1));
-        if (t2 < nt && k2 < a.k) g_pre[((int64_t)t2 * a.k + k2) * a.batch + b0 + r] = tile[ln * RP + r];
+        if (r < nr && t2 < nt && k2 < a.k) g_pre[((int64_t)t2 * a.k + k2) * a.batch + b0 + r] = tile[ln * RP + r];
       }
       __syncthreads();
     }
@@ -407,7 +427,8 @@ int fwd(const JxbSynArgs& a, cudaStream_t st) {
   for (int q = 0; q < 6; ++q) P.p[q] = (const T*)a.p[q];
   const int nt = a.n_syn / a.k;
   const int L = syn_lanes(a.k);
-  const dim3 grid((unsigned)((nt + 32 / L - 1) / (32 / L)), (unsigned)((a.batch + kFwdWarps - 1) / kFwdWarps));
+  const int rows_per_cta = kFwdWarps * kFwdRows;
+  const dim3 grid((unsigned)((nt + 32 / L - 1) / (32 / L)), (unsigned)((a.batch + rows_per_cta - 1) / rows_per_cta));
   const int th = 32 * kFwdWarps;
   switch (L) {
     case 1: syn_forward_kernel<T, 1><<<grid, th, 0, st>>>(a, P); break;
