@@ -203,7 +203,11 @@ class NetworkSimulation:
         stored = keep and self.stores_trajectory(T)
         saved = None
         if keep:
-            saved = {"states": self._zeros(T, B, low.n_slots), "stored": stored}
+            # every step's state (before it, and after the last) and the reciprocal
+            # pivots of its solve: the one-step adjoint launches read them instead of
+            # recomputing the step
+            saved = {"states": self._zeros(T + 1, B, low.n_slots), "piv": self._zeros(T, B, low.n_nodes),
+                     "stored": stored}
             if stored:  # every step's kinetic states, slopes and offsets
                 saved["s_traj"] = [self._zeros(T + 1, B, ty.E) if ty.kinetic else None for ty in self.types]
                 saved["lin"] = self._zeros(T, self.syn_size)
@@ -230,8 +234,9 @@ class NetworkSimulation:
                         saved["s_ckpt"][q][t // K].copy_(s_cur[q])
             for q, ty in enumerate(self.types):
                 self._syn_forward(ty, q, state, s_cur[q], s_nxt[q], lin, cst, syn_params[q])
-            a = m.args(state, 1, t, rec, pscale=pscale, ckpt=saved["states"] if keep else None,
-                       ckpt_every=1 if keep else 0)
+            a = m.args(state, 1, t, rec, pscale=pscale, traj=saved["states"][t] if keep else None)
+            if keep:
+                a.traj_piv = saved["piv"][t].data_ptr()
             self._set_syn(a, lin, cst)
             m.launch_forward(a)
             if not stored:
@@ -247,8 +252,6 @@ class NetworkSimulation:
         K = self.checkpoint
         adj = self._zeros(B, low.n_slots)
         pgrad = self._zeros(B, low.n_cols, dtype=torch.float64)
-        traj = self._zeros(1, B, low.n_slots)
-        piv = self._zeros(1, B, low.n_nodes)
         if not saved["stored"]:
             LC_lin = self._zeros(K, self.syn_size)
             LC_cst = self._zeros(K, self.syn_size)
@@ -284,10 +287,11 @@ class NetworkSimulation:
                                           syn_params[q])
             for i in range(k - 1, -1, -1):
                 t = t0 + i
-                a = m.args(states[t], 1, t, None, pscale=pscale, traj=traj, adj=adj, rec_grad=rec_grad,
+                a = m.args(states[t], 1, t, None, pscale=pscale, traj=states[t], adj=adj, rec_grad=rec_grad,
                            pgrad=pgrad)
                 a.ckpt = states[t].data_ptr()
-                a.traj_piv = piv.data_ptr()
+                a.traj_piv = saved["piv"][t].data_ptr()
+                a.traj_stored = 1
                 self._set_syn(a, LC_lin[i], LC_cst[i])
                 a.g_syn_lin = g_lin.data_ptr()
                 a.g_syn_const = g_cst.data_ptr()
