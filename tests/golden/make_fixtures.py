@@ -39,16 +39,18 @@ from jaxley_pytorch.synapses import KineticSynapse, SigmoidRateSynapse  # noqa: 
 from jaxley_pytorch_b200.problem import load_problem, problem_from_module, save_problem  # noqa: E402
 
 
-def golden_arrays(test_file: str, func: str) -> np.ndarray:
-    """The `voltages_081123` literal of a test function of the reference."""
+def golden_arrays(test_file: str, func: str, var: str = "voltages_081123", index: int = 0) -> np.ndarray:
+    """The `index`-th `var = np.asarray(<literal>)` of a test function of the
+    reference (its golden trace), read from the source text."""
     tree = ast.parse(open(test_file).read())
     for node in ast.walk(tree):
         if isinstance(node, ast.FunctionDef) and node.name == func:
-            for sub in ast.walk(node):
-                if (isinstance(sub, ast.Assign) and isinstance(sub.targets[0], ast.Name)
-                        and sub.targets[0].id == "voltages_081123"):
-                    call = sub.value
-                    return np.asarray(ast.literal_eval(call.args[0]), dtype=np.float64)
+            found = [sub for sub in ast.walk(node)
+                     if isinstance(sub, ast.Assign) and isinstance(sub.targets[0], ast.Name)
+                     and sub.targets[0].id == var]
+            found.sort(key=lambda sub: sub.lineno)
+            call = found[index].value
+            return np.asarray(ast.literal_eval(call.args[0]), dtype=np.float64)
     raise KeyError(func)
 
 
@@ -161,6 +163,58 @@ def golden_cases():
     branch.loc(0.0).record()
     branch.loc(0.0).stimulate(current)
     save("golden_branch", branch, delta_t=0.025, extra={"golden": g, "every": 20})
+    # test_cell: SimpleCell(3, 2) (branch parents of tests/conftest.py:24-31), HH
+    g = golden_arrays(test_file, "test_cell", "voltages_300724")
+    cell = jx.Cell([jx.Branch([jx.Compartment()] * 2)] * 3, parents=binary_parents(3))
+    cell.insert(HH())
+    cell.branch(1).loc(0.0).record()
+    cell.branch(1).loc(0.0).stimulate(current)
+    save("golden_cell_3x2", cell, delta_t=0.025, extra={"golden": g, "every": 20})
+    # test_branch_uneven_radiuses, backward Euler (its second trace; tolerance 1e-5)
+    g = golden_arrays(test_file, "test_branch_uneven_radiuses", "voltages_240920", index=1)
+    current2 = jx.step_current(i_delay=0.5, i_dur=1.0, i_amp=2.0, delta_t=0.025, t_max=10.0)
+    branch = jx.Branch([jx.Compartment()] * 8)
+    branch.set("axial_resistivity", 500.0)
+    branch.set("length", np.linspace(20, 300, 8))
+    branch.set("radius", np.linspace(1, 5, 8))
+    branch.insert(HH())
+    branch.loc(1.0).stimulate(current2)
+    branch.loc(0.0).record()
+    save("golden_branch_uneven_radiuses", branch, delta_t=0.025,
+         extra={"golden": g[None] if g.ndim == 1 else g, "every": 50, "tol": 1e-5})
+    # tests/jaxley_identical/test_radius_and_length.py: the same inputs (numpy's
+    # generator seeded with 1, as there) and its golden traces
+    rl_file = os.path.join(REFERENCE, "tests", "jaxley_identical", "test_radius_and_length.py")
+    g = golden_arrays(rl_file, "test_radius_and_length_compartment")
+    comp = jx.Compartment()
+    np.random.seed(1)
+    comp.set("length", 5 * np.random.rand(1))
+    comp.set("radius", np.random.rand(1))
+    comp.insert(HH())
+    comp.record()
+    comp.stimulate(current)
+    save("golden_radius_length_comp", comp, delta_t=0.025, extra={"golden": g, "every": 20})
+    g = golden_arrays(rl_file, "test_radius_and_length_branch", "voltages_300724")
+    branch = jx.Branch([jx.Compartment()] * 2)
+    np.random.seed(1)
+    branch.set("length", np.flip(5 * np.random.rand(2)))
+    branch.set("radius", np.flip(np.random.rand(2)))
+    branch.insert(HH())
+    branch.loc(0.0).record()
+    branch.loc(0.0).stimulate(current)
+    save("golden_radius_length_branch", branch, delta_t=0.025, extra={"golden": g, "every": 20})
+    g = golden_arrays(rl_file, "test_radius_and_length_cell", "voltages_300724")
+    cell = jx.Cell([jx.Branch([jx.Compartment()] * 2)] * 3, parents=binary_parents(3))
+    np.random.seed(1)
+    rands1 = 5 * np.random.rand(6)
+    rands2 = np.random.rand(6)
+    for b in range(3):
+        cell.branch(b).set("length", np.flip(rands1[2 * b:2 * b + 2]))
+        cell.branch(b).set("radius", np.flip(rands2[2 * b:2 * b + 2]))
+    cell.insert(HH())
+    cell.branch(1).loc(0.0).record()
+    cell.branch(1).loc(0.0).stimulate(current)
+    save("golden_radius_length_cell", cell, delta_t=0.025, extra={"golden": g, "every": 20})
 
 
 def config_small():

@@ -9,11 +9,14 @@ from conftest import fixture_names, load_fixture
 
 @pytest.mark.parametrize("name", fixture_names("golden_"))
 def test_oracle_matches_reference_golden_vectors(name):
-    # tests/jaxley_identical/test_basic_modules.py:25-122: max abs error <= 1e-8.
+    # tests/jaxley_identical/test_basic_modules.py:25-122, 125-243: max abs error
+    # <= 1e-8 (1e-5 for the uneven radii, as there).
     prob, extra = load_fixture(name)
     out = oracle.integrate(prob)
     every = int(extra["every"])
-    assert np.max(np.abs(out[0, :, ::every] - extra["golden"])) <= 1e-8
+    tol = float(extra["tol"]) if "tol" in extra else 1e-8
+    golden = extra["golden"].reshape(out[0, :, ::every].shape)
+    assert np.max(np.abs(out[0, :, ::every] - golden)) <= tol
 
 
 @pytest.mark.parametrize("name", fixture_names())
