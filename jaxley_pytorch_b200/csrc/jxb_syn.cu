@@ -264,10 +264,12 @@ template <typename T, int L>
 __global__ void __launch_bounds__(32 * kBwdWarps) syn_backward_kernel(JxbSynArgs a, SynP<T> P) {
   constexpr int TPW = 32 / L;
   constexpr int RP = kBwdWarps * kRowsPerWarp;  // rows per pass
-  // red[warp][lane][param]: the warps' parameter gradients of the current chunk;
-  // tile[lane][row of the pass]: its presynaptic voltage gradients.
-  __shared__ T red[kBwdWarps * 32 * 6];
-  __shared__ T tile[32 * RP];
+  // red[warp][lane][param]: the warps' parameter gradients of a chunk;
+  // tile[lane][row of the pass]: its presynaptic voltage gradients. Two of each,
+  // alternating by chunk: a chunk's sums and stores read one pair while the next
+  // chunk's arithmetic fills the other, so one barrier per chunk separates them.
+  __shared__ T red_buf[2][kBwdWarps * 32 * 6];
+  __shared__ T tile_buf[2][32 * RP];
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int c = lane & (L - 1);
   const int nt = a.n_syn / a.k;
@@ -296,6 +298,8 @@ __global__ void __launch_bounds__(32 * kBwdWarps) syn_backward_kernel(JxbSynArgs
       vp[m] = row ? rd((const T*)a.v + b * a.n_nodes + node) : T(0);
     }
     for (int i = 0; i < J; ++i) {
+      T* const red = red_buf[i & 1];
+      T* const tile = tile_buf[i & 1];
       const int kk = i * L + c;
       const bool act = tok && kk < a.k;
       const int64_t e = (int64_t)(tok ? tgt : 0) * a.k + (act ? kk : 0);
@@ -344,8 +348,8 @@ __global__ void __launch_bounds__(32 * kBwdWarps) syn_backward_kernel(JxbSynArgs
         const int t2 = blockIdx.x * TPW + ln / L, k2 = i * L + (ln & (L - 1));
         if (r < nr && t2 < nt && k2 < a.k) g_pre[((int64_t)t2 * a.k + k2) * a.batch + b0 + r] = tile[ln * RP + r];
       }
-      __syncthreads();
     }
+    __syncthreads();  // the last chunks' buffers are read before the next pass writes them
     // The target-voltage gradient of every (row, target): added to g_v here when
     // accumulating (one lane group owns the pair), else by syn_post_kernel.
 #pragma unroll
