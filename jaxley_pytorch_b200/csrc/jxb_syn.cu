@@ -185,12 +185,14 @@ __device__ __forceinline__ T group_sum(T v) {
 
 constexpr int kFwdWarps = 4;      // warps per forward CTA
 constexpr int kFwdRows = 4;       // batch rows of a forward warp
-constexpr int kFwdBatch = 4;      // synapses of a lane loaded together in the forward
+constexpr int kFwdBatch = 2;      // synapses of a lane loaded together in the forward
 constexpr int kBwdWarps = 8;      // warps per backward CTA
 constexpr int kRowsPerWarp = 4;   // rows of a backward warp per pass
 
+// float: at most 64 registers, so that eight CTAs (32 warps) per SM keep more gathers
+// in flight than wider batches of loads per thread with fewer warps would.
 template <typename T, int L>
-__global__ void __launch_bounds__(32 * kFwdWarps) syn_forward_kernel(JxbSynArgs a, SynP<T> P) {
+__global__ void __launch_bounds__(32 * kFwdWarps, sizeof(T) == 4 ? 8 : 4) syn_forward_kernel(JxbSynArgs a, SynP<T> P) {
   constexpr int TPW = 32 / L;  // targets per warp
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   const int c = lane & (L - 1);
