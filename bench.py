@@ -392,9 +392,13 @@ def run_uneven(args, device):
     T = args.uneven_tsteps
     prob = synth.config_uneven(n_cells=args.uneven_cells, n_steps=T)
     n_comp = int(len(prob.comp_inds))
+    wide = dict(forward_threads=args.forward_threads, forward_wide=args.forward_threads <= 256)
+    # the probes run the forward at its own launch shape, as the tuned run does, so
+    # that `threads` decides the adjoint's CTA size only
     choice, low, table = autotune(prob, dtype=torch.float32, device=device, probe_steps=40,
                                   block_nodes=(1024, 2048), threads=(256, 512), rows=(1,),
-                                  checkpoints=(50, 100, 200), horizon=T, reps=1)
+                                  checkpoints=(50, 100, 200), horizon=T, reps=2,
+                                  sim_kwargs=dict(wide, store_fraction=0.6))
 
     def timed(fn, reps):
         fn()
@@ -410,7 +414,6 @@ def run_uneven(args, device):
     def loss_of(target):
         return lambda rec: ((rec - target) ** 2).mean()
 
-    wide = dict(forward_threads=args.forward_threads, forward_wide=args.forward_threads <= 256)
     sim = Simulation(prob, low=low, dtype=torch.float32, device=device, threads=choice.threads,
                      rows_per_item=choice.rows_per_item, checkpoint=choice.checkpoint,
                      store_fraction=0.6, **wide)

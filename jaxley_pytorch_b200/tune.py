@@ -5,9 +5,13 @@ threads per CTA (warps per block of trees), batch rows per work item, and the
 checkpoint interval of the adjoint (steps recomputed per backward launch, traded
 against the memory of the stored states and trajectories). Each candidate is timed
 on a short horizon of the actual problem with CUDA events (forward + adjoint when
-`grad`, forward only otherwise); the fastest wins. Candidates that the launcher
-rejects (sizes) or that exceed the memory budget are skipped. Results are cached per
-problem signature in-process and, with `cache_path`, in a JSON file.
+`grad`, forward only otherwise), each timed run separately after a warm-up run, the
+shortest run counting (a run that host work or another process slowed down does not
+decide); the fastest candidate wins. `sim_kwargs` (for example the forward's own
+launch shape) go to every probe `Simulation`, so that a probe runs what the tuned run
+will. Candidates that the launcher rejects (sizes) or that exceed the memory budget
+are skipped. Results are cached per problem signature in-process and, with
+`cache_path`, in a JSON file.
 """
 from __future__ import annotations
 
@@ -77,12 +81,14 @@ def _time(sim: Simulation, T: int, grad: bool, reps: int) -> float:
     torch.cuda.synchronize(sim.model.device)
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
-    e0.record()
-    for _ in range(reps):
+    best = float("inf")
+    for _ in range(max(1, reps)):
+        e0.record()
         once()
-    e1.record()
-    torch.cuda.synchronize(sim.model.device)
-    return e0.elapsed_time(e1) / reps / T
+        e1.record()
+        torch.cuda.synchronize(sim.model.device)
+        best = min(best, e0.elapsed_time(e1))
+    return best / T
 
 
 def autotune(problem: Problem, dtype: torch.dtype = torch.float32, device="cuda", grad: bool = True,
@@ -91,6 +97,7 @@ def autotune(problem: Problem, dtype: torch.dtype = torch.float32, device="cuda"
              checkpoints: Sequence[int] = (50, 100, 200), horizon: Optional[int] = None,
              memory_budget: Optional[int] = None, keep_currents: bool = False,
              cache_path: Optional[str] = None, reps: int = 2,
+             sim_kwargs: Optional[dict] = None,
              verbose: bool = False) -> Tuple[Choice, Lowered, List[dict]]:
     """Returns `(choice, lowered model of the chosen block size, table of timings)`."""
     key = signature(problem, dtype, grad)
@@ -119,7 +126,7 @@ def autotune(problem: Problem, dtype: torch.dtype = torch.float32, device="cuda"
             for r in sorted({min(r, B) for r in rows}):
                 try:
                     sim = Simulation(problem, low=low, dtype=dtype, device=device, threads=th,
-                                     rows_per_item=r, checkpoint=Kp)
+                                     rows_per_item=r, checkpoint=Kp, **(sim_kwargs or {}))
                     ms = _time(sim, Kp, grad, reps)
                 except RuntimeError as e:  # sizes the launcher rejects
                     table.append({"max_block_nodes": mbn, "threads": th, "rows": r, "error": str(e)})
@@ -142,8 +149,8 @@ def autotune(problem: Problem, dtype: torch.dtype = torch.float32, device="cuda"
         timed = []
         for K in cands:
             sim = Simulation(problem, low=low, dtype=dtype, device=device, threads=th, rows_per_item=r,
-                             checkpoint=K)
-            msk = _time(sim, Tk, True, max(1, reps - 1))
+                             checkpoint=K, **(sim_kwargs or {}))
+            msk = _time(sim, Tk, True, reps)
             table.append({"checkpoint": K, "horizon": Tk, "ms_per_step": msk})
             if verbose:
                 print("tune", table[-1], flush=True)
