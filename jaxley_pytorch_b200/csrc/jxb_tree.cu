@@ -241,9 +241,11 @@ __global__ void tree_registers_kernel(const T* __restrict__ d, const T* __restri
 // rhs * upper / pivot) goes to shared memory once, on the level after its own
 // elimination, where its parent gathers it; the back-substitution passes the
 // parents' solutions through shared memory the same way. One barrier per height
-// and per depth level.
-template <typename T, int R>
-__global__ void __launch_bounds__(1024) tree_registers_cta_kernel(const T* __restrict__ d, const T* __restrict__ l,
+// and per depth level. A thread's off-diagonals and depths are loaded into registers
+// with its pivots and right-hand sides before the first level, so that no level
+// waits on a global load.
+template <typename T, int R, int MAXT>
+__global__ void __launch_bounds__(MAXT, 1) tree_registers_cta_kernel(const T* __restrict__ d, const T* __restrict__ l,
                                                                   const T* __restrict__ u, const T* __restrict__ s,
                                                                   T* __restrict__ x, JxbRegSchedule sc) {
   extern __shared__ __align__(16) char smem_raw[];
@@ -262,23 +264,26 @@ __global__ void __launch_bounds__(1024) tree_registers_cta_kernel(const T* __res
   const int* dep = sc.rel_depth + (size_t)blk * W;
   const int* kid = sc.rel_children + (size_t)blk * sc.num_slots * W;
   const int64_t base = row * sc.n_nodes + start;
-  T dv[R], sv[R];
-  int hv[R];
+  T dv[R], sv[R], lv[R], uv[R];
+  int hv[R], dp[R];
 #pragma unroll
   for (int r = 0; r < R; ++r) {
     const int j = tid + NT * r;
     const bool in = j < len;
     dv[r] = in ? d[base + j] : T(1);
     sv[r] = in ? s[base + j] : T(0);
+    lv[r] = in ? l[base + j] : T(0);
+    uv[r] = in ? u[base + j] : T(0);
     hv[r] = in ? hgt[j] : -1;
+    dp[r] = in ? dep[j] : -1;
   }
   for (int h = 1; h <= levels; ++h) {
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int j = tid + NT * r;
       if (hv[r] == h - 1) {  // eliminated on the previous level (leaves: height 0)
-        const T f = u[base + j] / dv[r];
-        A[j] = l[base + j] * f;
+        const T f = uv[r] / dv[r];
+        A[j] = lv[r] * f;
         Bv[j] = sv[r] * f;
       }
     }
@@ -302,9 +307,9 @@ __global__ void __launch_bounds__(1024) tree_registers_cta_kernel(const T* __res
 #pragma unroll
     for (int r = 0; r < R; ++r) {
       const int j = tid + NT * r;
-      if (j < len && dep[j] == k) {
+      if (dp[r] == k) {
         const T xp = k > 0 ? Bv[par[j]] : T(0);
-        sv[r] = (sv[r] - l[base + j] * xp) / dv[r];
+        sv[r] = (sv[r] - lv[r] * xp) / dv[r];
         Bv[j] = sv[r];
       }
     }
@@ -328,15 +333,17 @@ int launch_registers_cta(const void* d, const void* l, const void* u, const void
     snprintf(g_err, sizeof(g_err), "batch %lld exceeds the grid", (long long)batch);
     return JXB_ERR_ARG;
   }
-  cudaError_t e = cudaFuncSetAttribute(tree_registers_cta_kernel<T, R>,
-                                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  // up to 512 threads (blocks of up to 4096 nodes) with up to 128 registers, so that a
+  // thread's eight nodes stay in registers; 1024 threads at 64
+  void (*kern)(const T*, const T*, const T*, const T*, T*, JxbRegSchedule) =
+      threads <= 512 ? tree_registers_cta_kernel<T, R, 512> : tree_registers_cta_kernel<T, R, 1024>;
+  cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   if (e != cudaSuccess) {
     set_err("cudaFuncSetAttribute", e);
     return JXB_ERR_LAUNCH;
   }
   dim3 grid(sc.n_blocks, (unsigned)batch);
-  tree_registers_cta_kernel<T, R><<<grid, threads, smem, st>>>((const T*)d, (const T*)l, (const T*)u,
-                                                               (const T*)s, (T*)x, sc);
+  kern<<<grid, threads, smem, st>>>((const T*)d, (const T*)l, (const T*)u, (const T*)s, (T*)x, sc);
   e = cudaGetLastError();
   if (e != cudaSuccess) {
     set_err("tree_registers_cta_kernel", e);

@@ -32,7 +32,14 @@ from ..lower import block_schedule, chain_table
 from . import OP_NAMESPACE
 
 MAX_BLOCK = 8192  # registers variant: up to 256 nodes in one warp, larger blocks in a CTA
-LEVEL_BLOCK = 4096  # levels variant: nodes per block of trees (shared memory bound)
+LEVEL_BLOCK = 4096  # levels variant: largest block of trees (shared memory bound)
+# Levels variant: a forest of many small trees is cut into at least this many blocks
+# (one CTA per block and batch row), so that even a small batch fills the SMs; blocks
+# keep at least LEVEL_MIN_BLOCK nodes. Measured on 512 trees of 40 nodes x 32 rows:
+# blocks of 4096 / 1280 / 640 / 320 / 160 nodes took 36.3 / 27.7 / 22.0 / 19.9 /
+# 27.5 us per solve.
+LEVEL_MIN_BLOCKS = 64
+LEVEL_MIN_BLOCK = 256
 
 
 def _forest(parent: np.ndarray):
@@ -116,14 +123,18 @@ def build_forest_schedule(parent: np.ndarray, max_block: int = MAX_BLOCK) -> Dic
             "block_size": W, "regs_per_lane": regs, "num_slots": num_slots, "num_nodes": n}
 
 
-def build_level_schedule(parent: np.ndarray, block_nodes: int = LEVEL_BLOCK) -> Dict[str, np.ndarray]:
+def build_level_schedule(parent: np.ndarray, block_nodes: Optional[int] = None) -> Dict[str, np.ndarray]:
     """Schedule of the levels variant: trees packed into blocks of about
     `block_nodes` nodes (a larger tree gets its own block), each block's nodes in
-    chain order with its chains sorted by level (cf. reference `tree_solve.py:142-224`)."""
+    chain order with its chains sorted by level (cf. reference `tree_solve.py:142-224`).
+    By default a block holds up to LEVEL_BLOCK nodes, fewer (down to LEVEL_MIN_BLOCK)
+    when that leaves a forest in fewer than LEVEL_MIN_BLOCKS blocks."""
     parent, roots, ends = _forest(parent)
     n = len(parent)
     if int((ends - roots).max()) > 32767:
         raise ValueError("trees of more than 32767 nodes are not supported")
+    if block_nodes is None:
+        block_nodes = min(LEVEL_BLOCK, max(LEVEL_MIN_BLOCK, -(-n // LEVEL_MIN_BLOCKS)))
     order, tree_ptr, chains = chain_table(parent)
     blocks = _pack(roots, ends, block_nodes)
     # chain_table keeps the trees in order, so a block is the same range in both orders.
