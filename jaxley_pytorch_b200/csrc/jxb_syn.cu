@@ -299,13 +299,19 @@ __global__ void __launch_bounds__(32 * kBwdWarps) syn_backward_kernel(JxbSynArgs
       gconst[m] = row ? rd((const T*)a.g_const + b * nt + tgt) : T(0);
       vp[m] = row ? rd((const T*)a.v + b * a.n_nodes + node) : T(0);
     }
+    // The next chunk's synapse constants are loaded while the current chunk computes.
+    SynC<T> y_next = load_syn<T>(a, P, (int64_t)(tok ? tgt : 0) * a.k + ((tok && c < a.k) ? c : 0));
     for (int i = 0; i < J; ++i) {
       T* const red = red_buf[i & 1];
       T* const tile = tile_buf[i & 1];
       const int kk = i * L + c;
       const bool act = tok && kk < a.k;
       const int64_t e = (int64_t)(tok ? tgt : 0) * a.k + (act ? kk : 0);
-      SynC<T> y = load_syn<T>(a, P, e);
+      const SynC<T> y = y_next;
+      if (i + 1 < J) {
+        const int k1 = kk + L;
+        y_next = load_syn<T>(a, P, (int64_t)(tok ? tgt : 0) * a.k + ((tok && k1 < a.k) ? k1 : 0));
+      }
       T gp[6] = {T(0), T(0), T(0), T(0), T(0), T(0)};
 #pragma unroll
       for (int m = 0; m < kRowsPerWarp; ++m) {

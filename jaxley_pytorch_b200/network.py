@@ -114,9 +114,12 @@ class NetworkSimulation:
         if not problem.synapses:
             raise ValueError("the problem has no synapses (use Simulation)")
         self.problem = problem
+        # float32 cell steps of up to 256 threads use the forward kernels of two CTAs
+        # per SM with up to 128 registers
         self.sim = Simulation(problem, dtype=dtype, device=device, threads=threads, segment=1,
                               checkpoint=1, keep_currents=False, max_block_nodes=max_block_nodes,
-                              rows_per_item=rows_per_item)
+                              rows_per_item=rows_per_item,
+                              forward_wide=dtype == torch.float32 and threads <= 256)
         self.low = low = self.sim.low
         self.model = self.sim.model
         self.init_steady = bool(init_steady)  # channel gates start at their steady state
