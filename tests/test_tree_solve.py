@@ -70,12 +70,18 @@ def test_schedules_on_cpu():
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("mode", ["registers", "levels"])
+@pytest.mark.parametrize("mode", ["registers", "registers_warp", "levels"])
 @pytest.mark.parametrize("name", list(forests()))
 def test_tree_solve_matches_oracle(cuda_device, mode, name):
     parent = np.asarray(forests()[name])
-    kern = ts.make_tree_solve_kernel(parent, cuda_device, mode=mode)
-    assert isinstance(kern, ts.TreeSolveKernel if mode == "registers" else ts.LevelTreeSolveKernel)
+    if mode == "registers_warp":  # blocks of at most 256 nodes: one warp each
+        if max(np.diff(np.append(np.nonzero(parent < 0)[0], len(parent)))) > 256:
+            pytest.skip("a tree of more than 256 nodes")
+        kern = ts.TreeSolveKernel(ts.build_forest_schedule(parent, max_block=256), cuda_device)
+        assert kern.block_size <= 256
+    else:
+        kern = ts.make_tree_solve_kernel(parent, cuda_device, mode=mode)
+    assert isinstance(kern, ts.LevelTreeSolveKernel if mode == "levels" else ts.TreeSolveKernel)
     d, l, u, s = system(parent, 6, np.float64)
     ref = oracle.tree_solve(d, l, u, s, parent)
     for dtype, tol in [(torch.float64, 1e-12), (torch.float32, 1e-4)]:
