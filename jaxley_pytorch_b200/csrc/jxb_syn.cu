@@ -12,14 +12,14 @@
 // forward:  32 / L targets per warp, 4 rows per warp (the synapse constants loaded
 //           once for them), 4 warps per CTA over further rows.
 // backward: one CTA per group of 32 / L targets (two for k up to 128, one above)
-//           with 8 warps over the batch rows (each warp kRowsPerWarp rows per pass). Per synapse chunk (one
-//           value of i in c + i L) the parameter gradients are summed over the
-//           warp's rows in registers and over the warps in shared memory in a fixed
-//           order, and the presynaptic voltage gradients of the chunk are staged in
-//           shared memory and written to an (E, batch) buffer row-contiguously; a
-//           second kernel sums them per presynaptic node through the transposed
-//           index (four warps per node, each over a quarter of its synapses). No
-//           atomics, deterministic.
+//           with 8 warps over the batch rows (each warp kRowsPerWarp rows per
+//           pass). Per synapse chunk (one value of i in c + i L) the parameter
+//           gradients are summed over the warp's rows in registers and over the
+//           warps in shared memory in a fixed order, and the presynaptic voltage
+//           gradients of the chunk are staged in shared memory and written to an
+//           (E, batch) buffer row-contiguously; a second kernel sums them per
+//           presynaptic node through the transposed index (four warps per node,
+//           each over a quarter of its synapses). No atomics, deterministic.
 // float: fast reciprocal / division / exp (jxb_math.cuh); float64 stays exact.
 #include <cuda_runtime.h>
 #include <stdint.h>
