@@ -125,6 +125,28 @@ def test_tree_solve_gradcheck(cuda_device):
     assert torch.autograd.gradcheck(lambda *a: ts.fused_tree_solve(kern, *a), args)
 
 
+def test_default_block_sizes():
+    """Registers variant: blocks of at least REG_MIN_BLOCK nodes (a CTA each) unless a
+    tree is larger; levels variant: a forest of small trees in at least
+    LEVEL_MIN_BLOCKS blocks of at least LEVEL_MIN_BLOCK nodes."""
+    rng = np.random.default_rng(5)
+    forest = []
+    for _ in range(512):
+        b = len(forest)
+        forest += [-1] + [b + int(rng.integers(0, j)) for j in range(1, 40)]
+    forest = np.asarray(forest)
+    fs = ts.build_forest_schedule(forest)
+    assert fs["block_size"] == ts.REG_MIN_BLOCK
+    assert all(int(r[1]) <= ts.REG_MIN_BLOCK for r in fs["block_info"])
+    assert ts.build_forest_schedule(forest, max_block=64)["block_size"] == 64
+    lv = ts.build_level_schedule(forest)
+    assert len(lv["block_info"]) >= ts.LEVEL_MIN_BLOCKS
+    assert lv["max_block_nodes"] >= ts.LEVEL_MIN_BLOCK - 40
+    assert sum(int(r[1]) for r in lv["block_info"]) == len(forest)
+    one = np.asarray(forests()["deep_600"])  # one tree: one block whatever its size
+    assert len(ts.build_level_schedule(one)["block_info"]) == 1
+
+
 @pytest.mark.gpu
 def test_env_var_selects_variant(cuda_device, monkeypatch):
     parent = np.asarray(forests()["random_40"])
@@ -135,6 +157,7 @@ def test_env_var_selects_variant(cuda_device, monkeypatch):
     monkeypatch.setenv("JAXLEY_PYTORCH_TREE_KERNEL", "auto")
     deep = np.asarray(forests()["deep_600"])
     assert isinstance(ts.make_tree_solve_kernel(deep, cuda_device), ts.LevelTreeSolveKernel)
+    assert isinstance(ts.make_tree_solve_kernel(parent, cuda_device), ts.LevelTreeSolveKernel)
 
 
 def test_op_registry_holds_kernels_weakly():
