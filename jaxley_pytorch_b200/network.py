@@ -120,13 +120,15 @@ class NetworkSimulation:
         self.low = low = self.sim.low
         self.model = self.sim.model
         # A float32 cell step of up to 256 threads whose work items fit in one wave at
-        # two CTAs per SM runs on the forward kernels of two CTAs per SM with up to 128
-        # registers (measured on B200: point-neuron networks of 2048 cells x 32 rows,
-        # 256 items, 0.7 % faster; 2048 four-compartment cells, 1024 items, 6 % slower).
+        # two CTAs per SM runs on the kernels of two CTAs per SM with up to 128
+        # registers, forward and adjoint (measured on B200: point-neuron networks of
+        # 2048 cells x 32 rows, 256 items, 0.7 % faster each; 2048 four-compartment
+        # cells, 1024 items, 6 % slower with the forward on them).
         dev = torch.device(device)
         if dtype == torch.float32 and threads <= 256 and dev.type == "cuda" and torch.cuda.is_available():
             sms = torch.cuda.get_device_properties(dev).multi_processor_count
-            self.model.forward_wide = self.model.n_items <= 2 * sms
+            one_wave = self.model.n_items <= 2 * sms
+            self.model.forward_wide = self.model.backward_wide = one_wave
         self.init_steady = bool(init_steady)  # channel gates start at their steady state
         self.dtype, self.device = dtype, torch.device(device)
         self.B = low.batch

@@ -159,6 +159,8 @@ class DeviceModel:
         if tangent:
             self.kind_threads["forward"] = min(self.kind_threads["forward"], 512)
         self.forward_wide = bool(forward_wide) and not tangent
+        # the same for the adjoint launches (float32, up to 256 threads)
+        self.backward_wide = False
         # Threads per CTA of the groups whose work areas live in global memory (blocks
         # too large for shared memory; they run one CTA per SM at most, so they can
         # use more threads than the shared-memory groups).
@@ -342,7 +344,8 @@ class DeviceModel:
             setattr(a, k, v)
         if kind in self.kind_threads:
             a.threads = self.kind_threads[kind]
-            a.wide = int(kind == "forward" and self.forward_wide)
+            a.wide = int((kind == "forward" and self.forward_wide)
+                         or (kind == "backward" and self.backward_wide))
             ks = self.kind_sched.get(kind)
             if group["gm"] and self.gm_threads:
                 a.threads, a.wide, ks = self.gm_threads, 0, self.gm_sched
