@@ -159,7 +159,8 @@ class DeviceModel:
         if tangent:
             self.kind_threads["forward"] = min(self.kind_threads["forward"], 512)
         self.forward_wide = bool(forward_wide) and not tangent
-        # the same for the adjoint launches (float32, up to 256 threads)
+        # adjoint launches on the kernels of two CTAs per SM with up to 128 registers
+        # (float32, up to 256 threads; set by callers whose items fit in one wave)
         self.backward_wide = False
         # Threads per CTA of the groups whose work areas live in global memory (blocks
         # too large for shared memory; they run one CTA per SM at most, so they can

@@ -101,6 +101,8 @@ def autotune(problem: Problem, dtype: torch.dtype = torch.float32, device="cuda"
              verbose: bool = False) -> Tuple[Choice, Lowered, List[dict]]:
     """Returns `(choice, lowered model of the chosen block size, table of timings)`."""
     key = signature(problem, dtype, grad)
+    if sim_kwargs:  # a choice holds for the launch options it was timed with
+        key += "|" + json.dumps(sim_kwargs, sort_keys=True, default=str)
     table: List[dict] = []
     cached = _CACHE.get(key)
     if cached is None and cache_path and os.path.exists(cache_path):
